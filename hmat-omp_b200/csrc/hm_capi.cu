@@ -1,0 +1,214 @@
+// extern "C" entry points of libhmat_b200.so (declared in include/hmat_b200.h).
+// Every call converts C++ exceptions to an HM_* status and keeps the message in the
+// handle for hm_last_error().
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "hm_engine.h"
+
+struct hm_handle {
+    hm_opts opts;
+    std::string err;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    std::unique_ptr<hm::Engine> eng;
+};
+
+namespace {
+
+template <class F>
+int guard(hm_handle* h, F&& f) {
+    if (!h) return HM_ERR_ARG;
+    try {
+        f();
+        h->err.clear();
+        return HM_OK;
+    } catch (const hm::Error& e) {
+        h->err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        h->err = "host allocation failed";
+        return HM_ERR_CUDA;
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        return HM_ERR_CUDA;
+    }
+}
+
+hm::Engine& engine(hm_handle* h, hm::Engine::Kind kind) {
+    if (!h->eng || h->eng->kind() != kind) {
+        h->eng = std::make_unique<hm::Engine>(h->opts, kind);
+        h->eng->set_stream(h->stream);
+    }
+    return *h->eng;
+}
+
+hm::Engine& built(hm_handle* h) {
+    if (!h->eng) throw hm::Error(HM_ERR_STATE, "no operator built on this handle");
+    return *h->eng;
+}
+
+void validate(const hm_opts& o) {
+    HM_CHECK(o.tol == o.tol, HM_ERR_ARG, "tol is NaN");
+    HM_CHECK(o.rsvd_rank >= 0 && o.oversample >= 0 && o.rsvd_min_dim >= 1, HM_ERR_ARG, "bad rsvd options");
+    HM_CHECK(o.rsvd_rank + o.oversample <= hm::GJ_MAX, HM_ERR_UNSUPPORTED,
+             "rsvd_rank + oversample above the supported sketch width (160)");
+    HM_CHECK(o.power_iters >= 0 && o.max_rank >= 0, HM_ERR_ARG, "bad power_iters/max_rank");
+    HM_CHECK(o.sketch >= HM_SKETCH_REFERENCE_UNIFORM && o.sketch <= HM_SKETCH_DEVICE_NORMAL, HM_ERR_ARG,
+             "bad sketch");
+    HM_CHECK(o.precision == HM_FP64 || o.precision == HM_MIXED, HM_ERR_ARG, "bad precision");
+}
+
+}  // namespace
+
+extern "C" {
+
+void hm_opts_default(hm_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->tol = 1e-6;           // HODLRMatrix(double tol = 1e-6)  hodlr_routines.h:16
+    o->rsvd_rank = 64;       // rsvd_rank(64)                   hodlr_routines.h:16
+    o->oversample = 10;      // k = rank_guess + 10              compression.h:74
+    o->rsvd_min_dim = 256;   // m < 256 || n < 256 -> full SVD   compression.h:72
+    o->power_iters = 0;
+    o->max_rank = 0;
+    o->sketch = HM_SKETCH_REFERENCE_UNIFORM;
+    o->seed = 0;
+    o->precision = HM_FP64;
+    o->ir_tol = 1e-10;
+    o->ir_max_iter = 30;
+}
+
+int hm_create(const hm_opts* o, hm_handle** out) {
+    if (!out) return HM_ERR_ARG;
+    *out = nullptr;
+    auto h = std::make_unique<hm_handle>();
+    if (o) h->opts = *o;
+    else hm_opts_default(&h->opts);
+    int rc = guard(h.get(), [&] {
+        validate(h->opts);
+        int ndev = 0;
+        HM_CUDA(cudaGetDeviceCount(&ndev));
+        HM_CHECK(ndev > 0, HM_ERR_CUDA, "no CUDA device");
+        HM_CUDA(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+        h->stream = h->own;
+    });
+    if (rc != HM_OK) return rc;
+    *out = h.release();
+    return HM_OK;
+}
+
+int hm_destroy(hm_handle* h) {
+    if (!h) return HM_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->eng.reset();
+    if (h->own) cudaStreamDestroy(h->own);
+    delete h;
+    return HM_OK;
+}
+
+const char* hm_last_error(const hm_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int hm_set_stream(hm_handle* h, void* stream) {
+    return guard(h, [&] {
+        h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own;
+        if (h->eng) h->eng->set_stream(h->stream);
+    });
+}
+
+int hm_hodlr_build_from_dense_device(hm_handle* h, const double* dA, int N, int lda, int leaf) {
+    return guard(h, [&] {
+        engine(h, hm::Engine::HODLR).build_dense_device(dA, N, lda, leaf);
+    });
+}
+
+int hm_hodlr_build_from_dense(hm_handle* h, const double* A, int N, int lda, int leaf) {
+    return guard(h, [&] {
+        HM_CHECK(A && N > 0 && lda >= N, HM_ERR_ARG, "build_from_dense: bad arguments");
+        hm::DBuf<double> d((size_t)N * N);
+        HM_CUDA(cudaMemcpy2DAsync(d.p, (size_t)N * sizeof(double), A, (size_t)lda * sizeof(double),
+                                  (size_t)N * sizeof(double), N, cudaMemcpyHostToDevice, h->stream));
+        engine(h, hm::Engine::HODLR).build_dense_device(d.p, N, N, leaf);
+        HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int hm_hss_build_from_dense(hm_handle* h, const double* A, int N, int lda, int leaf) {
+    return guard(h, [&] {
+        HM_CHECK(A && N > 0 && lda >= N, HM_ERR_ARG, "build_from_dense: bad arguments");
+        hm::DBuf<double> d((size_t)N * N);
+        HM_CUDA(cudaMemcpy2DAsync(d.p, (size_t)N * sizeof(double), A, (size_t)lda * sizeof(double),
+                                  (size_t)N * sizeof(double), N, cudaMemcpyHostToDevice, h->stream));
+        engine(h, hm::Engine::HSS).build_dense_device(d.p, N, N, leaf);
+        HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int hm_hodlr_import(hm_handle* h, int N, int leaf, const int* r12, const int* r21, const double* const* D,
+                    const double* const* U, const double* const* V, const double* const* B12,
+                    const double* const* B21) {
+    return guard(h, [&] { engine(h, hm::Engine::HODLR).import_hodlr(N, leaf, r12, r21, D, U, V, B12, B21); });
+}
+
+int hm_num_nodes(const hm_handle* h) {
+    if (!h || !h->eng) return 0;
+    return (int)h->eng->nodes().size();
+}
+
+int hm_export_tree(const hm_handle* h, int* start, int* end, int* is_leaf, int* depth, int* r12, int* r21) {
+    return guard(const_cast<hm_handle*>(h), [&] {
+        built(const_cast<hm_handle*>(h)).export_tree(start, end, is_leaf, depth, r12, r21);
+    });
+}
+
+int hm_get_factor(const hm_handle* h, int node, int which, double* out, int* rows, int* cols) {
+    return guard(const_cast<hm_handle*>(h), [&] {
+        built(const_cast<hm_handle*>(h)).get_factor(node, which, out, rows, cols);
+    });
+}
+
+int hm_multiply_device(hm_handle* h, const double* dx, int nrhs, int ldx, double* dy, int ldy) {
+    return guard(h, [&] { built(h).multiply_device(dx, nrhs, ldx, dy, ldy); });
+}
+
+int hm_multiply(hm_handle* h, const double* x, int nrhs, int ldx, double* y, int ldy) {
+    return guard(h, [&] {
+        hm::Engine& e = built(h);
+        const int N = e.N();
+        HM_CHECK(x && y && nrhs >= 1 && ldx >= N && ldy >= N, HM_ERR_ARG, "multiply: bad arguments");
+        hm::DBuf<double> dx((size_t)N * nrhs), dy((size_t)N * nrhs);
+        HM_CUDA(cudaMemcpy2DAsync(dx.p, (size_t)N * 8, x, (size_t)ldx * 8, (size_t)N * 8, nrhs,
+                                  cudaMemcpyHostToDevice, h->stream));
+        e.multiply_device(dx.p, nrhs, N, dy.p, N);
+        HM_CUDA(cudaMemcpy2DAsync(y, (size_t)ldy * 8, dy.p, (size_t)N * 8, (size_t)N * 8, nrhs,
+                                  cudaMemcpyDeviceToHost, h->stream));
+        HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int hm_factor(hm_handle* h) {
+    return guard(h, [&] { built(h).factor(); });
+}
+
+int hm_solve_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx,
+                    hm_solve_stats* st) {
+    return guard(h, [&] { built(h).solve_device(db, nrhs, ldb, dx, ldx, st); });
+}
+
+int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ldx, hm_solve_stats* st) {
+    return guard(h, [&] {
+        hm::Engine& e = built(h);
+        const int N = e.N();
+        HM_CHECK(b && x && nrhs >= 1 && ldb >= N && ldx >= N, HM_ERR_ARG, "solve: bad arguments");
+        hm::DBuf<double> db((size_t)N * nrhs), dx((size_t)N * nrhs);
+        HM_CUDA(cudaMemcpy2DAsync(db.p, (size_t)N * 8, b, (size_t)ldb * 8, (size_t)N * 8, nrhs,
+                                  cudaMemcpyHostToDevice, h->stream));
+        e.solve_device(db.p, nrhs, N, dx.p, N, st);
+        HM_CUDA(cudaMemcpy2DAsync(x, (size_t)ldx * 8, dx.p, (size_t)N * 8, (size_t)N * 8, nrhs,
+                                  cudaMemcpyDeviceToHost, h->stream));
+        HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+}  // extern "C"

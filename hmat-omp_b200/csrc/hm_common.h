@@ -1,0 +1,75 @@
+// Shared definitions for the B200 hierarchical-matrix library (host + device).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/hmat_b200.h"
+
+namespace hm {
+
+// An error with an ABI status code; thrown by host code, converted at the C boundary.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define HM_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            throw ::hm::Error(HM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_) + \
+                                               " at " __FILE__ ":" + std::to_string(__LINE__)); \
+    } while (0)
+
+#define HM_CHECK(cond, code, msg)                                     \
+    do {                                                              \
+        if (!(cond)) throw ::hm::Error((code), std::string(msg));     \
+    } while (0)
+
+// Device-side status word bits (written by kernels, read by the host after a phase).
+enum : int {
+    ST_SINGULAR = 1,        // zero / non-finite pivot in an inversion
+    ST_NO_CONVERGE = 2,     // Jacobi sweeps hit their limit
+    ST_NONFINITE = 4,       // non-finite value met where a finite one is required
+};
+
+// A typed device allocation with RAII.
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    explicit DBuf(size_t count) { alloc(count); }
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DBuf() { release(); }
+    void alloc(size_t count) {
+        release();
+        n = count;
+        if (count) HM_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void zero(cudaStream_t s) {
+        if (n) HM_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+    }
+};
+
+inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace hm

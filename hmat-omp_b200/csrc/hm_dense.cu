@@ -1,0 +1,465 @@
+// Small batched dense kernels for sm_100a: one CTA per problem.
+//
+//  * gj_inverse_kernel  — Gauss-Jordan inversion with partial pivoting, the matrix held
+//                          in shared memory (n <= GJ_MAX).  Larger inverses are built by
+//                          2x2 block elimination over these plus batched GEMMs.
+//  * jacobi_kernel      — cyclic two-sided Jacobi for symmetric positive semi-definite
+//                          Gram matrices, parallel (round-robin) pair ordering, rotation
+//                          test relative to the diagonal so graded matrices keep small
+//                          eigenvalues to high relative accuracy (Demmel & Veselic, 1992).
+//  * prep_kernel        — sort eigenpairs, form the scaled/permuted rotation and the
+//                          truncation rank of compression.h:42-46.
+//  * copy / identity utilities.
+#include "hm_dense.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace hm {
+
+// ---------------------------------------------------------------------------------
+// Gauss-Jordan inverse
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) gj_inverse_kernel(const GJDesc* __restrict__ descs, int* status) {
+    extern __shared__ double sm[];
+    const GJDesc d = descs[blockIdx.x];
+    const int n = d.n;
+    if (n <= 0) return;
+    double* a = sm;                 // n x n, column-major, ld n
+    double* colv = a + n * n;
+    double* rowv = colv + n;
+    int* perm = reinterpret_cast<int*>(rowv + n);
+    __shared__ int s_piv;
+    __shared__ int s_bad;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < n * n; e += nt) {
+        int i = e % n, j = e / n;
+        a[e] = d.A[i + (size_t)j * d.lda];
+    }
+    if (tid == 0) s_bad = 0;
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+        if (tid < 32) {
+            double best = -1.0;
+            int bi = j;
+            for (int i = j + tid; i < n; i += 32) {
+                double v = fabs(a[i + j * n]);
+                if (v > best) { best = v; bi = i; }
+            }
+            for (int off = 16; off > 0; off >>= 1) {
+                double ob = __shfl_down_sync(0xffffffffu, best, off);
+                int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            if (tid == 0) {
+                s_piv = bi;
+                perm[j] = bi;
+                double pv = a[bi + j * n];
+                if (!(pv != 0.0) || !isfinite(pv)) s_bad = 1;
+            }
+        }
+        __syncthreads();
+        if (s_bad) break;
+        const int p = s_piv;
+        if (p != j)
+            for (int c = tid; c < n; c += nt) {
+                double t = a[j + c * n];
+                a[j + c * n] = a[p + c * n];
+                a[p + c * n] = t;
+            }
+        __syncthreads();
+        for (int i = tid; i < n; i += nt) colv[i] = a[i + j * n];
+        for (int c = tid; c < n; c += nt) rowv[c] = a[j + c * n];
+        __syncthreads();
+        const double inv = 1.0 / rowv[j];
+        for (int e = tid; e < n * n; e += nt) {
+            int i = e % n, c = e / n;
+            double r = (c == j) ? inv : rowv[c] * inv;
+            if (i == j) a[e] = r;
+            else a[e] = ((c == j) ? 0.0 : a[e]) - colv[i] * r;
+        }
+        __syncthreads();
+    }
+    if (s_bad) {
+        if (tid == 0) atomicOr(status, ST_SINGULAR);
+        for (int e = tid; e < n * n; e += nt) {
+            int i = e % n, j = e / n;
+            d.X[i + (size_t)j * d.ldx] = nan("");
+        }
+        return;
+    }
+    for (int j = n - 1; j >= 0; --j) {
+        const int p = perm[j];
+        if (p != j)
+            for (int i = tid; i < n; i += nt) {
+                double t = a[i + j * n];
+                a[i + j * n] = a[i + p * n];
+                a[i + p * n] = t;
+            }
+        __syncthreads();
+    }
+    for (int e = tid; e < n * n; e += nt) {
+        int i = e % n, j = e / n;
+        d.X[i + (size_t)j * d.ldx] = a[e];
+    }
+}
+
+void launch_gj(const DevTable<GJDesc>& t, int* status, cudaStream_t s) {
+    if (t.h.empty()) return;
+    int nmax = 0;
+    for (auto& d : t.h) nmax = std::max(nmax, d.n);
+    HM_CHECK(nmax <= GJ_MAX, HM_ERR_UNSUPPORTED, "Gauss-Jordan block larger than GJ_MAX");
+    size_t smem = (size_t)nmax * nmax * 8 + 2 * (size_t)nmax * 8 + (size_t)nmax * 4 + 16;
+    static bool attr = false;
+    if (!attr) {
+        HM_CUDA(cudaFuncSetAttribute(gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     227 * 1024));
+        attr = true;
+    }
+    gj_inverse_kernel<<<t.size(), 256, smem, s>>>(t.d.p, status);
+    HM_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------------
+// Cyclic Jacobi for symmetric PSD matrices (parallel round-robin ordering)
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ void jac_pair(int r, int i, int kk, int& p, int& q) {
+    // circle method on kk (even) players: player kk-1 fixed
+    const int m = kk - 1;
+    if (i == 0) { p = m; q = r; }
+    else { p = (r + i) % m; q = (r - i + m) % m; }
+    if (p > q) { int t = p; p = q; q = t; }
+}
+
+__global__ void __launch_bounds__(256) jacobi_kernel(const EigDesc* __restrict__ descs, int* status,
+                                                     int max_sweeps, int use_smem) {
+    extern __shared__ double sm[];
+    const EigDesc d = descs[blockIdx.x];
+    const int k = d.k;
+    if (k <= 0) return;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const bool in_smem = use_smem != 0;
+    const int ld = in_smem ? k : d.ldg;
+    double* g = in_smem ? sm : d.G;
+    double* cs = in_smem ? sm + k * k : sm;   // rotation cosines  (k/2+1)
+    const int kk = (k + 1) & ~1;              // even number of players (k = dummy if odd)
+    const int half = kk / 2;
+    double* sn = cs + half;
+    double* W = d.W;
+    const int ldw = d.ldw;
+    __shared__ int s_rot;
+    if (in_smem)
+        for (int e = tid; e < k * k; e += nt) {
+            int i = e % k, j = e / k;
+            g[e] = d.G[i + (size_t)j * d.ldg];
+        }
+    for (int e = tid; e < k * k; e += nt) {
+        int i = e % k, j = e / k;
+        W[i + (size_t)j * ldw] = (i == j) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const double eps = 4.0 * 2.220446049250313e-16;
+    int sweep = 0;
+    bool converged = (k == 1);
+    for (; sweep < max_sweeps && !converged; ++sweep) {
+        if (tid == 0) s_rot = 0;
+        __syncthreads();
+        for (int r = 0; r < kk - 1; ++r) {
+            for (int t = tid; t < half; t += nt) {
+                int p, q;
+                jac_pair(r, t, kk, p, q);
+                double c = 1.0, s = 0.0;
+                if (q < k) {
+                    const double app = g[p + p * ld], aqq = g[q + q * ld], apq = g[p + q * ld];
+                    const double thr = eps * sqrt(fabs(app)) * sqrt(fabs(aqq));
+                    if (fabs(apq) > thr && apq != 0.0) {
+                        const double tau = (aqq - app) / (2.0 * apq);
+                        const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + hypot(1.0, tau));
+                        c = 1.0 / sqrt(1.0 + tt * tt);
+                        s = tt * c;
+                        s_rot = 1;
+                    }
+                }
+                cs[t] = c;
+                sn[t] = s;
+            }
+            __syncthreads();
+            // G <- G J (columns p, q), W <- W J
+            for (int e = tid; e < half * k; e += nt) {
+                const int t = e / k, i = e % k;
+                const double s = sn[t];
+                if (s == 0.0) continue;
+                int p, q;
+                jac_pair(r, t, kk, p, q);
+                const double c = cs[t];
+                const double gp = g[i + p * ld], gq = g[i + q * ld];
+                g[i + p * ld] = c * gp - s * gq;
+                g[i + q * ld] = s * gp + c * gq;
+                const double wp = W[i + (size_t)p * ldw], wq = W[i + (size_t)q * ldw];
+                W[i + (size_t)p * ldw] = c * wp - s * wq;
+                W[i + (size_t)q * ldw] = s * wp + c * wq;
+            }
+            __syncthreads();
+            // G <- J^T G (rows p, q)
+            for (int e = tid; e < half * k; e += nt) {
+                const int t = e / k, j = e % k;
+                const double s = sn[t];
+                if (s == 0.0) continue;
+                int p, q;
+                jac_pair(r, t, kk, p, q);
+                const double c = cs[t];
+                const double gp = g[p + j * ld], gq = g[q + j * ld];
+                g[p + j * ld] = c * gp - s * gq;
+                g[q + j * ld] = s * gp + c * gq;
+            }
+            __syncthreads();
+            // exact zeros for the annihilated pairs, symmetric
+            for (int t = tid; t < half; t += nt) {
+                if (sn[t] == 0.0) continue;
+                int p, q;
+                jac_pair(r, t, kk, p, q);
+                g[p + q * ld] = 0.0;
+                g[q + p * ld] = 0.0;
+            }
+            __syncthreads();
+        }
+        converged = (s_rot == 0);
+        __syncthreads();
+    }
+    if (!converged && tid == 0) atomicOr(status, ST_NO_CONVERGE);
+    for (int i = tid; i < k; i += nt) d.lam[i] = g[i + i * ld];
+}
+
+void launch_jacobi(const DevTable<EigDesc>& t, int* status, cudaStream_t s, int max_sweeps) {
+    if (t.h.empty()) return;
+    int kmax = 0;
+    for (auto& d : t.h) kmax = std::max(kmax, d.k);
+    size_t smem = (kmax <= JAC_SMEM_MAX ? (size_t)kmax * kmax * 8 : 0) + ((size_t)kmax + 2) * 8;
+    static bool attr = false;
+    if (!attr) {
+        HM_CUDA(cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     227 * 1024));
+        attr = true;
+    }
+    jacobi_kernel<<<t.size(), 256, smem, s>>>(t.d.p, status, max_sweeps, kmax <= JAC_SMEM_MAX);
+    HM_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------------
+// Sort eigenpairs (descending), scale, truncation rank
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) prep_kernel(const PrepDesc* __restrict__ descs, double tol,
+                                                   int max_rank) {
+    extern __shared__ double sm[];
+    const PrepDesc d = descs[blockIdx.x];
+    const int k = d.k;
+    if (k <= 0) return;
+    double* lam = sm;
+    int* perm = reinterpret_cast<int*>(lam + k);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < k; i += nt) lam[i] = d.lam[i];
+    __syncthreads();
+    // rank of each entry in descending order (ties by index): perm[pos] = i
+    for (int i = tid; i < k; i += nt) {
+        const double v = lam[i];
+        int pos = 0;
+        for (int j = 0; j < k; ++j) {
+            const double w = lam[j];
+            pos += (w > v) || (w == v && j < i);
+        }
+        perm[pos] = i;
+    }
+    __syncthreads();
+    for (int e = tid; e < k * k; e += nt) {
+        const int i = e % k, c = e / k;
+        const int src = perm[c];
+        const double sig = sqrt(fmax(lam[src], 0.0));
+        const double w = d.W[i + (size_t)src * d.ldw];
+        d.Ws[i + (size_t)c * d.ldws] = sig > 0.0 ? w / sig : 0.0;
+        if (d.Wp) d.Wp[i + (size_t)c * d.ldwp] = w;
+    }
+    if (d.sigma)
+        for (int c = tid; c < k; c += nt) d.sigma[c] = sqrt(fmax(lam[perm[c]], 0.0));
+    if (d.rank && tid == 0) {
+        // compression.h:42-46: #{S_i > tol*S_0} when S_0 > 1e-15, at least 1
+        const double s0 = sqrt(fmax(lam[perm[0]], 0.0));
+        int r = 0;
+        if (s0 > 1e-15)
+            for (int c = 0; c < k; ++c) r += sqrt(fmax(lam[perm[c]], 0.0)) > tol * s0;
+        if (r == 0) r = 1;
+        if (max_rank > 0 && r > max_rank) r = max_rank;
+        *d.rank = r;
+    }
+}
+
+void launch_prep(const DevTable<PrepDesc>& t, double tol, int max_rank, cudaStream_t s) {
+    if (t.h.empty()) return;
+    int kmax = 0;
+    for (auto& d : t.h) kmax = std::max(kmax, d.k);
+    size_t smem = (size_t)kmax * 12 + 16;
+    prep_kernel<<<t.size(), 256, smem, s>>>(t.d.p, tol, max_rank);
+    HM_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------------
+// Copies (optionally transposed, optionally to FP32) and identity fills
+// ---------------------------------------------------------------------------------
+__global__ void copy_kernel(const CopyDesc* __restrict__ descs) {
+    const CopyDesc d = descs[blockIdx.y];
+    const size_t total = (size_t)d.rows * d.cols;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e % d.rows), j = (int)(e / d.rows);
+        const size_t si = d.trans ? j + (size_t)i * d.lds : i + (size_t)j * d.lds;
+        const double v = d.src_f32 ? (double)static_cast<const float*>(d.src)[si]
+                                   : static_cast<const double*>(d.src)[si];
+        const size_t di = i + (size_t)j * d.ldd;
+        if (d.dst_f32) static_cast<float*>(d.dst)[di] = (float)v;
+        else static_cast<double*>(d.dst)[di] = v;
+    }
+}
+
+void launch_copy(const DevTable<CopyDesc>& t, cudaStream_t s) {
+    if (t.h.empty()) return;
+    size_t mx = 0;
+    for (auto& d : t.h) mx = std::max(mx, (size_t)d.rows * d.cols);
+    int gx = (int)std::min<size_t>(std::max<size_t>(1, (mx + 255) / 256), 2048);
+    HM_CHECK(t.size() <= 65535, HM_ERR_UNSUPPORTED, "copy batch too large");
+    copy_kernel<<<dim3(gx, t.size()), 256, 0, s>>>(t.d.p);
+    HM_CUDA(cudaGetLastError());
+}
+
+__global__ void ident_kernel(const IdentDesc* __restrict__ descs) {
+    const IdentDesc d = descs[blockIdx.y];
+    const size_t total = (size_t)d.rows * d.cols;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e % d.rows), j = (int)(e / d.rows);
+        d.X[i + (size_t)j * d.ldx] = (i == j) ? d.diag : 0.0;
+    }
+}
+
+void launch_ident(const DevTable<IdentDesc>& t, cudaStream_t s) {
+    if (t.h.empty()) return;
+    size_t mx = 0;
+    for (auto& d : t.h) mx = std::max(mx, (size_t)d.rows * d.cols);
+    int gx = (int)std::min<size_t>(std::max<size_t>(1, (mx + 255) / 256), 1024);
+    HM_CHECK(t.size() <= 65535, HM_ERR_UNSUPPORTED, "identity batch too large");
+    ident_kernel<<<dim3(gx, t.size()), 256, 0, s>>>(t.d.p);
+    HM_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------------
+// Plans
+// ---------------------------------------------------------------------------------
+void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t s) {
+    std::vector<InvProblem> small, large;
+    for (auto& p : probs) {
+        if (p.n <= 0) continue;
+        (p.n <= GJ_MAX ? small : large).push_back(p);
+    }
+    if (!small.empty()) {
+        auto st = std::make_unique<GJStep>();
+        for (auto& p : small) st->t.h.push_back({p.A, p.lda, p.X, p.ldx, p.n});
+        st->t.upload(s);
+        plan.add(std::move(st));
+    }
+    if (large.empty()) return;
+    // 2x2 block elimination: X11 = inv(A11), T = X11 A12, W = A21 X11,
+    // S = A22 - A21 T, X22 = inv(S), X12 = -T X22, X21 = -X22 W, X11 -= X12 W.
+    std::vector<InvProblem> sub11, sub22;
+    auto copyS = std::make_unique<CopyStep>();
+    auto g1 = std::make_unique<GemmStep<double>>();
+    auto g2 = std::make_unique<GemmStep<double>>();
+    auto g3 = std::make_unique<GemmStep<double>>();
+    auto g4 = std::make_unique<GemmStep<double>>();
+    for (auto& p : large) {
+        HM_CHECK(p.A != p.X, HM_ERR_ARG, "block inverse cannot run in place");
+        const int a = p.n / 2, b = p.n - a;
+        const double* A11 = p.A;
+        const double* A12 = p.A + (size_t)a * p.lda;
+        const double* A21 = p.A + a;
+        const double* A22 = p.A + a + (size_t)a * p.lda;
+        double* X11 = p.X;
+        double* X12 = p.X + (size_t)a * p.ldx;
+        double* X21 = p.X + a;
+        double* X22 = p.X + a + (size_t)a * p.ldx;
+        double* T = plan.scratch((size_t)a * b);
+        double* W = plan.scratch((size_t)b * a);
+        double* S = plan.scratch((size_t)b * b);
+        sub11.push_back({A11, p.lda, X11, p.ldx, a});
+        copyS->t.h.push_back({A22, p.lda, S, b, b, b, 0, 0, 0});
+        g1->batch.add(a, b, a, 1.0, X11, p.ldx, OP_N, A12, p.lda, OP_N, 0.0, T, a);
+        g1->batch.add(b, a, a, 1.0, A21, p.lda, OP_N, X11, p.ldx, OP_N, 0.0, W, b);
+        g2->batch.add(b, b, a, -1.0, A21, p.lda, OP_N, T, a, OP_N, 1.0, S, b);
+        sub22.push_back({S, b, X22, p.ldx, b});
+        g3->batch.add(a, b, b, -1.0, T, a, OP_N, X22, p.ldx, OP_N, 0.0, X12, p.ldx);
+        g3->batch.add(b, a, b, -1.0, X22, p.ldx, OP_N, W, b, OP_N, 0.0, X21, p.ldx);
+        g4->batch.add(a, a, b, -1.0, X12, p.ldx, OP_N, W, b, OP_N, 1.0, X11, p.ldx);
+    }
+    copyS->t.upload(s);
+    plan.add(std::move(copyS));
+    plan_inverse(plan, sub11, s);
+    g1->batch.finalize(s);
+    plan.add(std::move(g1));
+    g2->batch.finalize(s);
+    plan.add(std::move(g2));
+    plan_inverse(plan, sub22, s);
+    g3->batch.finalize(s);
+    plan.add(std::move(g3));
+    g4->batch.finalize(s);
+    plan.add(std::move(g4));
+}
+
+void plan_gram_svd(Plan& plan, const std::vector<SvdProblem>& probs, double tol, int max_rank,
+                   cudaStream_t s) {
+    if (probs.empty()) return;
+    auto gramA = std::make_unique<GemmStep<double>>();
+    auto eigA = std::make_unique<EigStep>();
+    auto rotA = std::make_unique<GemmStep<double>>();
+    auto gramB = std::make_unique<GemmStep<double>>();
+    auto eigB = std::make_unique<EigStep>();
+    auto prep = std::make_unique<PrepStep>();
+    auto outL = std::make_unique<GemmStep<double>>();
+    auto outR = std::make_unique<GemmStep<double>>();
+    prep->tol = tol;
+    prep->max_rank = max_rank;
+    for (auto& p : probs) {
+        const int k = p.k, m = p.rows;
+        if (k <= 0 || m <= 0) continue;
+        double* G = plan.scratch((size_t)k * k);
+        double* W1 = plan.scratch((size_t)k * k);
+        double* W2 = plan.scratch((size_t)k * k);
+        double* lam1 = plan.scratch(k);
+        double* lam2 = plan.scratch(k);
+        double* Ws = plan.scratch((size_t)k * k);
+        double* Wp = p.R ? plan.scratch((size_t)k * k) : nullptr;
+        double* X1 = plan.scratch((size_t)m * k);
+        gramA->batch.add(k, k, m, 1.0, p.X, p.ldx, OP_T, p.X, p.ldx, OP_N, 0.0, G, k);
+        eigA->t.h.push_back({G, k, W1, k, lam1, k});
+        rotA->batch.add(m, k, k, 1.0, p.X, p.ldx, OP_N, W1, k, OP_N, 0.0, X1, m);
+        gramB->batch.add(k, k, m, 1.0, X1, m, OP_T, X1, m, OP_N, 0.0, G, k);
+        eigB->t.h.push_back({G, k, W2, k, lam2, k});
+        prep->t.h.push_back({lam2, W2, k, Ws, k, Wp, k, p.sigma, p.rank, k});
+        outL->batch.add(m, k, k, 1.0, X1, m, OP_N, Ws, k, OP_N, 0.0, p.L, p.ldl);
+        if (p.R) outR->batch.add(k, k, k, 1.0, W1, k, OP_N, Wp, k, OP_N, 0.0, p.R, p.ldr);
+    }
+    gramA->batch.finalize(s);
+    eigA->t.upload(s);
+    rotA->batch.finalize(s);
+    gramB->batch.finalize(s);
+    eigB->t.upload(s);
+    prep->t.upload(s);
+    outL->batch.finalize(s);
+    outR->batch.finalize(s);
+    plan.add(std::move(gramA));
+    plan.add(std::move(eigA));
+    plan.add(std::move(rotA));
+    plan.add(std::move(gramB));
+    plan.add(std::move(eigB));
+    plan.add(std::move(prep));
+    plan.add(std::move(outL));
+    if (!outR->batch.empty()) plan.add(std::move(outR));
+}
+
+}  // namespace hm

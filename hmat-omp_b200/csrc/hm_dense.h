@@ -1,0 +1,188 @@
+// Small batched dense kernels (one CTA per problem) and the host plans that chain
+// them with the batched GEMM: inverses, Gram/Jacobi SVDs, copies.
+#pragma once
+
+#include <algorithm>
+#include <memory>
+
+#include "hm_gemm.h"
+
+namespace hm {
+
+// Largest matrix inverted directly in shared memory by Gauss-Jordan.
+constexpr int GJ_MAX = 160;
+// Larger inverses are split 2x2 (block elimination) down to this size.
+constexpr int GJ_SPLIT = 128;
+// Largest Gram matrix held in shared memory by the Jacobi eigen-solver.
+constexpr int JAC_SMEM_MAX = 128;
+
+struct GJDesc {
+    const double* A;
+    int lda;
+    double* X;
+    int ldx;
+    int n;
+};
+
+struct EigDesc {
+    double* G;     // k x k symmetric (overwritten)
+    int ldg;
+    double* W;     // k x k eigenvectors (output)
+    int ldw;
+    double* lam;   // k eigenvalues (output, unsorted)
+    int k;
+};
+
+// Per-problem post-processing of a Jacobi eigen-decomposition of X^T X.
+struct PrepDesc {
+    const double* lam;   // k
+    const double* W;     // k x k
+    int ldw;
+    double* Ws;          // k x k: W[:, perm] * diag(1/sigma)  (0 where sigma == 0)
+    int ldws;
+    double* Wp;          // optional k x k: W[:, perm]
+    int ldwp;
+    double* sigma;       // optional k: sorted singular values
+    int* rank;           // optional: truncation rank
+    int k;
+};
+
+struct CopyDesc {
+    const void* src;     // double, or float when src_f32
+    int lds;
+    void* dst;           // double, or float when dst_f32
+    int ldd;
+    int rows, cols;      // of the destination
+    int trans;           // dst(i,j) = src(j,i)
+    int src_f32 = 0;
+    int dst_f32 = 0;
+};
+
+struct IdentDesc {
+    double* X;
+    int ldx;
+    int rows, cols;
+    double diag;
+};
+
+template <typename T>
+struct DevTable {
+    std::vector<T> h;
+    DBuf<T> d;
+    void upload(cudaStream_t s) {
+        if (h.empty()) return;
+        d.alloc(h.size());
+        HM_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    int size() const { return (int)h.size(); }
+};
+
+void launch_gj(const DevTable<GJDesc>& t, int* status, cudaStream_t s);
+void launch_jacobi(const DevTable<EigDesc>& t, int* status, cudaStream_t s, int max_sweeps = 40);
+void launch_prep(const DevTable<PrepDesc>& t, double tol, int max_rank, cudaStream_t s);
+void launch_copy(const DevTable<CopyDesc>& t, cudaStream_t s);
+void launch_ident(const DevTable<IdentDesc>& t, cudaStream_t s);
+
+// A recorded sequence of batched launches (the unit that is replayed or captured).
+class Plan {
+  public:
+    struct Step {
+        virtual ~Step() = default;
+        virtual void run(cudaStream_t s, int* status) const = 0;
+    };
+    void add(std::unique_ptr<Step> st) { steps_.push_back(std::move(st)); }
+    void run(cudaStream_t s, int* status) const {
+        for (auto& st : steps_) st->run(s, status);
+    }
+    bool empty() const { return steps_.empty(); }
+    // device scratch owned by the plan (bump-allocated from large chunks)
+    double* scratch(size_t count) { return static_cast<double*>(bump(count * sizeof(double))); }
+    float* scratch_f(size_t count) { return static_cast<float*>(bump(count * sizeof(float))); }
+    int* scratch_i(size_t count) { return static_cast<int*>(bump(count * sizeof(int))); }
+    void clear() { steps_.clear(); chunks_.clear(); used_ = cap_ = 0; }
+    size_t scratch_bytes() const {
+        size_t b = 0;
+        for (auto& c : chunks_) b += c.n;
+        return b;
+    }
+
+  private:
+    void* bump(size_t bytes) {
+        bytes = align_up(std::max<size_t>(bytes, 1), 256);
+        if (chunks_.empty() || used_ + bytes > cap_) {
+            size_t c = std::max<size_t>(bytes, size_t(64) << 20);
+            chunks_.emplace_back(c);
+            used_ = 0;
+            cap_ = c;
+        }
+        void* p = chunks_.back().p + used_;
+        used_ += bytes;
+        return p;
+    }
+    std::vector<std::unique_ptr<Step>> steps_;
+    std::vector<DBuf<unsigned char>> chunks_;
+    size_t used_ = 0, cap_ = 0;
+};
+
+template <typename T>
+struct GemmStep : Plan::Step {
+    GemmBatch<T> batch;
+    GenParams gp;
+    explicit GemmStep(int cfg = CFG_64x64, int gen = GEN_DENSE) : batch(cfg, gen) {}
+    void run(cudaStream_t s, int*) const override { batch.launch(s, gp); }
+};
+
+struct GJStep : Plan::Step {
+    DevTable<GJDesc> t;
+    void run(cudaStream_t s, int* st) const override { launch_gj(t, st, s); }
+};
+struct EigStep : Plan::Step {
+    DevTable<EigDesc> t;
+    void run(cudaStream_t s, int* st) const override { launch_jacobi(t, st, s); }
+};
+struct PrepStep : Plan::Step {
+    DevTable<PrepDesc> t;
+    double tol = 0;
+    int max_rank = 0;
+    void run(cudaStream_t s, int*) const override { launch_prep(t, tol, max_rank, s); }
+};
+struct CopyStep : Plan::Step {
+    DevTable<CopyDesc> t;
+    void run(cudaStream_t s, int*) const override { launch_copy(t, s); }
+};
+struct IdentStep : Plan::Step {
+    DevTable<IdentDesc> t;
+    void run(cudaStream_t s, int*) const override { launch_ident(t, s); }
+};
+
+// X_i = inv(A_i) for a batch of square FP64 matrices of any size (X may not alias A
+// when n > GJ_MAX).  Appends the launches to `plan`.
+struct InvProblem {
+    const double* A;
+    int lda;
+    double* X;
+    int ldx;
+    int n;
+};
+void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t s);
+
+// Gram/Jacobi SVD of tall X_i (rows x k): X = L diag(sigma) R^T with L (rows x k)
+// orthonormal columns and R (k x k) orthogonal, sigma sorted descending; optionally
+// the truncation rank.  Two rounds (X1 = X W1, then the graded X1^T X1) keep small
+// singular values accurate relative to their own size.
+struct SvdProblem {
+    const double* X;
+    int ldx;
+    int rows, k;
+    double* L;      // rows x k (may alias X)
+    int ldl;
+    double* R;      // k x k (nullptr: not needed, e.g. orthonormalisation only)
+    int ldr;
+    double* sigma;  // k (nullptr allowed)
+    int* rank;      // nullptr allowed
+    bool sort;
+};
+void plan_gram_svd(Plan& plan, const std::vector<SvdProblem>& probs, double tol, int max_rank,
+                   cudaStream_t s);
+
+}  // namespace hm

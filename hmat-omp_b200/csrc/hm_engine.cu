@@ -1,0 +1,1043 @@
+// Level-synchronous HODLR engine: every phase is a short sequence of batched launches
+// per tree level, each launch covering all nodes of that level.
+//
+// Operator (per internal node n with children c1 = [s, mid), c2 = [mid, e)):
+//   A_n = [[A_c1, U1 B12 V2^T], [U2 B21 V1^T, A_c2]]
+// HODLR (hodlr_routines.h:55-61): U1 = left.U, V2 = right.V, B12 = diag(S) of A12's
+// compression; U2 = right.U, V1 = left.V, B21 = diag(S) of A21's.
+//
+// Factorization (bottom-up; replaces the per-call recursion of hodlr_routines.h:112-175):
+//   leaves:  Dinv = D^{-1};  Q_c[rows of leaf] = Dinv U_c[rows of leaf] for every basis
+//            block c on the leaf's path to the root.
+//   level d (deepest first), node n:  K1 = V1^T Q1, K2 = V2^T Q2,
+//            M = [[I, K1 B12], [K2 B21, I]]  (= I + K B^, the stable capacitance form of
+//            hss_routines.h:253-254), P = B^ M^{-1},
+//            then for every basis block W on n's path: t = [V1^T W1; V2^T W2],
+//            delta = P t, W1 -= Q1 delta_1, W2 -= Q2 delta_2.
+// Solve: z = Dinv b per leaf, then the same update per level on z.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <random>
+
+#include "hm_engine.h"
+
+namespace hm {
+
+// ---------------------------------------------------------------------------------
+// Trees
+// ---------------------------------------------------------------------------------
+std::vector<Node> hodlr_tree(int N, int leaf) {
+    std::vector<Node> out;
+    std::function<int(int, int, int, int)> rec = [&](int s, int e, int d, int parent) -> int {
+        int id = (int)out.size();
+        out.emplace_back();
+        out[id].start = s;
+        out[id].end = e;
+        out[id].depth = d;
+        out[id].parent = parent;
+        if (e - s <= leaf) {
+            out[id].is_leaf = 1;
+        } else {
+            int m = (s + e) / 2;
+            int l = rec(s, m, d + 1, id);
+            int r = rec(m, e, d + 1, id);
+            out[id].left = l;
+            out[id].right = r;
+        }
+        return id;
+    };
+    rec(0, N, 0, -1);
+    return out;
+}
+
+std::vector<Node> hss_tree(int N, int leaf) {
+    std::vector<Node> out(1);
+    out[0].start = 0;
+    out[0].end = N;
+    std::function<void(int)> rec = [&](int id) {
+        Node n = out[id];
+        if (n.end - n.start <= leaf) {
+            out[id].is_leaf = 1;
+            return;
+        }
+        int m = (n.start + n.end) / 2;
+        int l = (int)out.size();
+        out.emplace_back();
+        out[l].start = n.start; out[l].end = m; out[l].depth = n.depth + 1; out[l].parent = id;
+        int r = (int)out.size();
+        out.emplace_back();
+        out[r].start = m; out[r].end = n.end; out[r].depth = n.depth + 1; out[r].parent = id;
+        out[id].left = l;
+        out[id].right = r;
+        rec(l);
+        rec(r);
+    };
+    rec(0);
+    return out;
+}
+
+// ---------------------------------------------------------------------------------
+// Small device kernels used by the engine
+// ---------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11), keyed by the seed; one N(0,1)
+// value per element via Box-Muller on the first two output words.
+__device__ __forceinline__ void philox_round(uint32_t (&c)[4], uint32_t (&k)[2]) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    uint32_t hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
+    uint32_t hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
+    uint32_t n0 = hi1 ^ c[1] ^ k[0], n1 = lo1, n2 = hi0 ^ c[3] ^ k[1], n3 = lo0;
+    c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+    k[0] += 0x9E3779B9u;
+    k[1] += 0xBB67AE85u;
+}
+
+__global__ void normal_fill_kernel(double* out, size_t count, unsigned long long seed,
+                                   unsigned long long base) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < count;
+         e += (size_t)gridDim.x * blockDim.x) {
+        unsigned long long g = base + e;
+        uint32_t c[4] = {(uint32_t)g, (uint32_t)(g >> 32), 0x5eedu, 0u};
+        uint32_t k[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+#pragma unroll
+        for (int r = 0; r < 10; ++r) philox_round(c, k);
+        const double u1 = ((double)c[0] + 1.0) * 2.3283064365386963e-10;  // (0, 1]
+        const double u2 = (double)c[1] * 2.3283064365386963e-10;          // [0, 1)
+        out[e] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+    }
+}
+
+// r = b - r (in place on r), rf = float(r), per-column sums of r^2 and b^2.
+__global__ void residual_kernel(const double* __restrict__ b, double* __restrict__ r,
+                                float* __restrict__ rf, int N, int s, double* __restrict__ nr2,
+                                double* __restrict__ nb2) {
+    const int j = blockIdx.y;
+    double a2 = 0.0, c2 = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        size_t e = i + (size_t)j * N;
+        double bv = b[e];
+        double rv = bv - r[e];
+        r[e] = rv;
+        rf[e] = (float)rv;
+        a2 += rv * rv;
+        c2 += bv * bv;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        a2 += __shfl_down_sync(0xffffffffu, a2, off);
+        c2 += __shfl_down_sync(0xffffffffu, c2, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&nr2[j], a2);
+        atomicAdd(&nb2[j], c2);
+    }
+}
+
+// x += double(d)
+__global__ void accumulate_kernel(double* __restrict__ x, const float* __restrict__ d, size_t n,
+                                  int first) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x)
+        x[e] = first ? (double)d[e] : x[e] + (double)d[e];
+}
+
+__global__ void to_float_kernel(const double* __restrict__ a, float* __restrict__ b, size_t n) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x)
+        b[e] = (float)a[e];
+}
+
+__global__ void nonfinite_kernel(const double* __restrict__ a, size_t n, int* status) {
+    bool bad = false;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x)
+        bad |= !isfinite(a[e]);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(status, ST_NONFINITE);
+}
+
+static int grid_for(size_t n, int bs = 256, int cap = 148 * 16) {
+    return (int)std::min<size_t>(std::max<size_t>(1, (n + bs - 1) / bs), (size_t)cap);
+}
+
+// ---------------------------------------------------------------------------------
+// Planning helpers
+// ---------------------------------------------------------------------------------
+std::vector<int> Engine::path_of(int n) const {
+    std::vector<int> p;
+    for (int c = n; c >= 0 && nodes_[c].parent >= 0; c = nodes_[c].parent) p.push_back(c);
+    return p;
+}
+
+void Engine::plan_levels() {
+    levels_.clear();
+    leaves_.clear();
+    int maxd = 0;
+    for (auto& n : nodes_) maxd = std::max(maxd, n.depth);
+    levels_.resize(maxd + 1);
+    for (int i = 0; i < (int)nodes_.size(); ++i) {
+        if (nodes_[i].is_leaf) leaves_.push_back(i);
+        else levels_[nodes_[i].depth].push_back(i);
+    }
+    while (!levels_.empty() && levels_.back().empty()) levels_.pop_back();
+}
+
+void Engine::check_status(const char* what) {
+    int st = 0;
+    HM_CUDA(cudaMemcpyAsync(&st, dstatus.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    HM_CUDA(cudaStreamSynchronize(stream_));
+    if (st & ST_SINGULAR) throw Error(HM_ERR_SINGULAR, std::string(what) + ": singular pivot");
+    if (st & ST_NONFINITE) throw Error(HM_ERR_NONFINITE, std::string(what) + ": non-finite values");
+    if (st & ST_NO_CONVERGE)
+        throw Error(HM_ERR_NO_CONVERGE, std::string(what) + ": Jacobi sweep limit reached");
+}
+
+// Column capacity of each basis block from the compression rules (compression.h:72-75).
+void Engine::alloc_bases() {
+    size_t offU = 0, offV = 0, offD = 0;
+    for (auto& n : nodes_) {
+        if (n.is_leaf) {
+            n.offD = offD;
+            offD += (size_t)n.len() * n.len();
+        }
+    }
+    for (auto& n : nodes_) {
+        if (n.parent < 0) continue;
+        n.offU = offU;
+        offU += (size_t)n.len() * n.capU;
+        n.offV = offV;
+        offV += (size_t)n.len() * n.capV;
+    }
+    dD.alloc(std::max<size_t>(offD, 1));
+    dU.alloc(std::max<size_t>(offU, 1));
+    dV.alloc(std::max<size_t>(offV, 1));
+    dU.zero(stream_);
+    dV.zero(stream_);
+}
+
+// ---------------------------------------------------------------------------------
+// Build from a dense device matrix (hodlr_routines.h:20-63 + compression.h)
+// ---------------------------------------------------------------------------------
+namespace {
+struct Block {
+    int node, which;   // which: 0 = A12 (rows c1, cols c2), 1 = A21 (rows c2, cols c1)
+    int m, n, r0, c0, crow, ccol;
+    bool rsvd;
+    int k;
+    size_t omega = 0;  // offset of Omega in the sketch buffer
+    int slot = 0;      // rank / sigma slot
+};
+}  // namespace
+
+void Engine::build_dense_device(const double* dA, int N, int lda, int leaf) {
+    HM_CHECK(N > 0 && leaf > 0 && lda >= N && dA, HM_ERR_ARG, "build_from_dense: bad arguments");
+    N_ = N;
+    leaf_ = leaf;
+    built_ = factored_ = false;
+    f64_.ready = f32_.ready = false;
+    mv_plans_.clear();
+    solve64_plans_.clear();
+    solve32_plans_.clear();
+    nodes_ = kind_ == HODLR ? hodlr_tree(N, leaf) : hss_tree(N, leaf);
+    plan_levels();
+    if (!dstatus.p) dstatus.alloc(1);
+    dstatus.zero(stream_);
+    {   // reject non-finite input before any compression
+        DevTable<CopyDesc> none;
+        (void)none;
+        for (int j = 0; j < N; j += 4096) {
+            const int cols = std::min(4096, N - j);
+            // columns j..j+cols are contiguous only when lda == N; check column by column otherwise
+            if (lda == N) {
+                const size_t cnt = (size_t)N * cols;
+                nonfinite_kernel<<<grid_for(cnt), 256, 0, stream_>>>(dA + (size_t)j * lda, cnt, dstatus.p);
+            } else {
+                for (int c = 0; c < cols; ++c)
+                    nonfinite_kernel<<<grid_for(N), 256, 0, stream_>>>(dA + (size_t)(j + c) * lda, N, dstatus.p);
+            }
+        }
+        HM_CUDA(cudaGetLastError());
+        check_status("build_from_dense: input");
+    }
+    if (kind_ == HODLR) build_hodlr(dA, lda);
+    else build_hss(dA, lda);
+    built_ = true;
+}
+
+void Engine::build_hodlr(const double* dA, int lda) {
+    const int kguess = opts_.rsvd_rank + opts_.oversample;
+    HM_CHECK(opts_.rsvd_rank >= 0 && opts_.oversample >= 0, HM_ERR_ARG, "bad rsvd_rank/oversample");
+    // blocks in the reference's serial post-order (hodlr_routines.h:43-53)
+    std::vector<Block> blocks;
+    std::function<void(int)> post = [&](int id) {
+        const Node& n = nodes_[id];
+        if (n.is_leaf) return;
+        post(n.left);
+        post(n.right);
+        const Node& L = nodes_[n.left];
+        const Node& R = nodes_[n.right];
+        for (int w = 0; w < 2; ++w) {
+            Block b{};
+            b.node = id;
+            b.which = w;
+            if (w == 0) { b.m = L.len(); b.n = R.len(); b.r0 = L.start; b.c0 = R.start; b.crow = n.left; b.ccol = n.right; }
+            else { b.m = R.len(); b.n = L.len(); b.r0 = R.start; b.c0 = L.start; b.crow = n.right; b.ccol = n.left; }
+            b.rsvd = b.m >= opts_.rsvd_min_dim && b.n >= opts_.rsvd_min_dim;  // compression.h:72
+            b.k = b.rsvd ? std::min(kguess, std::min(b.m, b.n)) : std::min(b.m, b.n);
+            b.slot = (int)blocks.size();
+            blocks.push_back(b);
+        }
+    };
+    post(0);
+    HM_CHECK((int)blocks.size() <= 1 << 26, HM_ERR_UNSUPPORTED, "tree too large");
+    // capacities
+    for (auto& b : blocks) {
+        nodes_[b.crow].capU = b.k;
+        nodes_[b.ccol].capV = b.k;
+    }
+    alloc_bases();
+    // leaf blocks D (hodlr_routines.h:32-34)
+    {
+        CopyStep cp;
+        for (int l : leaves_) {
+            const Node& n = nodes_[l];
+            cp.t.h.push_back({dA + n.start + (size_t)n.start * lda, lda, dD.p + n.offD, n.len(),
+                              n.len(), n.len(), 0, 0, 0});
+        }
+        cp.t.upload(stream_);
+        cp.run(stream_, dstatus.p);
+    }
+    // sketches
+    size_t omega_total = 0;
+    for (auto& b : blocks)
+        if (b.rsvd) { b.omega = omega_total; omega_total += (size_t)b.n * b.k; }
+    DBuf<double> dOmega(std::max<size_t>(omega_total, 1));
+    if (omega_total) {
+        if (opts_.sketch == HM_SKETCH_DEVICE_NORMAL) {
+            normal_fill_kernel<<<grid_for(omega_total), 256, 0, stream_>>>(dOmega.p, omega_total,
+                                                                           opts_.seed, 0ull);
+            HM_CUDA(cudaGetLastError());
+        } else {
+            // Matrix::Random (matrix.h:50-57): one std::mt19937 seeded once, a fresh
+            // distribution per call, column-major fill, calls in build order.
+            std::vector<double> host(omega_total);
+            std::mt19937 gen((std::mt19937::result_type)opts_.seed);
+            for (auto& b : blocks) {
+                if (!b.rsvd) continue;
+                double* o = host.data() + b.omega;
+                size_t cnt = (size_t)b.n * b.k;
+                if (opts_.sketch == HM_SKETCH_REFERENCE_NORMAL) {
+                    std::normal_distribution<double> dist(0.0, 1.0);
+                    for (size_t i = 0; i < cnt; ++i) o[i] = dist(gen);
+                } else {
+                    std::uniform_real_distribution<double> dist(0.0, 1.0);
+                    for (size_t i = 0; i < cnt; ++i) o[i] = dist(gen);
+                }
+            }
+            HM_CUDA(cudaMemcpyAsync(dOmega.p, host.data(), omega_total * sizeof(double),
+                                    cudaMemcpyHostToDevice, stream_));
+            HM_CUDA(cudaStreamSynchronize(stream_));
+        }
+    }
+    // per-block sigma and rank
+    std::vector<size_t> sig_off(blocks.size());
+    size_t sig_total = 0;
+    for (auto& b : blocks) { sig_off[b.slot] = sig_total; sig_total += b.k; }
+    DBuf<double> dSig(std::max<size_t>(sig_total, 1));
+    DBuf<int> dRank(std::max<size_t>(blocks.size(), 1));
+    dSig.zero(stream_);
+    dRank.zero(stream_);
+
+    // one batched pipeline per tree level
+    std::map<int, std::vector<Block*>> by_depth;
+    for (auto& b : blocks) by_depth[nodes_[b.node].depth].push_back(&b);
+    for (auto& kv : by_depth) {
+        Plan plan;
+        auto& lvl = kv.second;
+        std::vector<Block*> rs, fs;
+        for (auto* b : lvl) (b->rsvd ? rs : fs).push_back(b);
+        // ---- full SVDs (compression.h:18-64) on the tall orientation ----
+        if (!fs.empty()) {
+            auto cp = std::make_unique<CopyStep>();
+            std::vector<SvdProblem> sv;
+            for (auto* b : fs) {
+                const bool tall = b->m >= b->n;
+                const int rows = tall ? b->m : b->n, p = tall ? b->n : b->m;
+                double* X = plan.scratch((size_t)rows * p);
+                cp->t.h.push_back({dA + b->r0 + (size_t)b->c0 * lda, lda, X, rows, rows, p, tall ? 0 : 1, 0, 0});
+                Node& cr = nodes_[b->crow];
+                Node& cc = nodes_[b->ccol];
+                double* Uo = dU.p + cr.offU;
+                double* Vo = dV.p + cc.offV;
+                SvdProblem q{};
+                q.X = X; q.ldx = rows; q.rows = rows; q.k = p;
+                q.sigma = dSig.p + sig_off[b->slot];
+                q.rank = dRank.p + b->slot;
+                q.sort = true;
+                if (tall) { q.L = Uo; q.ldl = cr.len(); q.R = Vo; q.ldr = cc.len(); }
+                else { q.L = Vo; q.ldl = cc.len(); q.R = Uo; q.ldr = cr.len(); }
+                sv.push_back(q);
+            }
+            cp->t.upload(stream_);
+            plan.add(std::move(cp));
+            plan_gram_svd(plan, sv, opts_.tol, opts_.max_rank, stream_);
+        }
+        // ---- randomized SVDs (compression.h:67-99) ----
+        if (!rs.empty()) {
+            struct W { double *Y, *Q, *X, *Ub; };
+            std::vector<W> ws(rs.size());
+            auto gY = std::make_unique<GemmStep<double>>();
+            for (size_t i = 0; i < rs.size(); ++i) {
+                Block* b = rs[i];
+                ws[i].Y = plan.scratch((size_t)b->m * b->k);
+                ws[i].Q = plan.scratch((size_t)b->m * b->k);
+                ws[i].X = plan.scratch((size_t)b->n * b->k);
+                ws[i].Ub = plan.scratch((size_t)b->k * b->k);
+                // Y = A_blk Omega  (compression.h:79)
+                gY->batch.add(b->m, b->k, b->n, 1.0, dA + b->r0 + (size_t)b->c0 * lda, lda, OP_N,
+                              dOmega.p + b->omega, b->n, OP_N, 0.0, ws[i].Y, b->m);
+            }
+            gY->batch.finalize(stream_);
+            plan.add(std::move(gY));
+            auto orthY = [&]() {
+                std::vector<SvdProblem> sv;
+                for (size_t i = 0; i < rs.size(); ++i) {
+                    Block* b = rs[i];
+                    SvdProblem q{};
+                    q.X = ws[i].Y; q.ldx = b->m; q.rows = b->m; q.k = b->k;
+                    q.L = ws[i].Q; q.ldl = b->m;
+                    q.sort = false;
+                    sv.push_back(q);
+                }
+                plan_gram_svd(plan, sv, opts_.tol, 0, stream_);
+            };
+            orthY();  // Q = orthonormal basis of range(Y)  (compression.h:83-84)
+            for (int it = 0; it < opts_.power_iters; ++it) {  // extension
+                auto gZ = std::make_unique<GemmStep<double>>();
+                for (size_t i = 0; i < rs.size(); ++i) {
+                    Block* b = rs[i];
+                    gZ->batch.add(b->n, b->k, b->m, 1.0, dA + b->r0 + (size_t)b->c0 * lda, lda, OP_T,
+                                  ws[i].Q, b->m, OP_N, 0.0, ws[i].X, b->n);
+                }
+                gZ->batch.finalize(stream_);
+                plan.add(std::move(gZ));
+                std::vector<SvdProblem> sv;
+                for (size_t i = 0; i < rs.size(); ++i) {
+                    Block* b = rs[i];
+                    SvdProblem q{};
+                    q.X = ws[i].X; q.ldx = b->n; q.rows = b->n; q.k = b->k;
+                    q.L = ws[i].X; q.ldl = b->n;
+                    sv.push_back(q);
+                }
+                plan_gram_svd(plan, sv, opts_.tol, 0, stream_);
+                auto gY2 = std::make_unique<GemmStep<double>>();
+                for (size_t i = 0; i < rs.size(); ++i) {
+                    Block* b = rs[i];
+                    gY2->batch.add(b->m, b->k, b->n, 1.0, dA + b->r0 + (size_t)b->c0 * lda, lda, OP_N,
+                                   ws[i].X, b->n, OP_N, 0.0, ws[i].Y, b->m);
+                }
+                gY2->batch.finalize(stream_);
+                plan.add(std::move(gY2));
+                orthY();
+            }
+            // X = A_blk^T Q = (Q^T A_blk)^T  (compression.h:87)
+            auto gX = std::make_unique<GemmStep<double>>();
+            for (size_t i = 0; i < rs.size(); ++i) {
+                Block* b = rs[i];
+                gX->batch.add(b->n, b->k, b->m, 1.0, dA + b->r0 + (size_t)b->c0 * lda, lda, OP_T,
+                              ws[i].Q, b->m, OP_N, 0.0, ws[i].X, b->n);
+            }
+            gX->batch.finalize(stream_);
+            plan.add(std::move(gX));
+            // SVD of Q^T A (compression.h:90): X = V_b S U_b^T
+            std::vector<SvdProblem> sv;
+            for (size_t i = 0; i < rs.size(); ++i) {
+                Block* b = rs[i];
+                Node& cc = nodes_[b->ccol];
+                SvdProblem q{};
+                q.X = ws[i].X; q.ldx = b->n; q.rows = b->n; q.k = b->k;
+                q.L = dV.p + cc.offV; q.ldl = cc.len();
+                q.R = ws[i].Ub; q.ldr = b->k;
+                q.sigma = dSig.p + sig_off[b->slot];
+                q.rank = dRank.p + b->slot;
+                q.sort = true;
+                sv.push_back(q);
+            }
+            plan_gram_svd(plan, sv, opts_.tol, opts_.max_rank, stream_);
+            // U = Q U_b  (compression.h:94)
+            auto gU = std::make_unique<GemmStep<double>>();
+            for (size_t i = 0; i < rs.size(); ++i) {
+                Block* b = rs[i];
+                Node& cr = nodes_[b->crow];
+                gU->batch.add(b->m, b->k, b->k, 1.0, ws[i].Q, b->m, OP_N, ws[i].Ub, b->k, OP_N, 0.0,
+                              dU.p + cr.offU, cr.len());
+            }
+            gU->batch.finalize(stream_);
+            plan.add(std::move(gU));
+        }
+        plan.run(stream_, dstatus.p);
+        HM_CUDA(cudaStreamSynchronize(stream_));
+    }
+    check_status("build");
+    // ranks and singular values to the host; B = diag(S[:rank]) (compression.h:57-63)
+    std::vector<int> ranks(blocks.size());
+    std::vector<double> sig(sig_total);
+    HM_CUDA(cudaMemcpyAsync(ranks.data(), dRank.p, ranks.size() * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    if (sig_total)
+        HM_CUDA(cudaMemcpyAsync(sig.data(), dSig.p, sig_total * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    HM_CUDA(cudaStreamSynchronize(stream_));
+    std::vector<int> r12(nodes_.size(), 0), r21(nodes_.size(), 0);
+    std::vector<double> s12, s21;
+    size_t tot = 0;
+    for (auto& b : blocks) {
+        int r = std::min(ranks[b.slot], b.k);
+        Node& n = nodes_[b.node];
+        (b.which == 0 ? r12 : r21)[b.node] = r;
+        tot += (size_t)r * r;
+        (void)n;
+    }
+    std::vector<double> hB(std::max<size_t>(tot, 1), 0.0);
+    size_t off = 0;
+    for (auto& b : blocks) {
+        int r = std::min(ranks[b.slot], b.k);
+        Node& n = nodes_[b.node];
+        size_t o = off;
+        for (int i = 0; i < r; ++i) hB[o + i + (size_t)i * r] = sig[sig_off[b.slot] + i];
+        if (b.which == 0) {
+            n.offB12 = o;
+            nodes_[b.crow].rankU = r;   // left.U
+            nodes_[b.ccol].rankV = r;   // right.V
+        } else {
+            n.offB21 = o;
+            nodes_[b.crow].rankU = r;   // right.U
+            nodes_[b.ccol].rankV = r;   // left.V
+        }
+        off += (size_t)r * r;
+    }
+    dB.alloc(hB.size());
+    HM_CUDA(cudaMemcpyAsync(dB.p, hB.data(), hB.size() * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    HM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::build_hss(const double*, int) {
+    throw Error(HM_ERR_UNSUPPORTED, "HSS build not available in this build");
+}
+
+// ---------------------------------------------------------------------------------
+// Import reference factors
+// ---------------------------------------------------------------------------------
+void Engine::import_hodlr(int N, int leaf, const int* r12, const int* r21, const double* const* D,
+                          const double* const* U, const double* const* V, const double* const* B12,
+                          const double* const* B21) {
+    HM_CHECK(kind_ == HODLR, HM_ERR_STATE, "import is for HODLR handles");
+    HM_CHECK(N > 0 && leaf > 0 && r12 && r21 && D && U && V && B12 && B21, HM_ERR_ARG, "import: bad arguments");
+    N_ = N;
+    leaf_ = leaf;
+    built_ = factored_ = false;
+    f64_.ready = f32_.ready = false;
+    mv_plans_.clear();
+    solve64_plans_.clear();
+    solve32_plans_.clear();
+    nodes_ = hodlr_tree(N, leaf);
+    plan_levels();
+    if (!dstatus.p) dstatus.alloc(1);
+    dstatus.zero(stream_);
+    for (size_t i = 0; i < nodes_.size(); ++i) {
+        Node& n = nodes_[i];
+        if (n.is_leaf) continue;
+        HM_CHECK(r12[i] >= 0 && r21[i] >= 0, HM_ERR_ARG, "import: negative rank");
+        nodes_[n.left].capU = nodes_[n.left].rankU = r12[i];
+        nodes_[n.right].capV = nodes_[n.right].rankV = r12[i];
+        nodes_[n.right].capU = nodes_[n.right].rankU = r21[i];
+        nodes_[n.left].capV = nodes_[n.left].rankV = r21[i];
+    }
+    alloc_bases();
+    size_t tot = 0;
+    for (size_t i = 0; i < nodes_.size(); ++i) {
+        Node& n = nodes_[i];
+        if (n.is_leaf) continue;
+        n.offB12 = tot;
+        tot += (size_t)r12[i] * r12[i];
+        n.offB21 = tot;
+        tot += (size_t)r21[i] * r21[i];
+    }
+    dB.alloc(std::max<size_t>(tot, 1));
+    auto up = [&](double* dst, const double* src, size_t cnt) {
+        if (!cnt) return;
+        HM_CHECK(src, HM_ERR_ARG, "import: missing factor");
+        HM_CUDA(cudaMemcpyAsync(dst, src, cnt * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    };
+    for (size_t i = 0; i < nodes_.size(); ++i) {
+        Node& n = nodes_[i];
+        if (n.is_leaf) up(dD.p + n.offD, D[i], (size_t)n.len() * n.len());
+        else {
+            up(dB.p + n.offB12, B12[i], (size_t)r12[i] * r12[i]);
+            up(dB.p + n.offB21, B21[i], (size_t)r21[i] * r21[i]);
+        }
+        if (n.parent >= 0) {
+            up(dU.p + n.offU, U[i], (size_t)n.len() * n.rankU);
+            up(dV.p + n.offV, V[i], (size_t)n.len() * n.rankV);
+        }
+    }
+    HM_CUDA(cudaStreamSynchronize(stream_));
+    built_ = true;
+}
+
+// ---------------------------------------------------------------------------------
+// Factorization
+// ---------------------------------------------------------------------------------
+static CopyDesc flat_copy(const void* src, bool sf, void* dst, bool df, size_t n) {
+    CopyDesc c{};
+    c.src = src; c.lds = (int)n; c.dst = dst; c.ldd = (int)n;
+    c.rows = (int)n; c.cols = 1; c.trans = 0;
+    c.src_f32 = sf; c.dst_f32 = df;
+    return c;
+}
+
+template <typename T>
+void Engine::factor_t(FactorStore<T>& fs) {
+    constexpr bool F32 = std::is_same<T, float>::value;
+    cudaStream_t s = stream_;
+    dstatus.zero(s);
+    size_t offM = 0, offP = 0;
+    for (auto& n : nodes_) {
+        if (n.is_leaf) continue;
+        const Node& L = nodes_[n.left];
+        const Node& R = nodes_[n.right];
+        const int p = L.rankU + R.rankU, q = L.rankV + R.rankV;
+        n.offM = offM;
+        offM += (size_t)q * q;
+        n.offP = offP;
+        offP += (size_t)p * q;
+    }
+    size_t totU = 1, totV = 1, totD = 1;
+    for (auto& n : nodes_) {
+        if (n.parent >= 0) {
+            totU = std::max(totU, n.offU + (size_t)n.len() * n.capU);
+            totV = std::max(totV, n.offV + (size_t)n.len() * n.capV);
+        }
+        if (n.is_leaf) totD = std::max(totD, n.offD + (size_t)n.len() * n.len());
+    }
+    Plan plan;
+    if (!dDinv.p) {  // FP64 leaf inverses, shared by both precisions
+        dDinv.alloc(totD);
+        std::vector<InvProblem> inv;
+        for (int l : leaves_) {
+            const Node& n = nodes_[l];
+            inv.push_back({dD.p + n.offD, n.len(), dDinv.p + n.offD, n.len(), n.len()});
+        }
+        plan_inverse(plan, inv, s);
+    }
+    if (!dMinv.p || sizeM_ != offM) {
+        dMinv.alloc(std::max<size_t>(offM, 1));
+        sizeM_ = offM;
+    }
+    fs.Q.alloc(totU);
+    fs.P.alloc(std::max<size_t>(offP, 1));
+    sizeP_ = offP;
+    const T* Dinv;
+    const T* Vt;
+    const T* Ut;
+    DBuf<T> Utmp;
+    if constexpr (F32) {
+        fs.Dinv.alloc(totD);
+        fs.V.alloc(totV);
+        Utmp.alloc(totU);
+        auto cp = std::make_unique<CopyStep>();
+        cp->t.h.push_back(flat_copy(dDinv.p, false, fs.Dinv.p, true, totD));
+        cp->t.h.push_back(flat_copy(dV.p, false, fs.V.p, true, totV));
+        cp->t.h.push_back(flat_copy(dU.p, false, Utmp.p, true, totU));
+        cp->t.upload(s);
+        plan.add(std::move(cp));
+        Dinv = fs.Dinv.p;
+        Vt = fs.V.p;
+        Ut = Utmp.p;
+    } else {
+        Dinv = reinterpret_cast<const T*>(dDinv.p);
+        Vt = reinterpret_cast<const T*>(dV.p);
+        Ut = reinterpret_cast<const T*>(dU.p);
+    }
+    {   // Q_c[rows of leaf] = Dinv U_c[rows of leaf] for every basis block on the path
+        auto g = std::make_unique<GemmStep<T>>();
+        for (int l : leaves_) {
+            const Node& n = nodes_[l];
+            for (int c : path_of(l)) {
+                const Node& C = nodes_[c];
+                if (C.rankU == 0) continue;
+                const size_t o = C.offU + (size_t)(n.start - C.start);
+                g->batch.add(n.len(), C.rankU, n.len(), T(1), Dinv + n.offD, n.len(), OP_N, Ut + o,
+                             C.len(), OP_N, T(0), fs.Q.p + o, C.len());
+            }
+        }
+        g->batch.finalize(s);
+        plan.add(std::move(g));
+    }
+    plan.run(s, dstatus.p);
+    HM_CUDA(cudaStreamSynchronize(s));
+    check_status("factor: leaf inverses");
+
+    for (int d = (int)levels_.size() - 1; d >= 0; --d) {
+        Plan lp;
+        const auto& lvl = levels_[d];
+        auto gK = std::make_unique<GemmStep<T>>();
+        auto cvK = std::make_unique<CopyStep>();
+        auto ident = std::make_unique<IdentStep>();
+        auto gM = std::make_unique<GemmStep<double>>();
+        std::vector<InvProblem> inv;
+        auto gP = std::make_unique<GemmStep<double>>();
+        auto cvP = std::make_unique<CopyStep>();
+        auto gT = std::make_unique<GemmStep<T>>();
+        auto gD = std::make_unique<GemmStep<T>>();
+        auto gC = std::make_unique<GemmStep<T>>();
+        for (int id : lvl) {
+            const Node& n = nodes_[id];
+            const Node& L = nodes_[n.left];
+            const Node& R = nodes_[n.right];
+            const int p1 = L.rankU, p2 = R.rankU, q1 = L.rankV, q2 = R.rankV;
+            const int q = q1 + q2, p = p1 + p2;
+            const size_t kn = (size_t)q1 * p1 + (size_t)q2 * p2;
+            T* Kt;
+            double* K64;
+            if constexpr (F32) {
+                Kt = lp.scratch_f(std::max<size_t>(kn, 1));
+                K64 = lp.scratch(std::max<size_t>(kn, 1));
+                if (kn) cvK->t.h.push_back(flat_copy(Kt, true, K64, false, kn));
+            } else {
+                K64 = lp.scratch(std::max<size_t>(kn, 1));
+                Kt = K64;
+            }
+            // K1 = V1^T Q1, K2 = V2^T Q2
+            gK->batch.add(q1, p1, L.len(), T(1), Vt + L.offV, L.len(), OP_T, fs.Q.p + L.offU, L.len(),
+                          OP_N, T(0), Kt, q1);
+            gK->batch.add(q2, p2, R.len(), T(1), Vt + R.offV, R.len(), OP_T, fs.Q.p + R.offU, R.len(),
+                          OP_N, T(0), Kt + (size_t)q1 * p1, q2);
+            // M = [[I, K1 B12], [K2 B21, I]]
+            double* M = lp.scratch(std::max<size_t>((size_t)q * q, 1));
+            double* Minv = dMinv.p + n.offM;
+            if (q) ident->t.h.push_back({M, q, q, q, 1.0});
+            const double* B12 = dB.p + n.offB12;
+            const double* B21 = dB.p + n.offB21;
+            gM->batch.add(q1, q2, p1, 1.0, K64, q1, OP_N, B12, p1, OP_N, 0.0, M + (size_t)q1 * q, q);
+            gM->batch.add(q2, q1, p2, 1.0, K64 + (size_t)q1 * p1, q2, OP_N, B21, p2, OP_N, 0.0, M + q1, q);
+            if (q) inv.push_back({M, q, Minv, q, q});
+            // P = B^ Minv: P[0:p1,:] = B12 Minv[q1:,:], P[p1:,:] = B21 Minv[0:q1,:]
+            double* P64;
+            if constexpr (F32) {
+                P64 = lp.scratch(std::max<size_t>((size_t)p * q, 1));
+                if ((size_t)p * q) cvP->t.h.push_back(flat_copy(P64, false, fs.P.p + n.offP, true, (size_t)p * q));
+            } else {
+                P64 = fs.P.p + n.offP;
+            }
+            gP->batch.add(p1, q, q2, 1.0, B12, p1, OP_N, Minv + q1, q, OP_N, 0.0, P64, p);
+            gP->batch.add(p2, q, q1, 1.0, B21, p2, OP_N, Minv, q, OP_N, 0.0, P64 + p1, p);
+            // every basis block on n's path: W <- A_n^{-1} W (given blockdiag-solved W)
+            const T* Pn = fs.P.p + n.offP;
+            for (int c : path_of(id)) {
+                const Node& C = nodes_[c];
+                const int w = C.rankU;
+                if (w == 0) continue;
+                T* W = fs.Q.p + C.offU + (size_t)(n.start - C.start);
+                const int ldw = C.len();
+                T* Tt = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)q * w, 1)))
+                            : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)q * w, 1)));
+                T* Dt = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)p * w, 1)))
+                            : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)p * w, 1)));
+                gT->batch.add(q1, w, L.len(), T(1), Vt + L.offV, L.len(), OP_T, W, ldw, OP_N, T(0), Tt, q);
+                gT->batch.add(q2, w, R.len(), T(1), Vt + R.offV, R.len(), OP_T, W + L.len(), ldw, OP_N,
+                              T(0), Tt + q1, q);
+                gD->batch.add(p, w, q, T(1), Pn, p, OP_N, Tt, q, OP_N, T(0), Dt, p);
+                gC->batch.add(L.len(), w, p1, T(-1), fs.Q.p + L.offU, L.len(), OP_N, Dt, p, OP_N, T(1), W, ldw);
+                gC->batch.add(R.len(), w, p2, T(-1), fs.Q.p + R.offU, R.len(), OP_N, Dt + p1, p, OP_N,
+                              T(1), W + L.len(), ldw);
+            }
+        }
+        gK->batch.finalize(s);
+        lp.add(std::move(gK));
+        if (!cvK->t.h.empty()) { cvK->t.upload(s); lp.add(std::move(cvK)); }
+        ident->t.upload(s);
+        lp.add(std::move(ident));
+        gM->batch.finalize(s);
+        lp.add(std::move(gM));
+        plan_inverse(lp, inv, s);
+        gP->batch.finalize(s);
+        lp.add(std::move(gP));
+        if (!cvP->t.h.empty()) { cvP->t.upload(s); lp.add(std::move(cvP)); }
+        gT->batch.finalize(s);
+        lp.add(std::move(gT));
+        gD->batch.finalize(s);
+        lp.add(std::move(gD));
+        gC->batch.finalize(s);
+        lp.add(std::move(gC));
+        lp.run(s, dstatus.p);
+        HM_CUDA(cudaStreamSynchronize(s));
+        check_status("factor: capacitance");
+    }
+    fs.ready = true;
+}
+
+void Engine::factor() {
+    HM_CHECK(built_, HM_ERR_STATE, "factor before build");
+    if (!f64_.ready) factor_t<double>(f64_);
+    if (opts_.precision == HM_MIXED && !f32_.ready) factor_t<float>(f32_);
+    factored_ = true;
+}
+
+// ---------------------------------------------------------------------------------
+// Solve and multiply plans on the staging buffers (ld = N)
+// ---------------------------------------------------------------------------------
+void Engine::ensure_io(int s) {
+    if (s <= io_cols_) return;
+    const size_t n = (size_t)N_ * s;
+    ioX.alloc(n);
+    ioY.alloc(n);
+    ioR.alloc(n);
+    ioXf.alloc(n);
+    ioYf.alloc(n);
+    io_cols_ = s;
+    mv_plans_.clear();
+    solve64_plans_.clear();
+    solve32_plans_.clear();
+}
+
+// y = A x for s columns: in = x (ld N), out = y (ld N)
+static void add_matvec(Plan& pl, const std::vector<Node>& nodes, const std::vector<int>& leaves,
+                       const std::vector<std::vector<int>>& levels, const double* dD, const double* dU,
+                       const double* dV, const double* dB, const double* X, double* Y, int N, int s,
+                       cudaStream_t st) {
+    auto gLeaf = std::make_unique<GemmStep<double>>();
+    for (int l : leaves) {
+        const Node& n = nodes[l];
+        gLeaf->batch.add(n.len(), s, n.len(), 1.0, dD + n.offD, n.len(), OP_N, X + n.start, N, OP_N,
+                         0.0, Y + n.start, N);
+    }
+    auto gT = std::make_unique<GemmStep<double>>();
+    auto gD = std::make_unique<GemmStep<double>>();
+    std::vector<std::unique_ptr<GemmStep<double>>> gE(levels.size());
+    for (size_t d = 0; d < levels.size(); ++d) gE[d] = std::make_unique<GemmStep<double>>();
+    for (size_t d = 0; d < levels.size(); ++d) {
+        for (int id : levels[d]) {
+            const Node& n = nodes[id];
+            const Node& L = nodes[n.left];
+            const Node& R = nodes[n.right];
+            const int p1 = L.rankU, p2 = R.rankU, q1 = L.rankV, q2 = R.rankV;
+            double* T = pl.scratch(std::max<size_t>((size_t)(q1 + q2) * s, 1));
+            double* Dl = pl.scratch(std::max<size_t>((size_t)(p1 + p2) * s, 1));
+            // T1 = V1^T x1, T2 = V2^T x2
+            gT->batch.add(q1, s, L.len(), 1.0, dV + L.offV, L.len(), OP_T, X + L.start, N, OP_N, 0.0, T, q1 + q2);
+            gT->batch.add(q2, s, R.len(), 1.0, dV + R.offV, R.len(), OP_T, X + R.start, N, OP_N, 0.0,
+                          T + q1, q1 + q2);
+            // delta1 = B12 T2, delta2 = B21 T1
+            gD->batch.add(p1, s, q2, 1.0, dB + n.offB12, p1, OP_N, T + q1, q1 + q2, OP_N, 0.0, Dl, p1 + p2);
+            gD->batch.add(p2, s, q1, 1.0, dB + n.offB21, p2, OP_N, T, q1 + q2, OP_N, 0.0, Dl + p1, p1 + p2);
+            // y1 += U1 delta1, y2 += U2 delta2
+            gE[d]->batch.add(L.len(), s, p1, 1.0, dU + L.offU, L.len(), OP_N, Dl, p1 + p2, OP_N, 1.0,
+                             Y + L.start, N);
+            gE[d]->batch.add(R.len(), s, p2, 1.0, dU + R.offU, R.len(), OP_N, Dl + p1, p1 + p2, OP_N, 1.0,
+                             Y + R.start, N);
+        }
+    }
+    gLeaf->batch.finalize(st);
+    pl.add(std::move(gLeaf));
+    gT->batch.finalize(st);
+    pl.add(std::move(gT));
+    gD->batch.finalize(st);
+    pl.add(std::move(gD));
+    for (auto& g : gE) {
+        g->batch.finalize(st);
+        pl.add(std::move(g));
+    }
+}
+
+Plan& Engine::matvec_plan(int s) {
+    auto it = mv_plans_.find(s);
+    if (it != mv_plans_.end()) return it->second;
+    Plan& pl = mv_plans_[s];
+    add_matvec(pl, nodes_, leaves_, levels_, dD.p, dU.p, dV.p, dB.p, ioX.p, ioY.p, N_, s, stream_);
+    return pl;
+}
+
+// z = A^{-1} x in precision T: in = X (ld N), out = Z (ld N)
+template <typename T>
+static void add_solve(Plan& pl, const std::vector<Node>& nodes, const std::vector<int>& leaves,
+                      const std::vector<std::vector<int>>& levels, const T* Dinv, const T* Vt,
+                      const T* Q, const T* P, const T* X, T* Z, int N, int s, cudaStream_t st) {
+    constexpr bool F32 = std::is_same<T, float>::value;
+    auto gLeaf = std::make_unique<GemmStep<T>>();
+    for (int l : leaves) {
+        const Node& n = nodes[l];
+        gLeaf->batch.add(n.len(), s, n.len(), T(1), Dinv + n.offD, n.len(), OP_N, X + n.start, N, OP_N,
+                         T(0), Z + n.start, N);
+    }
+    gLeaf->batch.finalize(st);
+    pl.add(std::move(gLeaf));
+    for (int d = (int)levels.size() - 1; d >= 0; --d) {
+        auto gT = std::make_unique<GemmStep<T>>();
+        auto gD = std::make_unique<GemmStep<T>>();
+        auto gC = std::make_unique<GemmStep<T>>();
+        for (int id : levels[d]) {
+            const Node& n = nodes[id];
+            const Node& L = nodes[n.left];
+            const Node& R = nodes[n.right];
+            const int p1 = L.rankU, p2 = R.rankU, q1 = L.rankV, q2 = R.rankV;
+            const int p = p1 + p2, q = q1 + q2;
+            T* Tt = F32 ? reinterpret_cast<T*>(pl.scratch_f(std::max<size_t>((size_t)q * s, 1)))
+                        : reinterpret_cast<T*>(pl.scratch(std::max<size_t>((size_t)q * s, 1)));
+            T* Dt = F32 ? reinterpret_cast<T*>(pl.scratch_f(std::max<size_t>((size_t)p * s, 1)))
+                        : reinterpret_cast<T*>(pl.scratch(std::max<size_t>((size_t)p * s, 1)));
+            gT->batch.add(q1, s, L.len(), T(1), Vt + L.offV, L.len(), OP_T, Z + L.start, N, OP_N, T(0), Tt, q);
+            gT->batch.add(q2, s, R.len(), T(1), Vt + R.offV, R.len(), OP_T, Z + R.start, N, OP_N, T(0),
+                          Tt + q1, q);
+            gD->batch.add(p, s, q, T(1), P + n.offP, p, OP_N, Tt, q, OP_N, T(0), Dt, p);
+            gC->batch.add(L.len(), s, p1, T(-1), Q + L.offU, L.len(), OP_N, Dt, p, OP_N, T(1), Z + L.start, N);
+            gC->batch.add(R.len(), s, p2, T(-1), Q + R.offU, R.len(), OP_N, Dt + p1, p, OP_N, T(1),
+                          Z + R.start, N);
+        }
+        gT->batch.finalize(st);
+        pl.add(std::move(gT));
+        gD->batch.finalize(st);
+        pl.add(std::move(gD));
+        gC->batch.finalize(st);
+        pl.add(std::move(gC));
+    }
+}
+
+template <>
+Plan& Engine::solve_plan<double>(FactorStore<double>& fs, int s) {
+    auto it = solve64_plans_.find(s);
+    if (it != solve64_plans_.end()) return it->second;
+    Plan& pl = solve64_plans_[s];
+    add_solve<double>(pl, nodes_, leaves_, levels_, dDinv.p, dV.p, fs.Q.p, fs.P.p, ioX.p, ioY.p, N_, s,
+                      stream_);
+    return pl;
+}
+
+template <>
+Plan& Engine::solve_plan<float>(FactorStore<float>& fs, int s) {
+    auto it = solve32_plans_.find(s);
+    if (it != solve32_plans_.end()) return it->second;
+    Plan& pl = solve32_plans_[s];
+    add_solve<float>(pl, nodes_, leaves_, levels_, fs.Dinv.p, fs.V.p, fs.Q.p, fs.P.p, ioXf.p, ioYf.p,
+                     N_, s, stream_);
+    return pl;
+}
+
+static void copy_in(double* dst, const double* src, int N, int s, int ld, cudaStream_t st) {
+    HM_CUDA(cudaMemcpy2DAsync(dst, (size_t)N * sizeof(double), src, (size_t)ld * sizeof(double),
+                              (size_t)N * sizeof(double), s, cudaMemcpyDeviceToDevice, st));
+}
+
+void Engine::multiply_device(const double* dx, int s, int ldx, double* dy, int ldy) {
+    HM_CHECK(built_, HM_ERR_STATE, "multiply before build");
+    HM_CHECK(s >= 1 && ldx >= N_ && ldy >= N_ && dx && dy, HM_ERR_ARG, "multiply: bad arguments");
+    ensure_io(s);
+    copy_in(ioX.p, dx, N_, s, ldx, stream_);
+    matvec_plan(s).run(stream_, dstatus.p);
+    HM_CUDA(cudaMemcpy2DAsync(dy, (size_t)ldy * sizeof(double), ioY.p, (size_t)N_ * sizeof(double),
+                              (size_t)N_ * sizeof(double), s, cudaMemcpyDeviceToDevice, stream_));
+}
+
+void Engine::solve_fp64(const double* db, int s, int ldb, double* dx, int ldx) {
+    ensure_io(s);
+    copy_in(ioX.p, db, N_, s, ldb, stream_);
+    solve_plan<double>(f64_, s).run(stream_, dstatus.p);
+    HM_CUDA(cudaMemcpy2DAsync(dx, (size_t)ldx * sizeof(double), ioY.p, (size_t)N_ * sizeof(double),
+                              (size_t)N_ * sizeof(double), s, cudaMemcpyDeviceToDevice, stream_));
+}
+
+// Mixed precision: FP32 factor sweeps, refined against the FP64 operator
+// (x += A32^{-1} r, r = b - A64 x) until max_j ||r_j|| / ||b_j|| <= ir_tol.
+void Engine::solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st) {
+    ensure_io(s);
+    cudaStream_t q = stream_;
+    // ioR holds b, ioY x, ioX the matvec input (x), ioYf the correction.
+    DBuf<double> norms(2 * (size_t)s);
+    DBuf<double> bcopy((size_t)N_ * s);
+    copy_in(bcopy.p, db, N_, s, ldb, q);
+    to_float_kernel<<<grid_for((size_t)N_ * s), 256, 0, q>>>(bcopy.p, ioXf.p, (size_t)N_ * s);
+    Plan& sp = solve_plan<float>(f32_, s);
+    Plan& mp = matvec_plan(s);
+    std::vector<double> hn(2 * (size_t)s);
+    double worst = 0.0;
+    int it = 0;
+    for (; it < std::max(1, opts_.ir_max_iter); ++it) {
+        sp.run(q, dstatus.p);                                   // ioYf = A32^{-1} r
+        accumulate_kernel<<<grid_for((size_t)N_ * s), 256, 0, q>>>(ioX.p, ioYf.p, (size_t)N_ * s, it == 0);
+        mp.run(q, dstatus.p);                                   // ioY = A64 x
+        norms.zero(q);
+        residual_kernel<<<dim3(std::min(64, ceil_div(N_, 256)), s), 256, 0, q>>>(
+            bcopy.p, ioY.p, ioXf.p, N_, s, norms.p, norms.p + s);  // ioY = b - A x, ioXf = float(r)
+        HM_CUDA(cudaMemcpyAsync(hn.data(), norms.p, 2 * s * sizeof(double), cudaMemcpyDeviceToHost, q));
+        HM_CUDA(cudaStreamSynchronize(q));
+        worst = 0.0;
+        for (int j = 0; j < s; ++j) {
+            double den = std::sqrt(hn[s + j]);
+            double rel = den > 0 ? std::sqrt(hn[j]) / den : std::sqrt(hn[j]);
+            worst = std::max(worst, rel);
+        }
+        if (!(worst == worst)) break;  // NaN
+        if (worst <= opts_.ir_tol) { ++it; break; }
+    }
+    HM_CUDA(cudaMemcpy2DAsync(dx, (size_t)ldx * sizeof(double), ioX.p, (size_t)N_ * sizeof(double),
+                              (size_t)N_ * sizeof(double), s, cudaMemcpyDeviceToDevice, q));
+    HM_CUDA(cudaStreamSynchronize(q));
+    if (st) {
+        st->ir_iters = it;
+        st->rel_residual = worst;
+    }
+    if (!(worst <= opts_.ir_tol))
+        throw Error(HM_ERR_IR, "iterative refinement stopped at relative residual " + std::to_string(worst));
+}
+
+void Engine::solve_device(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st) {
+    HM_CHECK(built_, HM_ERR_STATE, "solve before build");
+    HM_CHECK(s >= 1 && ldb >= N_ && ldx >= N_ && db && dx, HM_ERR_ARG, "solve: bad arguments");
+    if (!factored_) factor();
+    if (st) { st->ir_iters = 0; st->rel_residual = -1.0; }
+    if (opts_.precision == HM_MIXED) solve_mixed(db, s, ldb, dx, ldx, st);
+    else solve_fp64(db, s, ldb, dx, ldx);
+}
+
+// ---------------------------------------------------------------------------------
+// Introspection
+// ---------------------------------------------------------------------------------
+void Engine::export_tree(int* start, int* end, int* is_leaf, int* depth, int* r12, int* r21) const {
+    for (size_t i = 0; i < nodes_.size(); ++i) {
+        const Node& n = nodes_[i];
+        if (start) start[i] = n.start;
+        if (end) end[i] = n.end;
+        if (is_leaf) is_leaf[i] = n.is_leaf;
+        if (depth) depth[i] = n.depth;
+        int a = 0, b = 0;
+        if (!n.is_leaf) {
+            if (kind_ == HODLR) { a = nodes_[n.left].rankU; b = nodes_[n.right].rankU; }
+        }
+        if (r12) r12[i] = a;
+        if (r21) r21[i] = b;
+    }
+}
+
+void Engine::get_factor(int node, int which, double* out, int* rows, int* cols) const {
+    HM_CHECK(built_, HM_ERR_STATE, "get_factor before build");
+    HM_CHECK(node >= 0 && node < (int)nodes_.size(), HM_ERR_ARG, "get_factor: bad node");
+    const Node& n = nodes_[node];
+    const double* src = nullptr;
+    int r = 0, c = 0, ld = 0;
+    switch (which) {
+        case 0: if (n.is_leaf) { src = dD.p + n.offD; r = c = ld = n.len(); } break;
+        case 1: if (n.parent >= 0) { src = dU.p + n.offU; r = ld = n.len(); c = n.rankU; } break;
+        case 2: if (n.parent >= 0) { src = dV.p + n.offV; r = ld = n.len(); c = n.rankV; } break;
+        case 3: if (!n.is_leaf) { src = dB.p + n.offB12; r = ld = nodes_[n.left].rankU; c = nodes_[n.right].rankV; } break;
+        case 4: if (!n.is_leaf) { src = dB.p + n.offB21; r = ld = nodes_[n.right].rankU; c = nodes_[n.left].rankV; } break;
+        default: throw Error(HM_ERR_ARG, "get_factor: bad selector");
+    }
+    if (rows) *rows = r;
+    if (cols) *cols = c;
+    if (out && r * c > 0) {
+        HM_CUDA(cudaMemcpy2D(out, (size_t)r * sizeof(double), src, (size_t)ld * sizeof(double),
+                             (size_t)r * sizeof(double), c, cudaMemcpyDeviceToHost));
+    }
+}
+
+template void Engine::factor_t<double>(FactorStore<double>&);
+template void Engine::factor_t<float>(FactorStore<float>&);
+
+}  // namespace hm

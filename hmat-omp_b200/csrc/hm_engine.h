@@ -1,0 +1,115 @@
+// Host-side engine: tree planning, device storage of the factors, and the recorded
+// level-synchronous launch sequences (build, factor, solve, multiply).
+#pragma once
+
+#include <map>
+#include <memory>
+
+#include "hm_dense.h"
+
+namespace hm {
+
+// One tree node.  HODLR nodes are kept in pre-order (root, left subtree, right
+// subtree: the recursion order of hodlr_routines.h:27-45); HSS nodes in build_topo id
+// order (hss_routines.h:293-306).
+struct Node {
+    int start = 0, end = 0, depth = 0;
+    int is_leaf = 0;
+    int left = -1, right = -1, parent = -1;
+    int len() const { return end - start; }
+    int mid() const { return (start + end) / 2; }
+    // Basis blocks owned by a non-root node (rows of this node):
+    //   U: len x rankU (HODLR: from the parent's block with this node as row side)
+    //   V: len x rankV
+    size_t offU = 0, offV = 0;
+    int capU = 0, capV = 0;
+    int rankU = 0, rankV = 0;
+    // Leaf: D (len x len).  Internal: dense B12 (p1 x q2), B21 (p2 x q1).
+    size_t offD = 0;
+    size_t offB12 = 0, offB21 = 0;
+    // factor storage (internal): Minv ((q1+q2)^2, FP64) and P ((p1+p2) x (q1+q2))
+    size_t offM = 0, offP = 0;
+};
+
+std::vector<Node> hodlr_tree(int N, int leaf);
+std::vector<Node> hss_tree(int N, int leaf);
+
+// Per-precision factorization storage.
+template <typename T>
+struct FactorStore {
+    DBuf<T> Q;      // like U: A_child^{-1} U_child
+    DBuf<T> V;      // V in precision T (FP64: unused, the FP64 V is used)
+    DBuf<T> P;      // B^ Minv per internal node
+    DBuf<T> Dinv;   // leaf inverses in precision T (FP64: unused)
+    bool ready = false;
+};
+
+class Engine {
+  public:
+    enum Kind { HODLR = 0, HSS = 1 };
+    Engine(const hm_opts& o, Kind kind) : opts_(o), kind_(kind) {}
+    virtual ~Engine() = default;
+
+    Kind kind() const { return kind_; }
+    int N() const { return N_; }
+    const std::vector<Node>& nodes() const { return nodes_; }
+
+    void set_stream(cudaStream_t s) { stream_ = s; }
+    cudaStream_t stream() const { return stream_; }
+
+    // builds
+    void build_dense_device(const double* dA, int N, int lda, int leaf);
+    void import_hodlr(int N, int leaf, const int* r12, const int* r21, const double* const* D,
+                      const double* const* U, const double* const* V, const double* const* B12,
+                      const double* const* B21);
+    // operations on device buffers
+    void multiply_device(const double* dx, int s, int ldx, double* dy, int ldy);
+    void factor();
+    void solve_device(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st);
+
+    // introspection
+    void export_tree(int* start, int* end, int* is_leaf, int* depth, int* r12, int* r21) const;
+    void get_factor(int node, int which, double* out, int* rows, int* cols) const;
+
+  protected:
+    void plan_levels();
+    void alloc_bases();
+    void build_hodlr(const double* dA, int lda);
+    void build_hss(const double* dA, int lda);
+    void finish_build_hodlr(const std::vector<int>& rank12, const std::vector<int>& rank21,
+                            const std::vector<double>& sig12, const std::vector<double>& sig21,
+                            const std::vector<size_t>& sig_off);
+    void check_status(const char* what);
+    template <typename T> void factor_t(FactorStore<T>& fs);
+    template <typename T> Plan& solve_plan(FactorStore<T>& fs, int s);
+    Plan& matvec_plan(int s);
+    void ensure_io(int s);
+    std::vector<int> path_of(int n) const;   // n and its ancestors below the root
+    void solve_fp64(const double* db, int s, int ldb, double* dx, int ldx);
+    void solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st);
+
+    hm_opts opts_;
+    Kind kind_;
+    cudaStream_t stream_ = nullptr;
+    int N_ = 0, leaf_ = 0;
+    std::vector<Node> nodes_;
+    std::vector<std::vector<int>> levels_;   // internal nodes by depth
+    std::vector<int> leaves_;
+    // FP64 operator storage
+    DBuf<double> dD, dU, dV, dB;
+    DBuf<int> dstatus;
+    bool built_ = false;
+    // factorizations
+    FactorStore<double> f64_;
+    FactorStore<float> f32_;
+    DBuf<double> dDinv, dMinv;    // FP64 leaf and capacitance inverses
+    size_t sizeM_ = 0, sizeP_ = 0;
+    bool factored_ = false;
+    // I/O staging buffers (ld = N)
+    DBuf<double> ioX, ioY, ioR;
+    DBuf<float> ioXf, ioYf;
+    int io_cols_ = 0;
+    std::map<int, Plan> mv_plans_, solve64_plans_, solve32_plans_;
+};
+
+}  // namespace hm

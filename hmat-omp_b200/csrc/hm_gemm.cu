@@ -1,0 +1,312 @@
+// Batched variable-size GEMM for sm_100a (FP64 DFMA / FP32 FFMA register tiles).
+//
+// One CTA computes one BM x BN output tile of one problem over one k-slice.  The
+// problem is found by binary search of the tile prefix sums in the descriptor table.
+// Operand tiles are staged through double-buffered shared memory with a register
+// prefetch of the next k-tile; each thread owns a TM x TN block of the tile strided by
+// the thread grid so that shared-memory reads and global stores are conflict-free and
+// coalesced along the column-major row index.
+#include "hm_gemm.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace hm {
+
+// ---------------------------------------------------------------------------------
+// Matrix-free operator entries (FP64 math; the FP32 engine rounds the result).
+// ---------------------------------------------------------------------------------
+template <int GEN>
+__device__ __forceinline__ double gen_entry(const GenParams& g, int r, int c) {
+    if constexpr (GEN == GEN_CAUCHY) {
+        double x = g.pts[r], y = g.pts[g.N + c];
+        double v = 1.0 / (x - y);
+        return r == c ? v + g.p0 : v;
+    } else if constexpr (GEN == GEN_GAUSSIAN) {
+        double d2 = 0.0;
+        for (int t = 0; t < g.dim; ++t) {
+            double d = g.pts[(size_t)r * g.dim + t] - g.pts[(size_t)c * g.dim + t];
+            d2 += d * d;
+        }
+        double v = exp(-d2 / (2.0 * g.p0 * g.p0));
+        return r == c ? v + g.p1 : v;
+    } else if constexpr (GEN == GEN_COULOMB) {
+        double d2 = 0.0;
+        for (int t = 0; t < g.dim; ++t) {
+            double d = g.pts[(size_t)r * g.dim + t] - g.pts[(size_t)c * g.dim + t];
+            d2 += d * d;
+        }
+        double v = 1.0 / (sqrt(d2) + g.p0);
+        return r == c ? v + g.p1 : v;
+    } else {
+        return 0.0;
+    }
+}
+
+template <typename T, int BM, int BN, int BK, int TM, int TN, int GEN>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+gemm_batched_kernel(const GemmDesc<T>* __restrict__ descs, int ndesc, GenParams gp) {
+    constexpr int NT = (BM / TM) * (BN / TN);
+    constexpr int TX = BM / TM;
+    constexpr int TY = BN / TN;
+    constexpr int LA = BM * BK / NT;
+    constexpr int LB = BN * BK / NT;
+    static_assert(BM * BK % NT == 0 && BN * BK % NT == 0, "tile/threads mismatch");
+    __shared__ __align__(16) T As[2][BK][BM + 1];
+    __shared__ __align__(16) T Bs[2][BK][BN + 1];
+
+    const int tile = blockIdx.x;
+    int lo = 0, hi = ndesc - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
+    }
+    const GemmDesc<T>& D = descs[lo];
+    const int m = D.m, n = D.n, k = D.k;
+    const int lda = D.lda, ldb = D.ldb;
+    const int opA = D.opA, opB = D.opB;
+    const T* __restrict__ A = D.A;
+    const T* __restrict__ B = D.B;
+    const T* __restrict__ ks = D.kscale;
+    int t = tile - D.tile0;
+    const int tm = t % D.tiles_m;
+    t /= D.tiles_m;
+    const int tn = t % D.tiles_n;
+    const int kslice = t / D.tiles_n;
+    const int m0 = tm * BM, n0 = tn * BN;
+    int kper = (k + D.ksplit - 1) / D.ksplit;
+    kper = (kper + BK - 1) / BK * BK;
+    const int kb = kslice * kper;
+    const int ke = min(k, kb + kper);
+
+    const int tid = threadIdx.x;
+    const int tx = tid % TX, ty = tid / TX;
+
+    T acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+
+    T ra[LA], rb[LB];
+
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < LA; ++q) {
+            int e = tid + NT * q;
+            int i, kk;
+            if (opA == OP_N) { i = e % BM; kk = e / BM; } else { i = e / BK; kk = e % BK; }
+            int gi = m0 + i, gk = k0 + kk;
+            T v = T(0);
+            if (gi < m && gk < ke) {
+                if constexpr (GEN == GEN_DENSE) {
+                    v = opA == OP_N ? A[gi + (size_t)gk * lda] : A[gk + (size_t)gi * lda];
+                } else {
+                    v = opA == OP_N ? (T)gen_entry<GEN>(gp, D.ga_r0 + gi, D.ga_c0 + gk)
+                                    : (T)gen_entry<GEN>(gp, D.ga_r0 + gk, D.ga_c0 + gi);
+                }
+            }
+            ra[q] = v;
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            int e = tid + NT * q;
+            int j, kk;
+            if (opB == OP_N) { kk = e % BK; j = e / BK; } else { j = e % BN; kk = e / BN; }
+            int gj = n0 + j, gk = k0 + kk;
+            T v = T(0);
+            if (gj < n && gk < ke) {
+                v = opB == OP_N ? B[gk + (size_t)gj * ldb] : B[gj + (size_t)gk * ldb];
+                if (ks) v *= ks[gk];
+            }
+            rb[q] = v;
+        }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < LA; ++q) {
+            int e = tid + NT * q;
+            int i, kk;
+            if (opA == OP_N) { i = e % BM; kk = e / BM; } else { i = e / BK; kk = e % BK; }
+            As[buf][kk][i] = ra[q];
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            int e = tid + NT * q;
+            int j, kk;
+            if (opB == OP_N) { kk = e % BK; j = e / BK; } else { j = e % BN; kk = e / BN; }
+            Bs[buf][kk][j] = rb[q];
+        }
+    };
+
+    const int nk = (ke - kb + BK - 1) / BK;
+    if (nk > 0) {
+        load(kb);
+        store(0);
+        __syncthreads();
+        for (int it = 0; it < nk; ++it) {
+            const int buf = it & 1;
+            if (it + 1 < nk) load(kb + (it + 1) * BK);
+#pragma unroll
+            for (int kk = 0; kk < BK; ++kk) {
+                T a[TM], b[TN];
+#pragma unroll
+                for (int i = 0; i < TM; ++i) a[i] = As[buf][kk][tx + TX * i];
+#pragma unroll
+                for (int j = 0; j < TN; ++j) b[j] = Bs[buf][kk][ty + TY * j];
+#pragma unroll
+                for (int i = 0; i < TM; ++i)
+#pragma unroll
+                    for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            }
+            if (it + 1 < nk) store(buf ^ 1);
+            __syncthreads();
+        }
+    }
+
+    T* __restrict__ C = D.C;
+    const int ldc = D.ldc;
+    const T alpha = D.alpha, beta = D.beta;
+    const bool split = D.ksplit > 1;
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+        int gi = m0 + tx + TX * i;
+        if (gi >= m) continue;
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+            int gj = n0 + ty + TY * j;
+            if (gj >= n) continue;
+            T v = alpha * acc[i][j];
+            T* c = C + gi + (size_t)gj * ldc;
+            if (split) atomicAdd(c, v);
+            else *c = (beta == T(0)) ? v : fma(beta, *c, v);
+        }
+    }
+}
+
+template <typename T>
+__global__ void zero_regions_kernel(const ZeroRegion<T>* __restrict__ z, int count) {
+    // one block per region, block-stride inside
+    int r = blockIdx.x;
+    if (r >= count) return;
+    ZeroRegion<T> q = z[r];
+    size_t total = (size_t)q.m * q.n;
+    for (size_t e = threadIdx.x; e < total; e += blockDim.x) {
+        int i = (int)(e % q.m), j = (int)(e / q.m);
+        q.C[i + (size_t)j * q.ldc] = T(0);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------------
+struct CfgShape { int BM, BN, BK; };
+static CfgShape cfg_shape(int cfg) {
+    switch (cfg) {
+        case CFG_N_SKINNY: return {128, 16, 16};
+        default: return {64, 64, 16};
+    }
+}
+
+template <typename T>
+void GemmBatch<T>::add(int m, int n, int k, T alpha, const T* A, int lda, int opA, const T* B,
+                       int ldb, int opB, T beta, T* C, int ldc, const T* kscale, int ksplit,
+                       int ga_r0, int ga_c0) {
+    if (m <= 0 || n <= 0) return;
+    HM_CHECK(!finalized_, HM_ERR_STATE, "GemmBatch::add after finalize");
+    CfgShape cs = cfg_shape(cfg_);
+    GemmDesc<T> d{};
+    d.A = A; d.B = B; d.C = C; d.kscale = kscale;
+    d.alpha = alpha; d.beta = beta;
+    d.m = m; d.n = n; d.k = std::max(k, 0);
+    d.lda = lda; d.ldb = ldb; d.ldc = ldc;
+    d.opA = opA; d.opB = opB;
+    d.tiles_m = ceil_div(m, cs.BM);
+    d.tiles_n = ceil_div(n, cs.BN);
+    d.ga_r0 = ga_r0; d.ga_c0 = ga_c0;
+    if (ksplit <= 0) {
+        int tiles = d.tiles_m * d.tiles_n;
+        ksplit = 1;
+        if (tiles < 32 && k >= 512) ksplit = std::min(std::max(1, k / 256), std::max(1, 128 / tiles));
+    }
+    ksplit = std::max(1, std::min(ksplit, std::max(1, ceil_div(std::max(k, 1), cs.BK))));
+    if (ksplit > 1 && beta != T(0)) {
+        HM_CHECK(beta == T(1), HM_ERR_ARG, "split-K GEMM needs beta 0 or 1");
+    }
+    d.ksplit = ksplit;
+    if (ksplit > 1 && beta == T(0)) hz_.push_back({C, m, n, ldc});
+    if (k <= 0 && beta == T(0)) {
+        // empty product: C = 0
+        d.ksplit = 1;
+    }
+    h_.push_back(d);
+}
+
+template <typename T>
+void GemmBatch<T>::finalize(cudaStream_t s) {
+    int t = 0;
+    for (auto& d : h_) {
+        d.tile0 = t;
+        t += d.tiles_m * d.tiles_n * d.ksplit;
+    }
+    total_tiles_ = t;
+    if (!h_.empty()) {
+        d_.alloc(h_.size());
+        HM_CUDA(cudaMemcpyAsync(d_.p, h_.data(), h_.size() * sizeof(GemmDesc<T>),
+                                cudaMemcpyHostToDevice, s));
+    }
+    if (!hz_.empty()) {
+        dz_.alloc(hz_.size());
+        HM_CUDA(cudaMemcpyAsync(dz_.p, hz_.data(), hz_.size() * sizeof(ZeroRegion<T>),
+                                cudaMemcpyHostToDevice, s));
+    }
+    // the host vectors must outlive the async copies: keep them
+    finalized_ = true;
+}
+
+template <typename T>
+void GemmBatch<T>::clear() {
+    h_.clear();
+    hz_.clear();
+    d_.release();
+    dz_.release();
+    total_tiles_ = 0;
+    finalized_ = false;
+}
+
+template <typename T, int BM, int BN, int BK, int TM, int TN>
+static void launch_gen(int gen, int grid, cudaStream_t s, const GemmDesc<T>* d, int nd,
+                       const GenParams& gp) {
+    constexpr int NT = (BM / TM) * (BN / TN);
+    switch (gen) {
+        case GEN_CAUCHY:
+            gemm_batched_kernel<T, BM, BN, BK, TM, TN, GEN_CAUCHY><<<grid, NT, 0, s>>>(d, nd, gp);
+            break;
+        case GEN_GAUSSIAN:
+            gemm_batched_kernel<T, BM, BN, BK, TM, TN, GEN_GAUSSIAN><<<grid, NT, 0, s>>>(d, nd, gp);
+            break;
+        case GEN_COULOMB:
+            gemm_batched_kernel<T, BM, BN, BK, TM, TN, GEN_COULOMB><<<grid, NT, 0, s>>>(d, nd, gp);
+            break;
+        default:
+            gemm_batched_kernel<T, BM, BN, BK, TM, TN, GEN_DENSE><<<grid, NT, 0, s>>>(d, nd, gp);
+    }
+}
+
+template <typename T>
+void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp) const {
+    if (h_.empty()) return;
+    HM_CHECK(finalized_, HM_ERR_STATE, "GemmBatch::launch before finalize");
+    if (!hz_.empty())
+        zero_regions_kernel<T><<<(int)hz_.size(), 256, 0, s>>>(dz_.p, (int)hz_.size());
+    if (cfg_ == CFG_N_SKINNY)
+        launch_gen<T, 128, 16, 16, 4, 2>(gen_, total_tiles_, s, d_.p, (int)h_.size(), gp);
+    else
+        launch_gen<T, 64, 64, 16, 4, 4>(gen_, total_tiles_, s, d_.p, (int)h_.size(), gp);
+    HM_CUDA(cudaGetLastError());
+}
+
+template class GemmBatch<double>;
+template class GemmBatch<float>;
+
+}  // namespace hm

@@ -1,0 +1,81 @@
+// Variable-size batched GEMM: every node of a tree level (and every system of a
+// batch) is one problem in a descriptor table; one launch covers the whole table.
+//
+//   C = alpha * op(A) * diag(kscale) * op(B) + beta * C
+//
+// op(X) is X or X^T of a column-major block with an explicit leading dimension.
+// A may instead be generated on the fly from point coordinates (matrix-free kernel
+// blocks).  Problems whose k is long and whose output is small are split along k
+// ("split-K"); their partial products are added with atomics, so C must already
+// hold beta*C (the batch zeroes C first when beta == 0).
+#pragma once
+
+#include "hm_common.h"
+
+namespace hm {
+
+enum : int { OP_N = 0, OP_T = 1 };
+
+// Matrix-free A source.  Element (r, c) of the global N x N operator.
+enum : int { GEN_DENSE = 0, GEN_CAUCHY = 1, GEN_GAUSSIAN = 2, GEN_COULOMB = 3 };
+
+struct GenParams {
+    const double* pts = nullptr;  // GEN_CAUCHY: x = pts[0:N], y = pts[N:2N]; else N x dim, point-major
+    int N = 0;
+    int dim = 1;
+    double p0 = 0, p1 = 0;        // kernel parameters (see hmat_b200.h HM_KERNEL_*)
+};
+
+template <typename T>
+struct ZeroRegion {
+    T* C;
+    int m, n, ldc;
+};
+
+template <typename T>
+struct GemmDesc {
+    const T* A;
+    const T* B;
+    T* C;
+    const T* kscale;   // optional, length k
+    T alpha, beta;
+    int m, n, k;
+    int lda, ldb, ldc;
+    int opA, opB;
+    int ksplit;
+    int tiles_m, tiles_n;
+    int tile0;         // first global tile index of this problem
+    int ga_r0, ga_c0;  // generated A: origin of the block in the global operator
+};
+
+// Tile configurations.
+enum : int { CFG_64x64 = 0, CFG_N_SKINNY = 1 };
+
+template <typename T>
+class GemmBatch {
+  public:
+    explicit GemmBatch(int cfg = CFG_64x64, int gen = GEN_DENSE) : cfg_(cfg), gen_(gen) {}
+    // Add C = alpha op(A) diag(kscale) op(B) + beta C.  ksplit <= 0 picks a split.
+    void add(int m, int n, int k, T alpha, const T* A, int lda, int opA, const T* B, int ldb,
+             int opB, T beta, T* C, int ldc, const T* kscale = nullptr, int ksplit = 0,
+             int ga_r0 = 0, int ga_c0 = 0);
+    bool empty() const { return h_.empty(); }
+    size_t size() const { return h_.size(); }
+    // Upload the table (once); later launches reuse it (and may be graph-captured).
+    void finalize(cudaStream_t s);
+    void launch(cudaStream_t s, const GenParams& gp = GenParams()) const;
+    void clear();
+    int cfg() const { return cfg_; }
+
+  private:
+    int cfg_, gen_;
+    std::vector<GemmDesc<T>> h_;
+    DBuf<GemmDesc<T>> d_;
+    // regions to zero before a split-K launch
+    std::vector<ZeroRegion<T>> hz_;
+    DBuf<ZeroRegion<T>> dz_;
+    int total_tiles_ = 0;
+    bool finalized_ = false;
+};
+
+}  // namespace hm

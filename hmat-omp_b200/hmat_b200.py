@@ -1,0 +1,251 @@
+"""ctypes binding of libhmat_b200.so (the C ABI in include/hmat_b200.h).
+
+The classes mirror the reference's C++ API (chenxinye/hmat-omp
+include/hodlr_routines.h:8-176, include/hss_routines.h:10-307): a constructor taking the
+tolerance, public ``tolerance``/``rsvd_rank`` fields, ``build_from_dense(A, leaf_size)``,
+``multiply(x)`` and ``solve(b)``.  Host arrays are numpy FP64; ``*_device`` methods take
+raw device pointers (e.g. ``torch.Tensor.data_ptr()``).  There is no CPU fallback: if the
+library is missing or no GPU is present the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhmat_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "hmat_b200.h")
+
+HM_OK, HM_ERR_ARG, HM_ERR_CUDA, HM_ERR_SINGULAR, HM_ERR_NO_CONVERGE = 0, 1, 2, 3, 4
+HM_ERR_NONFINITE, HM_ERR_STATE, HM_ERR_UNSUPPORTED, HM_ERR_IR = 5, 6, 7, 8
+SKETCH_REFERENCE_UNIFORM, SKETCH_REFERENCE_NORMAL, SKETCH_DEVICE_NORMAL = 0, 1, 2
+FP64, MIXED = 0, 1
+KERNEL_CAUCHY, KERNEL_GAUSSIAN, KERNEL_COULOMB = 1, 2, 3
+
+
+class HmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("tol", C.c_double),
+        ("rsvd_rank", C.c_int),
+        ("oversample", C.c_int),
+        ("rsvd_min_dim", C.c_int),
+        ("power_iters", C.c_int),
+        ("max_rank", C.c_int),
+        ("sketch", C.c_int),
+        ("seed", C.c_ulonglong),
+        ("precision", C.c_int),
+        ("ir_tol", C.c_double),
+        ("ir_max_iter", C.c_int),
+    ]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("ir_iters", C.c_int), ("rel_residual", C.c_double)]
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} not built: run `make -C hmat-omp_b200`")
+    L = C.CDLL(LIB_PATH)
+    L.hm_opts_default.argtypes = [C.POINTER(Opts)]
+    L.hm_opts_default.restype = None
+    L.hm_create.argtypes = [C.POINTER(Opts), C.POINTER(C.c_void_p)]
+    L.hm_destroy.argtypes = [C.c_void_p]
+    L.hm_last_error.argtypes = [C.c_void_p]
+    L.hm_last_error.restype = C.c_char_p
+    L.hm_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    for f in ("hm_hodlr_build_from_dense", "hm_hss_build_from_dense"):
+        getattr(L, f).argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, C.c_int]
+    L.hm_hodlr_build_from_dense_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
+    PP = C.POINTER(C.c_void_p)
+    L.hm_hodlr_import.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip, PP, PP, PP, PP, PP]
+    L.hm_num_nodes.argtypes = [C.c_void_p]
+    L.hm_export_tree.argtypes = [C.c_void_p] + [_ip] * 6
+    L.hm_get_factor.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _ip, _ip]
+    L.hm_multiply.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_int]
+    L.hm_multiply_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]
+    L.hm_factor.argtypes = [C.c_void_p]
+    L.hm_solve.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_int, C.POINTER(SolveStats)]
+    L.hm_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                  C.POINTER(SolveStats)]
+    _lib = L
+    return L
+
+
+def header_functions() -> list[str]:
+    """Names of the functions declared in include/hmat_b200.h."""
+    import re
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^HM_API\s+[\w\s\*]+?\b(hm_\w+)\(", txt, flags=re.M)))
+
+
+def default_opts() -> Opts:
+    o = Opts()
+    load().hm_opts_default(C.byref(o))
+    return o
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class _Handle:
+    def __init__(self, tol: float, **kw):
+        self._L = load()
+        self.opts = default_opts()
+        self.opts.tol = tol
+        for k, v in kw.items():
+            setattr(self.opts, k, v)
+        self._h = C.c_void_p()
+        self._check(self._L.hm_create(C.byref(self.opts), C.byref(self._h)), create=True)
+        self.N = 0
+
+    # reference public fields
+    @property
+    def tolerance(self) -> float:
+        return self.opts.tol
+
+    @property
+    def rsvd_rank(self) -> int:
+        return self.opts.rsvd_rank
+
+    def _check(self, rc: int, create: bool = False):
+        if rc != HM_OK:
+            msg = "hm_create failed" if create else self._L.hm_last_error(self._h).decode()
+            raise HmError(rc, msg)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.hm_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self._L.hm_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def multiply(self, x: np.ndarray) -> np.ndarray:
+        x = np.asarray(x, dtype=np.float64)
+        vec = x.ndim == 1
+        X = np.asfortranarray(x.reshape(self.N, -1))
+        Y = np.zeros_like(X, order="F")
+        self._check(self._L.hm_multiply(self._h, _d(X), X.shape[1], self.N, _d(Y), self.N))
+        return Y.ravel() if vec else Y
+
+    def multiply_device(self, dx: int, nrhs: int, ldx: int, dy: int, ldy: int):
+        self._check(self._L.hm_multiply_device(self._h, C.c_void_p(dx), nrhs, ldx, C.c_void_p(dy), ldy))
+
+    def factor(self):
+        self._check(self._L.hm_factor(self._h))
+
+    def solve(self, b: np.ndarray, stats: bool = False):
+        b = np.asarray(b, dtype=np.float64)
+        vec = b.ndim == 1
+        B = np.asfortranarray(b.reshape(self.N, -1))
+        X = np.zeros_like(B, order="F")
+        st = SolveStats()
+        self._check(self._L.hm_solve(self._h, _d(B), B.shape[1], self.N, _d(X), self.N, C.byref(st)))
+        out = X.ravel() if vec else X
+        return (out, st) if stats else out
+
+    def solve_device(self, db: int, nrhs: int, ldb: int, dx: int, ldx: int) -> SolveStats:
+        st = SolveStats()
+        self._check(self._L.hm_solve_device(self._h, C.c_void_p(db), nrhs, ldb, C.c_void_p(dx), ldx,
+                                            C.byref(st)))
+        return st
+
+    def num_nodes(self) -> int:
+        return self._L.hm_num_nodes(self._h)
+
+    def tree(self) -> dict:
+        n = self.num_nodes()
+        names = ["start", "end", "is_leaf", "depth", "rank12", "rank21"]
+        arrs = [np.zeros(n, dtype=np.int32) for _ in names]
+        self._check(self._L.hm_export_tree(self._h, *[a.ctypes.data_as(_ip) for a in arrs]))
+        return dict(zip(names, arrs))
+
+    def get_factor(self, node: int, which: int) -> np.ndarray:
+        r, c = C.c_int(), C.c_int()
+        self._check(self._L.hm_get_factor(self._h, node, which, None, C.byref(r), C.byref(c)))
+        out = np.zeros(r.value * c.value)
+        if out.size:
+            self._check(self._L.hm_get_factor(self._h, node, which, _d(out), C.byref(r), C.byref(c)))
+        return out.reshape(c.value, r.value).T.copy()
+
+
+class HODLRMatrix(_Handle):
+    """Mirror of HODLRMatrix (hodlr_routines.h:8-176) on the device path."""
+
+    D, U, V, B12, B21 = 0, 1, 2, 3, 4
+
+    def __init__(self, tol: float = 1e-6, **kw):
+        super().__init__(tol, **kw)
+
+    def build_from_dense(self, A: np.ndarray, leaf_size: int):
+        A = np.asfortranarray(A, dtype=np.float64)
+        self.N = A.shape[0]
+        self._check(self._L.hm_hodlr_build_from_dense(self._h, _d(A), self.N, self.N, leaf_size))
+
+    def build_from_dense_device(self, dA: int, N: int, lda: int, leaf_size: int):
+        self.N = N
+        self._check(self._L.hm_hodlr_build_from_dense_device(self._h, C.c_void_p(dA), N, lda, leaf_size))
+
+    def import_factors(self, N: int, leaf_size: int, nodes) -> None:
+        """Upload a tree of reference factors; ``nodes`` in pre-order with attributes
+        D/U/V/B12/B21 (numpy or None), as oracle.hmat_oracle.HNode holds them."""
+        self.N = N
+        n = len(nodes)
+        keep = []
+
+        def arr(m):
+            if m is None or m.size == 0:
+                return None
+            a = np.asfortranarray(m, dtype=np.float64)
+            keep.append(a)
+            return a.ctypes.data
+
+        PP = C.c_void_p * n
+        D = PP(*[arr(x.D) if x.is_leaf else None for x in nodes])
+        U = PP(*[arr(x.U) if i > 0 else None for i, x in enumerate(nodes)])
+        V = PP(*[arr(x.V) if i > 0 else None for i, x in enumerate(nodes)])
+        B12 = PP(*[arr(x.B12) if not x.is_leaf else None for x in nodes])
+        B21 = PP(*[arr(x.B21) if not x.is_leaf else None for x in nodes])
+        r12 = np.array([0 if x.is_leaf else x.B12.shape[0] for x in nodes], dtype=np.int32)
+        r21 = np.array([0 if x.is_leaf else x.B21.shape[0] for x in nodes], dtype=np.int32)
+        self._check(self._L.hm_hodlr_import(self._h, N, leaf_size, r12.ctypes.data_as(_ip),
+                                            r21.ctypes.data_as(_ip), D, U, V, B12, B21))
+
+
+class HSSMatrix(_Handle):
+    """Mirror of HSSMatrix (hss_routines.h:10-307) on the device path."""
+
+    D, U, V, R, W, B = 0, 1, 2, 3, 4, 5
+
+    def __init__(self, tol: float = 1e-9, **kw):
+        super().__init__(tol, **kw)
+
+    def build_from_dense(self, A: np.ndarray, leaf_size: int):
+        A = np.asfortranarray(A, dtype=np.float64)
+        self.N = A.shape[0]
+        self._check(self._L.hm_hss_build_from_dense(self._h, _d(A), self.N, self.N, leaf_size))

@@ -1,0 +1,150 @@
+/* hmat_b200.h — C ABI of the B200 hierarchical-matrix library (libhmat_b200.so).
+ *
+ * The reference (chenxinye/hmat-omp) is a header-only C++ library whose callers use
+ * four classes — HODLRMatrix[OMP] and HSSMatrix[OMP] — with the same three methods:
+ *   ctor(double tol)                          include/hodlr_routines.h:16, hss_routines.h:18
+ *   void build_from_dense(const Matrix&, int) include/hodlr_routines.h:20, hss_routines.h:50
+ *   Matrix multiply(const Matrix& x)          include/hodlr_routines.h:66, hss_routines.h:118
+ *   Matrix solve(const Matrix& b)             include/hodlr_routines.h:108, hss_routines.h:197
+ * and the public fields root/nodes/N/tolerance/rsvd_rank (hodlr_routines.h:10-14).
+ * Each entry point below names the reference interface it replaces.  Matrices are
+ * column-major FP64 with an explicit leading dimension, as Matrix stores them
+ * (include/matrix.h:36).  Every function returns an HM_* status; 0 is success and
+ * hm_last_error() holds the message of the last failure on a handle.
+ *
+ * Device work runs on the handle's CUDA stream (hm_set_stream).  Host-buffer entry
+ * points copy in and out and return when the result is on the host.  Calls on one
+ * handle must not overlap; different handles may be used from different threads.
+ */
+#ifndef HMAT_B200_H
+#define HMAT_B200_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define HM_API __attribute__((visibility("default")))
+#else
+#define HM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+enum {
+    HM_OK = 0,
+    HM_ERR_ARG = 1,          /* invalid argument (shape, pointer, option) */
+    HM_ERR_CUDA = 2,         /* CUDA runtime error */
+    HM_ERR_SINGULAR = 3,     /* zero or non-finite pivot in a leaf or capacitance inverse */
+    HM_ERR_NO_CONVERGE = 4,  /* a Jacobi eigen/SVD iteration hit its sweep limit */
+    HM_ERR_NONFINITE = 5,    /* non-finite input or result */
+    HM_ERR_STATE = 6,        /* call out of order (e.g. solve before build) */
+    HM_ERR_UNSUPPORTED = 7,  /* size or option outside what this build supports */
+    HM_ERR_IR = 8            /* iterative refinement did not reach ir_tol */
+};
+
+/* ---- sketch sources for the randomized SVD (compression.h:78) ---- */
+enum {
+    HM_SKETCH_REFERENCE_UNIFORM = 0, /* std::mt19937(seed) + uniform_real_distribution<double>(0,1),
+                                        drawn on the host in the reference's serial build order
+                                        (Matrix::Random, matrix.h:50-57): bit-identical sketches */
+    HM_SKETCH_REFERENCE_NORMAL = 1,  /* same stream through normal_distribution<double>(0,1) */
+    HM_SKETCH_DEVICE_NORMAL = 2      /* N(0,1) from a counter-based generator on the device */
+};
+
+enum { HM_FP64 = 0, HM_MIXED = 1 };
+
+/* Matrix-free kernel generators (hm_hodlr_build_from_kernel). */
+enum {
+    HM_KERNEL_CAUCHY = 1,   /* A_ij = 1/(x_i - y_j) + p0*delta_ij; rows x = pts[0:N], cols y = pts[N:2N] */
+    HM_KERNEL_GAUSSIAN = 2, /* A_ij = exp(-|p_i - p_j|^2 / (2 p0^2)) + p1*delta_ij */
+    HM_KERNEL_COULOMB = 3   /* A_ij = 1/(|p_i - p_j| + p0) + p1*delta_ij */
+};
+
+typedef struct hm_opts {
+    double tol;          /* truncation tolerance: HODLRMatrix(tol) (hodlr_routines.h:16) */
+    int rsvd_rank;       /* rank guess, public field rsvd_rank = 64 (hodlr_routines.h:16) */
+    int oversample;      /* k = rsvd_rank + oversample (compression.h:74: 10) */
+    int rsvd_min_dim;    /* blocks with m or n below this use a full SVD (compression.h:72: 256) */
+    int power_iters;     /* extension (0 = reference behaviour) */
+    int max_rank;        /* extension: cap on every block rank (0 = no cap, the reference) */
+    int sketch;          /* HM_SKETCH_* */
+    unsigned long long seed;
+    int precision;       /* HM_FP64, or HM_MIXED (FP32 bulk + FP64 LUs + FP64-residual refinement) */
+    double ir_tol;       /* HM_MIXED: target max_j ||b_j - A x_j|| / ||b_j|| */
+    int ir_max_iter;     /* HM_MIXED: refinement iteration limit */
+} hm_opts;
+
+typedef struct hm_handle hm_handle;
+
+typedef struct hm_solve_stats {
+    int ir_iters;          /* refinement iterations taken (0 in FP64 mode) */
+    double rel_residual;   /* max_j ||b_j - A~ x_j|| / ||b_j|| against the FP64 compressed operator
+                              (computed in HM_MIXED mode; -1 when not computed) */
+} hm_solve_stats;
+
+/* Defaults mirror the reference: tol 1e-6, rsvd_rank 64, oversample 10, min dim 256,
+ * no power iteration, no rank cap, reference uniform sketch with seed 0, FP64. */
+HM_API void hm_opts_default(hm_opts* o);
+
+/* Replaces the constructors HODLRMatrix(tol) / HSSMatrix(tol) (hodlr_routines.h:16,
+ * hss_routines.h:18): options, stream and device memory live in the handle. */
+HM_API int hm_create(const hm_opts* o, hm_handle** out);
+/* Replaces ~HODLRMatrix / ~HSSMatrix (hodlr_routines.h:17, hss_routines.h:19). */
+HM_API int hm_destroy(hm_handle* h);
+HM_API const char* hm_last_error(const hm_handle* h);
+/* Work is enqueued on `stream` (a cudaStream_t); NULL = the handle's own stream. */
+HM_API int hm_set_stream(hm_handle* h, void* stream);
+
+/* HODLRMatrix::build_from_dense(A, leaf_size) (hodlr_routines.h:20-63): tree split
+ * mid=(s+e)/2, leaf iff len <= leaf; A12 -> (left.U, right.V, B_12), A21 -> (right.U,
+ * left.V, B_21) by compress_rsvd (compression.h:67-99).  A: host, N x N, column-major. */
+HM_API int hm_hodlr_build_from_dense(hm_handle* h, const double* A, int N, int lda, int leaf_size);
+/* Same, with A already in device memory. */
+HM_API int hm_hodlr_build_from_dense_device(hm_handle* h, const double* dA, int N, int lda, int leaf_size);
+
+/* HSSMatrix::build_from_dense(A, leaf_size) (hss_routines.h:50-113): build_topo ids,
+ * leaf row/column bases of the off-diagonal strips, identity transfers, dense B. */
+HM_API int hm_hss_build_from_dense(hm_handle* h, const double* A, int N, int lda, int leaf_size);
+
+/* Upload a HODLR tree built elsewhere (e.g. by HODLRMatrix::build_from_dense) so the
+ * device path can multiply/solve with exactly those factors.  Nodes in pre-order
+ * (root, left subtree, right subtree); per node pointers to host column-major
+ * blocks: D (leaf, len x len), U and V (non-root, len x rank from the parent's
+ * compression), B12/B21 (internal, rank x rank).  NULL where the reference field is
+ * empty.  ranks12/ranks21: B_12/B_21 sizes (0 for leaves). */
+HM_API int hm_hodlr_import(hm_handle* h, int N, int leaf_size, const int* ranks12, const int* ranks21,
+                    const double* const* D, const double* const* U, const double* const* V,
+                    const double* const* B12, const double* const* B21);
+
+/* Tree introspection, pre-order for HODLR (the reference's recursion order) and id
+ * order for HSS (hss_routines.h:293-306).  rank12/rank21 are B_12/B_21 sizes for
+ * HODLR and rank_U/rank_V for HSS. */
+HM_API int hm_num_nodes(const hm_handle* h);
+HM_API int hm_export_tree(const hm_handle* h, int* idx_start, int* idx_end, int* is_leaf, int* depth,
+                   int* rank12, int* rank21);
+/* Download one node's factor in the reference layout.  HODLR which: 0 D, 1 U, 2 V,
+ * 3 B_12, 4 B_21 (utils.h:6-29).  HSS which: 0 D, 1 U, 2 V, 3 R, 4 W, 5 B (utils.h:32-55).
+ * rows/cols receive the shape; out may be NULL to query the shape only. */
+HM_API int hm_get_factor(const hm_handle* h, int node, int which, double* out, int* rows, int* cols);
+
+/* multiply(x) (hodlr_routines.h:66-105, hss_routines.h:118-192) for nrhs columns. */
+HM_API int hm_multiply(hm_handle* h, const double* x, int nrhs, int ldx, double* y, int ldy);
+HM_API int hm_multiply_device(hm_handle* h, const double* dx, int nrhs, int ldx, double* dy, int ldy);
+
+/* Factor once: leaf inverses and one Woodbury capacitance inverse per node, bottom-up
+ * (the quantities the reference's solve recomputes on every call,
+ * hodlr_routines.h:112-175, hss_routines.h:205-279).  solve() factors on demand. */
+HM_API int hm_factor(hm_handle* h);
+
+/* solve(b) (hodlr_routines.h:108-175, hss_routines.h:197-290) for nrhs columns. */
+HM_API int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ldx,
+             hm_solve_stats* stats);
+HM_API int hm_solve_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx,
+                    hm_solve_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HMAT_B200_H */
