@@ -22,9 +22,11 @@ struct Error : std::runtime_error {
 #define HM_CUDA(call)                                                                      \
     do {                                                                                   \
         cudaError_t e_ = (call);                                                           \
-        if (e_ != cudaSuccess)                                                             \
+        if (e_ != cudaSuccess) {                                                           \
+            (void)cudaGetLastError();                                                      \
             throw ::hm::Error(HM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_) + \
                                                " at " __FILE__ ":" + std::to_string(__LINE__)); \
+        }                                                                                  \
     } while (0)
 
 #define HM_CHECK(cond, code, msg)                                     \
@@ -68,6 +70,14 @@ struct DBuf {
         if (n) HM_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
     }
 };
+
+// Raise a kernel's dynamic shared-memory limit to `bytes` (once per larger request).
+template <typename K>
+inline void ensure_dyn_smem(K kernel, size_t bytes, size_t& current) {
+    if (bytes <= current || bytes <= 48 * 1024) return;
+    HM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    current = bytes;
+}
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }

@@ -110,12 +110,8 @@ void launch_gj(const DevTable<GJDesc>& t, int* status, cudaStream_t s) {
     for (auto& d : t.h) nmax = std::max(nmax, d.n);
     HM_CHECK(nmax <= GJ_MAX, HM_ERR_UNSUPPORTED, "Gauss-Jordan block larger than GJ_MAX");
     size_t smem = (size_t)nmax * nmax * 8 + 2 * (size_t)nmax * 8 + (size_t)nmax * 4 + 16;
-    static bool attr = false;
-    if (!attr) {
-        HM_CUDA(cudaFuncSetAttribute(gj_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     227 * 1024));
-        attr = true;
-    }
+    static size_t cur = 0;
+    ensure_dyn_smem(gj_inverse_kernel, smem, cur);
     gj_inverse_kernel<<<t.size(), 256, smem, s>>>(t.d.p, status);
     HM_CUDA(cudaGetLastError());
 }
@@ -235,57 +231,96 @@ void launch_jacobi(const DevTable<EigDesc>& t, int* status, cudaStream_t s, int 
     int kmax = 0;
     for (auto& d : t.h) kmax = std::max(kmax, d.k);
     size_t smem = (kmax <= JAC_SMEM_MAX ? (size_t)kmax * kmax * 8 : 0) + ((size_t)kmax + 2) * 8;
-    static bool attr = false;
-    if (!attr) {
-        HM_CUDA(cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     227 * 1024));
-        attr = true;
-    }
+    static size_t cur = 0;
+    ensure_dyn_smem(jacobi_kernel, smem, cur);
     jacobi_kernel<<<t.size(), 256, smem, s>>>(t.d.p, status, max_sweeps, kmax <= JAC_SMEM_MAX);
     HM_CUDA(cudaGetLastError());
 }
 
 // ---------------------------------------------------------------------------------
-// Sort eigenpairs (descending), scale, truncation rank
+// Column norms, sort + truncation rank, permute/scale
 // ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) norms_kernel(const NormDesc* __restrict__ descs) {
+    const NormDesc d = descs[blockIdx.x];
+    const int c = blockIdx.y;
+    if (c >= d.k) return;
+    const double* x = d.X + (size_t)c * d.ld;
+    // scaled sum of squares (no overflow/underflow for tiny or huge columns)
+    double mx = 0.0;
+    for (int i = threadIdx.x; i < d.rows; i += blockDim.x) mx = fmax(mx, fabs(x[i]));
+    __shared__ double red[32];
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        mx = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
+        if (threadIdx.x == 0) red[0] = mx;
+    }
+    __syncthreads();
+    mx = red[0];
+    __syncthreads();
+    if (mx == 0.0) {
+        if (threadIdx.x == 0) d.out[c] = 0.0;
+        return;
+    }
+    const double inv = 1.0 / mx;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < d.rows; i += blockDim.x) {
+        const double v = x[i] * inv;
+        s = fma(v, v, s);
+    }
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+        if (threadIdx.x == 0) d.out[c] = mx * sqrt(s);
+    }
+}
+
+void launch_norms(const DevTable<NormDesc>& t, cudaStream_t s) {
+    if (t.h.empty()) return;
+    int kmax = 0;
+    for (auto& d : t.h) kmax = std::max(kmax, d.k);
+    HM_CHECK(kmax <= 65535, HM_ERR_UNSUPPORTED, "too many columns");
+    norms_kernel<<<dim3(t.size(), kmax), 256, 0, s>>>(t.d.p);
+    HM_CUDA(cudaGetLastError());
+}
+
 __global__ void __launch_bounds__(256) prep_kernel(const PrepDesc* __restrict__ descs, double tol,
                                                    int max_rank) {
     extern __shared__ double sm[];
     const PrepDesc d = descs[blockIdx.x];
     const int k = d.k;
     if (k <= 0) return;
-    double* lam = sm;
-    int* perm = reinterpret_cast<int*>(lam + k);
+    double* sg = sm;
+    int* perm = reinterpret_cast<int*>(sg + k);
     const int tid = threadIdx.x, nt = blockDim.x;
-    for (int i = tid; i < k; i += nt) lam[i] = d.lam[i];
+    for (int i = tid; i < k; i += nt) sg[i] = d.sig_in[i];
     __syncthreads();
-    // rank of each entry in descending order (ties by index): perm[pos] = i
+    // position of each entry in descending order (ties by index)
     for (int i = tid; i < k; i += nt) {
-        const double v = lam[i];
+        const double v = sg[i];
         int pos = 0;
         for (int j = 0; j < k; ++j) {
-            const double w = lam[j];
+            const double w = sg[j];
             pos += (w > v) || (w == v && j < i);
         }
         perm[pos] = i;
     }
     __syncthreads();
-    for (int e = tid; e < k * k; e += nt) {
-        const int i = e % k, c = e / k;
-        const int src = perm[c];
-        const double sig = sqrt(fmax(lam[src], 0.0));
-        const double w = d.W[i + (size_t)src * d.ldw];
-        d.Ws[i + (size_t)c * d.ldws] = sig > 0.0 ? w / sig : 0.0;
-        if (d.Wp) d.Wp[i + (size_t)c * d.ldwp] = w;
+    for (int c = tid; c < k; c += nt) {
+        d.perm[c] = perm[c];
+        if (d.sigma) d.sigma[c] = sg[perm[c]];
     }
-    if (d.sigma)
-        for (int c = tid; c < k; c += nt) d.sigma[c] = sqrt(fmax(lam[perm[c]], 0.0));
     if (d.rank && tid == 0) {
         // compression.h:42-46: #{S_i > tol*S_0} when S_0 > 1e-15, at least 1
-        const double s0 = sqrt(fmax(lam[perm[0]], 0.0));
+        const double s0 = sg[perm[0]];
         int r = 0;
         if (s0 > 1e-15)
-            for (int c = 0; c < k; ++c) r += sqrt(fmax(lam[perm[c]], 0.0)) > tol * s0;
+            for (int c = 0; c < k; ++c) r += sg[perm[c]] > tol * s0;
         if (r == 0) r = 1;
         if (max_rank > 0 && r > max_rank) r = max_rank;
         *d.rank = r;
@@ -298,6 +333,32 @@ void launch_prep(const DevTable<PrepDesc>& t, double tol, int max_rank, cudaStre
     for (auto& d : t.h) kmax = std::max(kmax, d.k);
     size_t smem = (size_t)kmax * 12 + 16;
     prep_kernel<<<t.size(), 256, smem, s>>>(t.d.p, tol, max_rank);
+    HM_CUDA(cudaGetLastError());
+}
+
+__global__ void permute_kernel(const PermDesc* __restrict__ descs) {
+    const PermDesc d = descs[blockIdx.y];
+    const size_t total = (size_t)d.rows * d.k;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e % d.rows), c = (int)(e / d.rows);
+        const int src = d.perm[c];
+        double v = d.src[i + (size_t)src * d.lds];
+        if (d.sig) {
+            const double sg = d.sig[c];
+            v = sg > 0.0 ? v / sg : 0.0;
+        }
+        d.dst[i + (size_t)c * d.ldd] = v;
+    }
+}
+
+void launch_permute(const DevTable<PermDesc>& t, cudaStream_t s) {
+    if (t.h.empty()) return;
+    size_t mx = 0;
+    for (auto& d : t.h) mx = std::max(mx, (size_t)d.rows * d.k);
+    int gx = (int)std::min<size_t>(std::max<size_t>(1, (mx + 255) / 256), 1024);
+    HM_CHECK(t.size() <= 65535, HM_ERR_UNSUPPORTED, "permute batch too large");
+    permute_kernel<<<dim3(gx, t.size()), 256, 0, s>>>(t.d.p);
     HM_CUDA(cudaGetLastError());
 }
 
@@ -412,54 +473,71 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
 }
 
 void plan_gram_svd(Plan& plan, const std::vector<SvdProblem>& probs, double tol, int max_rank,
-                   cudaStream_t s) {
+                   cudaStream_t s, int rounds) {
     if (probs.empty()) return;
-    auto gramA = std::make_unique<GemmStep<double>>();
-    auto eigA = std::make_unique<EigStep>();
-    auto rotA = std::make_unique<GemmStep<double>>();
-    auto gramB = std::make_unique<GemmStep<double>>();
-    auto eigB = std::make_unique<EigStep>();
+    rounds = std::max(1, rounds);
+    struct Work { const SvdProblem* p; const double* X; int ldx; double* Wt; };
+    std::vector<Work> w;
+    for (auto& p : probs)
+        if (p.k > 0 && p.rows > 0) w.push_back({&p, p.X, p.ldx, nullptr});
+    if (w.empty()) return;
+    for (int r = 0; r < rounds; ++r) {
+        auto gram = std::make_unique<GemmStep<double>>();
+        auto eig = std::make_unique<EigStep>();
+        auto rot = std::make_unique<GemmStep<double>>();
+        auto acc = std::make_unique<GemmStep<double>>();
+        for (auto& x : w) {
+            const int k = x.p->k, m = x.p->rows;
+            double* G = plan.scratch((size_t)k * k);
+            double* W = plan.scratch((size_t)k * k);
+            double* lam = plan.scratch(k);
+            double* Xn = plan.scratch((size_t)m * k);
+            gram->batch.add(k, k, m, 1.0, x.X, x.ldx, OP_T, x.X, x.ldx, OP_N, 0.0, G, k);
+            eig->t.h.push_back({G, k, W, k, lam, k});
+            rot->batch.add(m, k, k, 1.0, x.X, x.ldx, OP_N, W, k, OP_N, 0.0, Xn, m);
+            if (x.p->R) {
+                if (!x.Wt) {
+                    x.Wt = W;
+                } else {
+                    double* Wn = plan.scratch((size_t)k * k);
+                    acc->batch.add(k, k, k, 1.0, x.Wt, k, OP_N, W, k, OP_N, 0.0, Wn, k);
+                    x.Wt = Wn;
+                }
+            }
+            x.X = Xn;
+            x.ldx = m;
+        }
+        gram->batch.finalize(s);
+        eig->t.upload(s);
+        rot->batch.finalize(s);
+        acc->batch.finalize(s);
+        plan.add(std::move(gram));
+        plan.add(std::move(eig));
+        plan.add(std::move(rot));
+        if (!acc->batch.empty()) plan.add(std::move(acc));
+    }
+    auto nrm = std::make_unique<NormStep>();
     auto prep = std::make_unique<PrepStep>();
-    auto outL = std::make_unique<GemmStep<double>>();
-    auto outR = std::make_unique<GemmStep<double>>();
+    auto perm = std::make_unique<PermStep>();
     prep->tol = tol;
     prep->max_rank = max_rank;
-    for (auto& p : probs) {
+    for (auto& x : w) {
+        const SvdProblem& p = *x.p;
         const int k = p.k, m = p.rows;
-        if (k <= 0 || m <= 0) continue;
-        double* G = plan.scratch((size_t)k * k);
-        double* W1 = plan.scratch((size_t)k * k);
-        double* W2 = plan.scratch((size_t)k * k);
-        double* lam1 = plan.scratch(k);
-        double* lam2 = plan.scratch(k);
-        double* Ws = plan.scratch((size_t)k * k);
-        double* Wp = p.R ? plan.scratch((size_t)k * k) : nullptr;
-        double* X1 = plan.scratch((size_t)m * k);
-        gramA->batch.add(k, k, m, 1.0, p.X, p.ldx, OP_T, p.X, p.ldx, OP_N, 0.0, G, k);
-        eigA->t.h.push_back({G, k, W1, k, lam1, k});
-        rotA->batch.add(m, k, k, 1.0, p.X, p.ldx, OP_N, W1, k, OP_N, 0.0, X1, m);
-        gramB->batch.add(k, k, m, 1.0, X1, m, OP_T, X1, m, OP_N, 0.0, G, k);
-        eigB->t.h.push_back({G, k, W2, k, lam2, k});
-        prep->t.h.push_back({lam2, W2, k, Ws, k, Wp, k, p.sigma, p.rank, k});
-        outL->batch.add(m, k, k, 1.0, X1, m, OP_N, Ws, k, OP_N, 0.0, p.L, p.ldl);
-        if (p.R) outR->batch.add(k, k, k, 1.0, W1, k, OP_N, Wp, k, OP_N, 0.0, p.R, p.ldr);
+        double* raw = plan.scratch(k);
+        double* sig = p.sigma ? p.sigma : plan.scratch(k);
+        int* pm = plan.scratch_i(k);
+        nrm->t.h.push_back({x.X, x.ldx, m, k, raw});
+        prep->t.h.push_back({raw, sig, pm, p.rank, k});
+        perm->t.h.push_back({x.X, x.ldx, p.L, p.ldl, m, k, pm, sig});
+        if (p.R) perm->t.h.push_back({x.Wt, k, p.R, p.ldr, k, k, pm, nullptr});
     }
-    gramA->batch.finalize(s);
-    eigA->t.upload(s);
-    rotA->batch.finalize(s);
-    gramB->batch.finalize(s);
-    eigB->t.upload(s);
+    nrm->t.upload(s);
     prep->t.upload(s);
-    outL->batch.finalize(s);
-    outR->batch.finalize(s);
-    plan.add(std::move(gramA));
-    plan.add(std::move(eigA));
-    plan.add(std::move(rotA));
-    plan.add(std::move(gramB));
-    plan.add(std::move(eigB));
+    perm->t.upload(s);
+    plan.add(std::move(nrm));
     plan.add(std::move(prep));
-    plan.add(std::move(outL));
-    if (!outR->batch.empty()) plan.add(std::move(outR));
+    plan.add(std::move(perm));
 }
 
 }  // namespace hm

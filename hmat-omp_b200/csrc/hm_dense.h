@@ -33,18 +33,32 @@ struct EigDesc {
     int k;
 };
 
-// Per-problem post-processing of a Jacobi eigen-decomposition of X^T X.
+// Column norms of a tall block.
+struct NormDesc {
+    const double* X;
+    int ld;
+    int rows, k;
+    double* out;         // k
+};
+
+// Sort singular values (descending) and derive the truncation rank.
 struct PrepDesc {
-    const double* lam;   // k
-    const double* W;     // k x k
-    int ldw;
-    double* Ws;          // k x k: W[:, perm] * diag(1/sigma)  (0 where sigma == 0)
-    int ldws;
-    double* Wp;          // optional k x k: W[:, perm]
-    int ldwp;
-    double* sigma;       // optional k: sorted singular values
-    int* rank;           // optional: truncation rank
+    const double* sig_in;  // k, unsorted
+    double* sigma;         // k, sorted (nullptr allowed)
+    int* perm;             // k: sorted position -> source column
+    int* rank;             // truncation rank (nullptr allowed)
     int k;
+};
+
+// dst[:, c] = src[:, perm[c]] / sig[c]  (sig == nullptr: no scaling; sig[c] == 0: zero column)
+struct PermDesc {
+    const double* src;
+    int lds;
+    double* dst;
+    int ldd;
+    int rows, k;
+    const int* perm;
+    const double* sig;
 };
 
 struct CopyDesc {
@@ -80,6 +94,8 @@ struct DevTable {
 void launch_gj(const DevTable<GJDesc>& t, int* status, cudaStream_t s);
 void launch_jacobi(const DevTable<EigDesc>& t, int* status, cudaStream_t s, int max_sweeps = 40);
 void launch_prep(const DevTable<PrepDesc>& t, double tol, int max_rank, cudaStream_t s);
+void launch_norms(const DevTable<NormDesc>& t, cudaStream_t s);
+void launch_permute(const DevTable<PermDesc>& t, cudaStream_t s);
 void launch_copy(const DevTable<CopyDesc>& t, cudaStream_t s);
 void launch_ident(const DevTable<IdentDesc>& t, cudaStream_t s);
 
@@ -146,6 +162,14 @@ struct PrepStep : Plan::Step {
     int max_rank = 0;
     void run(cudaStream_t s, int*) const override { launch_prep(t, tol, max_rank, s); }
 };
+struct NormStep : Plan::Step {
+    DevTable<NormDesc> t;
+    void run(cudaStream_t s, int*) const override { launch_norms(t, s); }
+};
+struct PermStep : Plan::Step {
+    DevTable<PermDesc> t;
+    void run(cudaStream_t s, int*) const override { launch_permute(t, s); }
+};
 struct CopyStep : Plan::Step {
     DevTable<CopyDesc> t;
     void run(cudaStream_t s, int*) const override { launch_copy(t, s); }
@@ -168,8 +192,11 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
 
 // Gram/Jacobi SVD of tall X_i (rows x k): X = L diag(sigma) R^T with L (rows x k)
 // orthonormal columns and R (k x k) orthogonal, sigma sorted descending; optionally
-// the truncation rank.  Two rounds (X1 = X W1, then the graded X1^T X1) keep small
-// singular values accurate relative to their own size.
+// the truncation rank.  Each round rotates X by the eigenvectors of its Gram matrix
+// (X <- X W, W from Jacobi on X^T X); a Gram matrix resolves about half of the double
+// precision range of singular values relative to its own columns, so three rounds
+// separate the full range (sigma down to ~1e-16 sigma_0).  sigma is taken from the
+// column norms of the final rotated X, not from the Gram diagonal.
 struct SvdProblem {
     const double* X;
     int ldx;
@@ -183,6 +210,6 @@ struct SvdProblem {
     bool sort;
 };
 void plan_gram_svd(Plan& plan, const std::vector<SvdProblem>& probs, double tol, int max_rank,
-                   cudaStream_t s);
+                   cudaStream_t s, int rounds = 3);
 
 }  // namespace hm

@@ -70,7 +70,7 @@ def test_imported_reference_factors(golden_dir, name):
     h = H.HODLRMatrix(c["tol"])
     h.import_factors(A.shape[0], c["leaf"], o.nodes)
     assert O.rel_err(g["y"], h.multiply(x)) < 1e-12
-    assert O.rel_err(g["xs"], h.solve(b)) < 1e-11
+    assert O.rel_err(g["xs"], h.solve(b)) < 1e-10
     # factor download round-trips
     for i in (1, 2, len(o.nodes) - 1):
         n = o.nodes[i]
