@@ -1,0 +1,354 @@
+"""Benchmark: HODLR factor + solve, mixed precision vs the plain FP64 GPU path.
+
+Workload (the headline configuration): 2-D Coulomb kernel
+A_ij = 1/(|p_i - p_j| + 1e-3) + 4 delta_ij on N = 2^18 points uniform in the unit
+square (seed 3), Morton-sorted; HODLR with leaf 256, ranks <= 96 (RSVD, sketch width
+106, Gaussian sketch), built matrix-free on the device; 64 right-hand sides
+b ~ N(0,1).  One step = factor + solve of the 64 right-hand sides; the mixed path
+refines against the FP64 compressed operator to relative residual <= 1e-10.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  --impl reference times the reference's own OpenMP
+solve (the oracle library compiled from the reference sources) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for sub in ("hmat-omp_b200", "oracle"):
+    sys.path.insert(0, os.path.join(ROOT, sub))
+
+import numpy as np  # noqa: E402
+
+METRIC = "HODLR factor+solve RHS/s at N=2^18 (Coulomb 2-D, 64 RHS, mixed precision refined to resid<=1e-10)"
+UNIT = "RHS/s"
+
+
+def morton_points(N: int, seed: int) -> np.ndarray:
+    import hmat_oracle as O  # point ordering helper only (not the measured path)
+    p = np.random.default_rng(seed).random((N, 2))
+    return np.ascontiguousarray(p[O.morton_order(p)])
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1 << 18)
+    ap.add_argument("--leaf", type=int, default=256)
+    ap.add_argument("--rank", type=int, default=96)
+    ap.add_argument("--nrhs", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-only", action="store_true", help="one profiled step, no timing")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------------------
+# CPU reference (oracle/_ref: the reference's OpenMP HODLR solve)
+# --------------------------------------------------------------------------------------
+def reference_sample(n_small=(4096, 8192), nrhs=64, leaf=256, rank=96, reps=1):
+    """Time HODLRMatrixOMP::solve (the reference has no separate factor: its solve is
+    factor+solve) on Coulomb problems of the workload's kind at CPU-feasible sizes, fit
+    t ~ N^alpha and scale to the benchmark N.  Returns dict."""
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")  # run_tests.sh:7
+    import hmat_oracle as O
+    import ref
+    out = {}
+    for N in n_small:
+        p = morton_points(N, 3)
+        A = O.coulomb_matrix(p)
+        R = ref.RefHODLR(A, leaf, 1e-10, rank, seed=0)
+        b = np.random.default_rng(3).standard_normal((N, nrhs))
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            R.solve_omp(b)
+            ts.append(time.perf_counter() - t0)
+        out[N] = min(ts)
+        R.close()
+    threads = ref.lib().hmref_omp_max_threads()
+    return out, threads
+
+
+def extrapolate(times: dict, N: int):
+    ns = sorted(times)
+    a = np.log(times[ns[-1]] / times[ns[0]]) / np.log(ns[-1] / ns[0])
+    a = float(min(max(a, 1.5), 2.5))
+    return times[ns[-1]] * (N / ns[-1]) ** a, a
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent)"}))
+        return
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    # alpha from two sample sizes, then timed steps at the larger sample
+    times, threads = reference_sample()
+    t_full, alpha = extrapolate(times, args.n)
+    import hmat_oracle as O
+    import ref as R_
+    Ns = 8192
+    A = O.coulomb_matrix(morton_points(Ns, 3))
+    R = R_.RefHODLR(A, args.leaf, 1e-10, args.rank, seed=0)
+    b = np.random.default_rng(3).standard_normal((Ns, args.nrhs))
+    for _ in range(args.warmup):
+        R.solve_omp(b)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        R.solve_omp(b)
+    per = (time.perf_counter() - t0) / args.steps
+    R.close()
+    t_step_full = per * (args.n / Ns) ** alpha
+    v = args.nrhs / t_step_full
+    sample = (f"HODLRMatrixOMP::solve, 64 RHS, Coulomb 2-D N={Ns} leaf {args.leaf} rsvd_rank {args.rank} "
+              f"(measured {per:.3f} s/step), scaled to N={args.n} by the measured N^{alpha:.2f} law "
+              f"(sizes {sorted(times)})")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step_full * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(args),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def workload_config(args):
+    return {
+        "workload": f"hodlr_coulomb2d_N{args.n}_leaf{args.leaf}_rank{args.rank}_nrhs{args.nrhs}",
+        "N": args.n, "leaf": args.leaf, "max_rank": args.rank, "sketch_width": args.rank + 10,
+        "nrhs": args.nrhs, "kernel": "1/(|p_i-p_j|+1e-3)+4*delta_ij, p~U[0,1]^2 seed 3, Morton order",
+        "precision": "mixed: FP32 factor/solve sweeps, FP64 leaf+capacitance inverses, FP64 residual refinement",
+        "ir_tol": 1e-10,
+        "l2": "no flush: factor data (GBs) exceeds the 126 MB L2",
+        "parallelism": "one system per GPU (replicas)",
+    }
+
+
+# --------------------------------------------------------------------------------------
+# Clock sampling during the timed region
+# --------------------------------------------------------------------------------------
+class Clocks:
+    def __init__(self, dev: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={dev}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) > 2 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 2 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and "Active" in r[5 + i] and "Not" not in r[5 + i]:
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------------------
+# Our path
+# --------------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import hmat_b200 as H
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    N, s = args.n, args.nrhs
+    pts = morton_points(N, 3)
+    h = H.HODLRMatrix(1e-10, rsvd_rank=args.rank, oversample=10, max_rank=args.rank, sketch=H.SKETCH_DEVICE_NORMAL,
+                      seed=0, precision=H.MIXED, ir_tol=1e-10, ir_max_iter=30)
+    h.set_stream(stream.cuda_stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    h.build_from_kernel(H.KERNEL_COULOMB, pts, [1e-3, 4.0], args.leaf)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_build = ev0.elapsed_time(ev1) / 1e3
+    tree = h.tree()
+    internal = tree["is_leaf"] == 0
+    ranks = np.concatenate([tree["rank12"][internal], tree["rank21"][internal]])
+
+    g = torch.Generator(device="cpu").manual_seed(3 + rank)
+    b_host = torch.randn(s, N, generator=g, dtype=torch.float64).pin_memory()  # column-major N x s
+    x_host = torch.empty(s, N, dtype=torch.float64).pin_memory()
+    b = b_host.to(dev)
+    x = torch.empty_like(b)
+
+    def step():
+        h.factor()
+        return h.solve_device(b.data_ptr(), s, N, x.data_ptr(), N)
+
+    def timed(K, fn):
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        out = None
+        for _ in range(K):
+            out = fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / K
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, out
+
+    if args.profile_only:
+        step()
+        H.profile_enable(True)
+        step()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": H.profile_report()}))
+        return
+
+    # ---- mixed precision (headline) ----
+    for _ in range(args.warmup):
+        step()
+    launches0 = H.launch_count()
+    clk = Clocks(local)
+    ms_mixed, st = timed(args.steps, step)
+    clocks = clk.stop()
+    launches = (H.launch_count() - launches0) // max(1, args.steps)
+    mixed_resid, mixed_iters = st.rel_residual, st.ir_iters
+    # separate factor / solve split
+    ms_factor, _ = timed(max(1, args.steps // 2), h.factor)
+    ms_solve, _ = timed(max(1, args.steps // 2),
+                        lambda: h.solve_device(b.data_ptr(), s, N, x.data_ptr(), N))
+
+    # ---- end to end through the C ABI with host buffers ----
+    import ctypes
+
+    def e2e_step():  # host (pinned) b in, host x out: copies inside the timed region
+        h.factor()
+        h._check(h._L.hm_solve(h._h, ctypes.cast(ctypes.c_void_p(b_host.data_ptr()), H._dp), s, N,
+                               ctypes.cast(ctypes.c_void_p(x_host.data_ptr()), H._dp), N, None))
+    for _ in range(1):
+        e2e_step()
+    ms_e2e, _ = timed(args.steps, e2e_step)
+
+    # ---- plain FP64 path on the same operator ----
+    h.set_precision(H.FP64)
+    for _ in range(max(1, args.warmup - 1)):
+        step()
+    ms_fp64, _ = timed(args.steps, step)
+    # FP64 residual against the compressed operator (outside the timed region)
+    y = torch.empty_like(b)
+    h.multiply_device(x.data_ptr(), s, N, y.data_ptr(), N)
+    fp64_resid = float(((b - y).norm(dim=1) / b.norm(dim=1)).max())
+    ms_f64_factor, _ = timed(max(1, args.steps // 2), h.factor)
+
+    # ---- one profiled mixed step: per-kernel CUDA-event times ----
+    h.set_precision(H.MIXED)
+    step()
+    H.profile_enable(True)
+    step()
+    torch.cuda.synchronize()
+    prof = H.profile_report()
+    H.profile_enable(False)
+
+    value = world * s / (ms_mixed / 1e3)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic", "config": workload_config(args),
+        "mixed": {"ms_factor": ms_factor, "ms_solve": ms_solve, "ir_iters": mixed_iters,
+                  "rel_residual": mixed_resid},
+        "fp64": {"ms_per_step": ms_fp64, "ms_factor": ms_f64_factor, "rhs_per_s": world * s / (ms_fp64 / 1e3),
+                 "rel_residual": fp64_resid},
+        "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "build_s": t_build,
+        "ranks": {"min": int(ranks.min()), "median": float(np.median(ranks)), "max": int(ranks.max())},
+        "e2e": {"value": world * s / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": s * N * 8,
+                "d2h_bytes_per_step": s * N * 8},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "profile": {k: {"launches": v[0], "ms": v[1], "flops": v[2], "bytes": v[3]} for k, v in prof.items()},
+    }
+    out["roofline"] = roofline(prof)
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            times, threads = reference_sample(reps=1)
+            t_full, alpha = extrapolate(times, N)
+            out["cpu_baseline"] = {
+                "value": s / t_full, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"HODLRMatrixOMP::solve (factor+solve), 64 RHS, Coulomb 2-D N in {sorted(times)} "
+                          f"(times {[round(times[k], 3) for k in sorted(times)]} s), scaled to N={N} by N^{alpha:.2f}"}
+        except Exception as e:  # the oracle library may be absent
+            out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                   "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def roofline(prof: dict):
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        src = "measured"
+    except Exception:
+        src = "fallback"
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    name, (n, ms, fl, by) = max(prof.items(), key=lambda kv: kv[1][1])
+    achieved = by / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "traffic": None, "peak_source": src,
+            "achieved_tflops": fl / (ms / 1e3) / 1e12 if ms > 0 else 0.0,
+            "note": "SIMT FMA GEMM: the FMA pipe, not HBM, bounds it; see achieved_tflops"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

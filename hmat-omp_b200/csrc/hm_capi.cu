@@ -1,6 +1,7 @@
 // extern "C" entry points of libhmat_b200.so (declared in include/hmat_b200.h).
 // Every call converts C++ exceptions to an HM_* status and keeps the message in the
 // handle for hm_last_error().
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -117,6 +118,14 @@ int hm_set_stream(hm_handle* h, void* stream) {
     });
 }
 
+int hm_set_precision(hm_handle* h, int precision) {
+    return guard(h, [&] {
+        HM_CHECK(precision == HM_FP64 || precision == HM_MIXED, HM_ERR_ARG, "bad precision");
+        h->opts.precision = precision;
+        if (h->eng) h->eng->set_precision(precision);
+    });
+}
+
 int hm_hodlr_build_from_dense_device(hm_handle* h, const double* dA, int N, int lda, int leaf) {
     return guard(h, [&] {
         engine(h, hm::Engine::HODLR).build_dense_device(dA, N, lda, leaf);
@@ -130,6 +139,22 @@ int hm_hodlr_build_from_dense(hm_handle* h, const double* A, int N, int lda, int
         HM_CUDA(cudaMemcpy2DAsync(d.p, (size_t)N * sizeof(double), A, (size_t)lda * sizeof(double),
                                   (size_t)N * sizeof(double), N, cudaMemcpyHostToDevice, h->stream));
         engine(h, hm::Engine::HODLR).build_dense_device(d.p, N, N, leaf);
+        HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int hm_hodlr_build_from_kernel(hm_handle* h, int kernel, const double* points, int dim, int N,
+                               const double* params, int nparams, int leaf) {
+    return guard(h, [&] {
+        HM_CHECK(points && N > 0 && dim >= 1, HM_ERR_ARG, "build_from_kernel: bad arguments");
+        HM_CHECK(nparams >= 2 && params, HM_ERR_ARG, "build_from_kernel: two parameters expected");
+        int gen = kernel == HM_KERNEL_CAUCHY ? hm::GEN_CAUCHY
+                  : kernel == HM_KERNEL_GAUSSIAN ? hm::GEN_GAUSSIAN
+                  : kernel == HM_KERNEL_COULOMB ? hm::GEN_COULOMB : -1;
+        HM_CHECK(gen > 0, HM_ERR_ARG, "build_from_kernel: unknown kernel");
+        HM_CHECK(kernel != HM_KERNEL_CAUCHY || dim == 1, HM_ERR_ARG, "Cauchy points are 1-D");
+        size_t npts = kernel == HM_KERNEL_CAUCHY ? 2 * (size_t)N : (size_t)N * dim;
+        engine(h, hm::Engine::HODLR).build_kernel(gen, points, npts, dim, N, params[0], params[1], leaf);
         HM_CUDA(cudaStreamSynchronize(h->stream));
     });
 }
@@ -174,15 +199,7 @@ int hm_multiply_device(hm_handle* h, const double* dx, int nrhs, int ldx, double
 
 int hm_multiply(hm_handle* h, const double* x, int nrhs, int ldx, double* y, int ldy) {
     return guard(h, [&] {
-        hm::Engine& e = built(h);
-        const int N = e.N();
-        HM_CHECK(x && y && nrhs >= 1 && ldx >= N && ldy >= N, HM_ERR_ARG, "multiply: bad arguments");
-        hm::DBuf<double> dx((size_t)N * nrhs), dy((size_t)N * nrhs);
-        HM_CUDA(cudaMemcpy2DAsync(dx.p, (size_t)N * 8, x, (size_t)ldx * 8, (size_t)N * 8, nrhs,
-                                  cudaMemcpyHostToDevice, h->stream));
-        e.multiply_device(dx.p, nrhs, N, dy.p, N);
-        HM_CUDA(cudaMemcpy2DAsync(y, (size_t)ldy * 8, dy.p, (size_t)N * 8, (size_t)N * 8, nrhs,
-                                  cudaMemcpyDeviceToHost, h->stream));
+        built(h).multiply_device(x, nrhs, ldx, y, ldy);   // host pointers: unified addressing
         HM_CUDA(cudaStreamSynchronize(h->stream));
     });
 }
@@ -198,17 +215,32 @@ int hm_solve_device(hm_handle* h, const double* db, int nrhs, int ldb, double* d
 
 int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ldx, hm_solve_stats* st) {
     return guard(h, [&] {
-        hm::Engine& e = built(h);
-        const int N = e.N();
-        HM_CHECK(b && x && nrhs >= 1 && ldb >= N && ldx >= N, HM_ERR_ARG, "solve: bad arguments");
-        hm::DBuf<double> db((size_t)N * nrhs), dx((size_t)N * nrhs);
-        HM_CUDA(cudaMemcpy2DAsync(db.p, (size_t)N * 8, b, (size_t)ldb * 8, (size_t)N * 8, nrhs,
-                                  cudaMemcpyHostToDevice, h->stream));
-        e.solve_device(db.p, nrhs, N, dx.p, N, st);
-        HM_CUDA(cudaMemcpy2DAsync(x, (size_t)ldx * 8, dx.p, (size_t)N * 8, (size_t)N * 8, nrhs,
-                                  cudaMemcpyDeviceToHost, h->stream));
+        built(h).solve_device(b, nrhs, ldb, x, ldx, st);    // host pointers: unified addressing
         HM_CUDA(cudaStreamSynchronize(h->stream));
     });
+}
+
+void hm_profile_enable(int on) {
+    hm::Profiler& p = hm::Profiler::get();
+    p.enabled = on != 0;
+    p.reset();
+}
+
+long long hm_launch_count(void) { return hm::Profiler::get().launches; }
+
+size_t hm_profile_report(char* buf, size_t len) {
+    std::string r;
+    try {
+        r = hm::Profiler::get().report();
+    } catch (const std::exception& e) {
+        r = std::string("{\"error\": \"") + e.what() + "\"}";
+    }
+    if (buf && len) {
+        size_t n = std::min(len - 1, r.size());
+        std::memcpy(buf, r.data(), n);
+        buf[n] = 0;
+    }
+    return r.size() + 1;
 }
 
 }  // extern "C"

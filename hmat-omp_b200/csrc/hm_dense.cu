@@ -18,6 +18,74 @@
 namespace hm {
 
 // ---------------------------------------------------------------------------------
+// Profiler and plan execution
+// ---------------------------------------------------------------------------------
+Profiler& Profiler::get() {
+    static Profiler p;
+    return p;
+}
+
+cudaEvent_t Profiler::event() {
+    if (!pool.empty()) {
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    HM_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void Profiler::reset() {
+    for (auto& r : recs) {
+        pool.push_back(r.a);
+        pool.push_back(r.b);
+    }
+    recs.clear();
+}
+
+std::string Profiler::report() {
+    struct Agg { long long n = 0; double ms = 0, flops = 0, bytes = 0; };
+    std::vector<std::pair<std::string, Agg>> agg;
+    for (auto& r : recs) {
+        HM_CUDA(cudaEventSynchronize(r.b));
+        float ms = 0;
+        HM_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        auto it = std::find_if(agg.begin(), agg.end(), [&](auto& x) { return x.first == r.name; });
+        if (it == agg.end()) { agg.push_back({r.name, Agg{}}); it = agg.end() - 1; }
+        it->second.n += r.launches;
+        it->second.ms += ms;
+        it->second.flops += r.flops;
+        it->second.bytes += r.bytes;
+    }
+    std::string out = "{";
+    char buf[256];
+    for (size_t i = 0; i < agg.size(); ++i) {
+        snprintf(buf, sizeof buf, "%s\"%s\": [%lld, %.6f, %.6e, %.6e]", i ? ", " : "", agg[i].first.c_str(),
+                 agg[i].second.n, agg[i].second.ms, agg[i].second.flops, agg[i].second.bytes);
+        out += buf;
+    }
+    return out + "}";
+}
+
+void Plan::run(cudaStream_t s, int* status) const {
+    Profiler& P = Profiler::get();
+    for (auto& st : steps_) {
+        const int nl = st->nlaunch();
+        if (P.enabled && nl > 0) {
+            Profiler::Rec r{st->name(), P.event(), P.event(), st->flops(), st->bytes(), nl};
+            HM_CUDA(cudaEventRecord(r.a, s));
+            st->run(s, status);
+            HM_CUDA(cudaEventRecord(r.b, s));
+            P.recs.push_back(r);
+        } else {
+            st->run(s, status);
+        }
+        P.launches += nl;
+    }
+}
+
+// ---------------------------------------------------------------------------------
 // Gauss-Jordan inverse
 // ---------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) gj_inverse_kernel(const GJDesc* __restrict__ descs, int* status) {

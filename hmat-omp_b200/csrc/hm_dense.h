@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <memory>
+#include <string>
 
 #include "hm_gemm.h"
 
@@ -99,17 +100,39 @@ void launch_permute(const DevTable<PermDesc>& t, cudaStream_t s);
 void launch_copy(const DevTable<CopyDesc>& t, cudaStream_t s);
 void launch_ident(const DevTable<IdentDesc>& t, cudaStream_t s);
 
+// Process-wide launch counter and optional per-step CUDA-event timing.
+struct Profiler {
+    struct Rec {
+        std::string name;
+        cudaEvent_t a, b;
+        double flops, bytes;
+        int launches;
+    };
+    bool enabled = false;
+    long long launches = 0;
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    static Profiler& get();
+    cudaEvent_t event();
+    void reset();
+    // {"name": [launches, ms, flops, bytes], ...} (synchronises)
+    std::string report();
+};
+inline void count_launch(int n = 1) { Profiler::get().launches += n; }
+
 // A recorded sequence of batched launches (the unit that is replayed or captured).
 class Plan {
   public:
     struct Step {
         virtual ~Step() = default;
         virtual void run(cudaStream_t s, int* status) const = 0;
+        virtual const char* name() const = 0;
+        virtual int nlaunch() const { return 1; }
+        virtual double flops() const { return 0; }
+        virtual double bytes() const { return 0; }
     };
     void add(std::unique_ptr<Step> st) { steps_.push_back(std::move(st)); }
-    void run(cudaStream_t s, int* status) const {
-        for (auto& st : steps_) st->run(s, status);
-    }
+    void run(cudaStream_t s, int* status) const;
     bool empty() const { return steps_.empty(); }
     // device scratch owned by the plan (bump-allocated from large chunks)
     double* scratch(size_t count) { return static_cast<double*>(bump(count * sizeof(double))); }
@@ -146,37 +169,80 @@ struct GemmStep : Plan::Step {
     GenParams gp;
     explicit GemmStep(int cfg = CFG_64x64, int gen = GEN_DENSE) : batch(cfg, gen) {}
     void run(cudaStream_t s, int*) const override { batch.launch(s, gp); }
+    const char* name() const override {
+        if (batch.gen() != GEN_DENSE) return "gemm_kernel_gen_f64";
+        return sizeof(T) == 8 ? "gemm_f64" : "gemm_f32";
+    }
+    int nlaunch() const override { return batch.nlaunch(); }
+    double flops() const override { return batch.flops(); }
+    double bytes() const override { return batch.bytes(); }
 };
 
 struct GJStep : Plan::Step {
     DevTable<GJDesc> t;
     void run(cudaStream_t s, int* st) const override { launch_gj(t, st, s); }
+    const char* name() const override { return "gauss_jordan_inverse"; }
+    double flops() const override {
+        double f = 0;
+        for (auto& d : t.h) f += 2.0 * d.n * d.n * (double)d.n;
+        return f;
+    }
+    double bytes() const override {
+        double b = 0;
+        for (auto& d : t.h) b += 16.0 * d.n * d.n;
+        return b;
+    }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
 };
 struct EigStep : Plan::Step {
     DevTable<EigDesc> t;
     void run(cudaStream_t s, int* st) const override { launch_jacobi(t, st, s); }
+    const char* name() const override { return "jacobi_eigen"; }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
 };
 struct PrepStep : Plan::Step {
     DevTable<PrepDesc> t;
     double tol = 0;
     int max_rank = 0;
     void run(cudaStream_t s, int*) const override { launch_prep(t, tol, max_rank, s); }
+    const char* name() const override { return "sort_rank"; }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
 };
 struct NormStep : Plan::Step {
     DevTable<NormDesc> t;
     void run(cudaStream_t s, int*) const override { launch_norms(t, s); }
+    const char* name() const override { return "column_norms"; }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
 };
 struct PermStep : Plan::Step {
     DevTable<PermDesc> t;
     void run(cudaStream_t s, int*) const override { launch_permute(t, s); }
+    const char* name() const override { return "permute_scale"; }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
+};
+struct GenFillStep : Plan::Step {
+    DevTable<GenFillDesc> t;
+    int gen = GEN_DENSE;
+    GenParams gp;
+    void run(cudaStream_t s, int*) const override {
+        int mx = 0;
+        for (auto& d : t.h) mx = std::max(mx, d.rows * d.cols);
+        launch_gen_fill(t.d.p, t.size(), mx, gen, gp, s);
+    }
+    const char* name() const override { return "kernel_fill"; }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
 };
 struct CopyStep : Plan::Step {
     DevTable<CopyDesc> t;
     void run(cudaStream_t s, int*) const override { launch_copy(t, s); }
+    const char* name() const override { return "copy"; }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
 };
 struct IdentStep : Plan::Step {
     DevTable<IdentDesc> t;
     void run(cudaStream_t s, int*) const override { launch_ident(t, s); }
+    const char* name() const override { return "identity_fill"; }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
 };
 
 // X_i = inv(A_i) for a batch of square FP64 matrices of any size (X may not alias A

@@ -228,12 +228,13 @@ struct Block {
 };
 }  // namespace
 
-void Engine::build_dense_device(const double* dA, int N, int lda, int leaf) {
-    HM_CHECK(N > 0 && leaf > 0 && lda >= N && dA, HM_ERR_ARG, "build_from_dense: bad arguments");
+void Engine::begin_build(int N, int leaf) {
+    HM_CHECK(N > 0 && leaf > 0, HM_ERR_ARG, "build: N and leaf_size must be positive");
     N_ = N;
     leaf_ = leaf;
     built_ = factored_ = false;
     f64_.ready = f32_.ready = false;
+    dDinv.release();
     mv_plans_.clear();
     solve64_plans_.clear();
     solve32_plans_.clear();
@@ -241,29 +242,77 @@ void Engine::build_dense_device(const double* dA, int N, int lda, int leaf) {
     plan_levels();
     if (!dstatus.p) dstatus.alloc(1);
     dstatus.zero(stream_);
+}
+
+void Engine::build_dense_device(const double* dA, int N, int lda, int leaf) {
+    HM_CHECK(N > 0 && leaf > 0 && lda >= N && dA, HM_ERR_ARG, "build_from_dense: bad arguments");
+    begin_build(N, leaf);
     {   // reject non-finite input before any compression
-        DevTable<CopyDesc> none;
-        (void)none;
-        for (int j = 0; j < N; j += 4096) {
-            const int cols = std::min(4096, N - j);
-            // columns j..j+cols are contiguous only when lda == N; check column by column otherwise
-            if (lda == N) {
-                const size_t cnt = (size_t)N * cols;
-                nonfinite_kernel<<<grid_for(cnt), 256, 0, stream_>>>(dA + (size_t)j * lda, cnt, dstatus.p);
-            } else {
-                for (int c = 0; c < cols; ++c)
-                    nonfinite_kernel<<<grid_for(N), 256, 0, stream_>>>(dA + (size_t)(j + c) * lda, N, dstatus.p);
-            }
+        if (lda == N) {
+            const size_t cnt = (size_t)N * N;
+            nonfinite_kernel<<<grid_for(cnt), 256, 0, stream_>>>(dA, cnt, dstatus.p);
+        } else {
+            for (int c = 0; c < N; ++c)
+                nonfinite_kernel<<<grid_for(N), 256, 0, stream_>>>(dA + (size_t)c * lda, N, dstatus.p);
         }
         HM_CUDA(cudaGetLastError());
         check_status("build_from_dense: input");
     }
-    if (kind_ == HODLR) build_hodlr(dA, lda);
-    else build_hss(dA, lda);
+    Source src;
+    src.dA = dA;
+    src.lda = lda;
+    if (kind_ == HODLR) build_hodlr(src);
+    else build_hss(src);
     built_ = true;
 }
 
-void Engine::build_hodlr(const double* dA, int lda) {
+void Engine::build_kernel(int gen, const double* pts, size_t npts, int dim, int N, double p0, double p1,
+                          int leaf) {
+    HM_CHECK(gen == GEN_CAUCHY || gen == GEN_GAUSSIAN || gen == GEN_COULOMB, HM_ERR_ARG, "unknown kernel");
+    HM_CHECK(pts && dim >= 1 && dim <= 3, HM_ERR_ARG, "build_from_kernel: bad points");
+    for (size_t i = 0; i < npts; ++i)
+        HM_CHECK(std::isfinite(pts[i]), HM_ERR_NONFINITE, "build_from_kernel: non-finite point");
+    begin_build(N, leaf);
+    dPts.alloc(npts);
+    HM_CUDA(cudaMemcpyAsync(dPts.p, pts, npts * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    Source src;
+    src.gen = gen;
+    src.gp.pts = dPts.p;
+    src.gp.N = N;
+    src.gp.dim = dim;
+    src.gp.p0 = p0;
+    src.gp.p1 = p1;
+    if (kind_ == HODLR) build_hodlr(src);
+    else build_hss(src);
+    built_ = true;
+}
+
+void Engine::add_block_fill(Plan& plan, const Source& src,
+                            const std::vector<std::tuple<int, int, int, int, int, double*, int>>& blocks) {
+    // (r0, c0, rows, cols, trans, dst, ldd): dst = trans ? A[r0.., c0..]^T : A[r0.., c0..]
+    if (blocks.empty()) return;
+    if (src.dense()) {
+        auto cp = std::make_unique<CopyStep>();
+        for (auto& b : blocks) {
+            auto [r0, c0, rows, cols, trans, dst, ldd] = b;
+            cp->t.h.push_back({src.blk(r0, c0), src.lda, dst, ldd, rows, cols, trans, 0, 0});
+        }
+        cp->t.upload(stream_);
+        plan.add(std::move(cp));
+    } else {
+        auto gf = std::make_unique<GenFillStep>();
+        gf->gen = src.gen;
+        gf->gp = src.gp;
+        for (auto& b : blocks) {
+            auto [r0, c0, rows, cols, trans, dst, ldd] = b;
+            gf->t.h.push_back({r0, c0, rows, cols, trans, dst, ldd});
+        }
+        gf->t.upload(stream_);
+        plan.add(std::move(gf));
+    }
+}
+
+void Engine::build_hodlr(const Source& src) {
     const int kguess = opts_.rsvd_rank + opts_.oversample;
     HM_CHECK(opts_.rsvd_rank >= 0 && opts_.oversample >= 0, HM_ERR_ARG, "bad rsvd_rank/oversample");
     // blocks in the reference's serial post-order (hodlr_routines.h:43-53)
@@ -297,14 +346,16 @@ void Engine::build_hodlr(const double* dA, int lda) {
     alloc_bases();
     // leaf blocks D (hodlr_routines.h:32-34)
     {
-        CopyStep cp;
+        Plan lp;
+        std::vector<std::tuple<int, int, int, int, int, double*, int>> fill;
         for (int l : leaves_) {
             const Node& n = nodes_[l];
-            cp.t.h.push_back({dA + n.start + (size_t)n.start * lda, lda, dD.p + n.offD, n.len(),
-                              n.len(), n.len(), 0, 0, 0});
+            fill.emplace_back(n.start, n.start, n.len(), n.len(), 0, dD.p + n.offD, n.len());
+            if (fill.size() == 60000) { add_block_fill(lp, src, fill); fill.clear(); }
         }
-        cp.t.upload(stream_);
-        cp.run(stream_, dstatus.p);
+        add_block_fill(lp, src, fill);
+        lp.run(stream_, dstatus.p);
+        HM_CUDA(cudaStreamSynchronize(stream_));
     }
     // sketches
     size_t omega_total = 0;
@@ -357,13 +408,13 @@ void Engine::build_hodlr(const double* dA, int lda) {
         for (auto* b : lvl) (b->rsvd ? rs : fs).push_back(b);
         // ---- full SVDs (compression.h:18-64) on the tall orientation ----
         if (!fs.empty()) {
-            auto cp = std::make_unique<CopyStep>();
+            std::vector<std::tuple<int, int, int, int, int, double*, int>> fill;
             std::vector<SvdProblem> sv;
             for (auto* b : fs) {
                 const bool tall = b->m >= b->n;
                 const int rows = tall ? b->m : b->n, p = tall ? b->n : b->m;
                 double* X = plan.scratch((size_t)rows * p);
-                cp->t.h.push_back({dA + b->r0 + (size_t)b->c0 * lda, lda, X, rows, rows, p, tall ? 0 : 1, 0, 0});
+                fill.emplace_back(b->r0, b->c0, rows, p, tall ? 0 : 1, X, rows);
                 Node& cr = nodes_[b->crow];
                 Node& cc = nodes_[b->ccol];
                 double* Uo = dU.p + cr.offU;
@@ -377,15 +428,19 @@ void Engine::build_hodlr(const double* dA, int lda) {
                 else { q.L = Vo; q.ldl = cc.len(); q.R = Uo; q.ldr = cr.len(); }
                 sv.push_back(q);
             }
-            cp->t.upload(stream_);
-            plan.add(std::move(cp));
+            add_block_fill(plan, src, fill);
             plan_gram_svd(plan, sv, opts_.tol, opts_.max_rank, stream_);
         }
         // ---- randomized SVDs (compression.h:67-99) ----
         if (!rs.empty()) {
             struct W { double *Y, *Q, *X, *Ub; };
             std::vector<W> ws(rs.size());
-            auto gY = std::make_unique<GemmStep<double>>();
+            auto mkA = [&]() {
+                auto g = std::make_unique<GemmStep<double>>(CFG_64x64, src.gen);
+                g->gp = src.gp;
+                return g;
+            };
+            auto gY = mkA();
             for (size_t i = 0; i < rs.size(); ++i) {
                 Block* b = rs[i];
                 ws[i].Y = plan.scratch((size_t)b->m * b->k);
@@ -393,8 +448,8 @@ void Engine::build_hodlr(const double* dA, int lda) {
                 ws[i].X = plan.scratch((size_t)b->n * b->k);
                 ws[i].Ub = plan.scratch((size_t)b->k * b->k);
                 // Y = A_blk Omega  (compression.h:79)
-                gY->batch.add(b->m, b->k, b->n, 1.0, dA + b->r0 + (size_t)b->c0 * lda, lda, OP_N,
-                              dOmega.p + b->omega, b->n, OP_N, 0.0, ws[i].Y, b->m);
+                gY->batch.add(b->m, b->k, b->n, 1.0, src.blk(b->r0, b->c0), src.lda, OP_N,
+                              dOmega.p + b->omega, b->n, OP_N, 0.0, ws[i].Y, b->m, nullptr, 0, b->r0, b->c0);
             }
             gY->batch.finalize(stream_);
             plan.add(std::move(gY));
@@ -412,11 +467,11 @@ void Engine::build_hodlr(const double* dA, int lda) {
             };
             orthY();  // Q = orthonormal basis of range(Y)  (compression.h:83-84)
             for (int it = 0; it < opts_.power_iters; ++it) {  // extension
-                auto gZ = std::make_unique<GemmStep<double>>();
+                auto gZ = mkA();
                 for (size_t i = 0; i < rs.size(); ++i) {
                     Block* b = rs[i];
-                    gZ->batch.add(b->n, b->k, b->m, 1.0, dA + b->r0 + (size_t)b->c0 * lda, lda, OP_T,
-                                  ws[i].Q, b->m, OP_N, 0.0, ws[i].X, b->n);
+                    gZ->batch.add(b->n, b->k, b->m, 1.0, src.blk(b->r0, b->c0), src.lda, OP_T,
+                                  ws[i].Q, b->m, OP_N, 0.0, ws[i].X, b->n, nullptr, 0, b->r0, b->c0);
                 }
                 gZ->batch.finalize(stream_);
                 plan.add(std::move(gZ));
@@ -429,22 +484,22 @@ void Engine::build_hodlr(const double* dA, int lda) {
                     sv.push_back(q);
                 }
                 plan_gram_svd(plan, sv, opts_.tol, 0, stream_);
-                auto gY2 = std::make_unique<GemmStep<double>>();
+                auto gY2 = mkA();
                 for (size_t i = 0; i < rs.size(); ++i) {
                     Block* b = rs[i];
-                    gY2->batch.add(b->m, b->k, b->n, 1.0, dA + b->r0 + (size_t)b->c0 * lda, lda, OP_N,
-                                   ws[i].X, b->n, OP_N, 0.0, ws[i].Y, b->m);
+                    gY2->batch.add(b->m, b->k, b->n, 1.0, src.blk(b->r0, b->c0), src.lda, OP_N,
+                                   ws[i].X, b->n, OP_N, 0.0, ws[i].Y, b->m, nullptr, 0, b->r0, b->c0);
                 }
                 gY2->batch.finalize(stream_);
                 plan.add(std::move(gY2));
                 orthY();
             }
             // X = A_blk^T Q = (Q^T A_blk)^T  (compression.h:87)
-            auto gX = std::make_unique<GemmStep<double>>();
+            auto gX = mkA();
             for (size_t i = 0; i < rs.size(); ++i) {
                 Block* b = rs[i];
-                gX->batch.add(b->n, b->k, b->m, 1.0, dA + b->r0 + (size_t)b->c0 * lda, lda, OP_T,
-                              ws[i].Q, b->m, OP_N, 0.0, ws[i].X, b->n);
+                gX->batch.add(b->n, b->k, b->m, 1.0, src.blk(b->r0, b->c0), src.lda, OP_T,
+                              ws[i].Q, b->m, OP_N, 0.0, ws[i].X, b->n, nullptr, 0, b->r0, b->c0);
             }
             gX->batch.finalize(stream_);
             plan.add(std::move(gX));
@@ -518,7 +573,7 @@ void Engine::build_hodlr(const double* dA, int lda) {
     HM_CUDA(cudaStreamSynchronize(stream_));
 }
 
-void Engine::build_hss(const double*, int) {
+void Engine::build_hss(const Source&) {
     throw Error(HM_ERR_UNSUPPORTED, "HSS build not available in this build");
 }
 
@@ -530,17 +585,7 @@ void Engine::import_hodlr(int N, int leaf, const int* r12, const int* r21, const
                           const double* const* B21) {
     HM_CHECK(kind_ == HODLR, HM_ERR_STATE, "import is for HODLR handles");
     HM_CHECK(N > 0 && leaf > 0 && r12 && r21 && D && U && V && B12 && B21, HM_ERR_ARG, "import: bad arguments");
-    N_ = N;
-    leaf_ = leaf;
-    built_ = factored_ = false;
-    f64_.ready = f32_.ready = false;
-    mv_plans_.clear();
-    solve64_plans_.clear();
-    solve32_plans_.clear();
-    nodes_ = hodlr_tree(N, leaf);
-    plan_levels();
-    if (!dstatus.p) dstatus.alloc(1);
-    dstatus.zero(stream_);
+    begin_build(N, leaf);
     for (size_t i = 0; i < nodes_.size(); ++i) {
         Node& n = nodes_[i];
         if (n.is_leaf) continue;
@@ -618,8 +663,8 @@ void Engine::factor_t(FactorStore<T>& fs) {
         if (n.is_leaf) totD = std::max(totD, n.offD + (size_t)n.len() * n.len());
     }
     Plan plan;
-    if (!dDinv.p) {  // FP64 leaf inverses, shared by both precisions
-        dDinv.alloc(totD);
+    {   // FP64 leaf inverses
+        if (dDinv.n < totD) dDinv.alloc(totD);
         std::vector<InvProblem> inv;
         for (int l : leaves_) {
             const Node& n = nodes_[l];
@@ -627,20 +672,18 @@ void Engine::factor_t(FactorStore<T>& fs) {
         }
         plan_inverse(plan, inv, s);
     }
-    if (!dMinv.p || sizeM_ != offM) {
-        dMinv.alloc(std::max<size_t>(offM, 1));
-        sizeM_ = offM;
-    }
-    fs.Q.alloc(totU);
-    fs.P.alloc(std::max<size_t>(offP, 1));
+    if (dMinv.n < std::max<size_t>(offM, 1)) dMinv.alloc(std::max<size_t>(offM, 1));
+    sizeM_ = offM;
+    if (fs.Q.n < totU) fs.Q.alloc(totU);
+    if (fs.P.n < std::max<size_t>(offP, 1)) fs.P.alloc(std::max<size_t>(offP, 1));
     sizeP_ = offP;
     const T* Dinv;
     const T* Vt;
     const T* Ut;
     DBuf<T> Utmp;
     if constexpr (F32) {
-        fs.Dinv.alloc(totD);
-        fs.V.alloc(totV);
+        if (fs.Dinv.n < totD) fs.Dinv.alloc(totD);
+        if (fs.V.n < totV) fs.V.alloc(totV);
         Utmp.alloc(totU);
         auto cp = std::make_unique<CopyStep>();
         cp->t.h.push_back(flat_copy(dDinv.p, false, fs.Dinv.p, true, totD));
@@ -774,10 +817,12 @@ void Engine::factor_t(FactorStore<T>& fs) {
     fs.ready = true;
 }
 
+// Recomputes every time it is called (a rebuild or a new operator needs no flag).
 void Engine::factor() {
     HM_CHECK(built_, HM_ERR_STATE, "factor before build");
-    if (!f64_.ready) factor_t<double>(f64_);
-    if (opts_.precision == HM_MIXED && !f32_.ready) factor_t<float>(f32_);
+    factored_ = false;
+    if (opts_.precision == HM_MIXED) factor_t<float>(f32_);
+    else factor_t<double>(f64_);
     factored_ = true;
 }
 
@@ -792,6 +837,7 @@ void Engine::ensure_io(int s) {
     ioR.alloc(n);
     ioXf.alloc(n);
     ioYf.alloc(n);
+    ioNorm.alloc(2 * (size_t)s);
     io_cols_ = s;
     mv_plans_.clear();
     solve64_plans_.clear();
@@ -920,9 +966,14 @@ Plan& Engine::solve_plan<float>(FactorStore<float>& fs, int s) {
     return pl;
 }
 
+// Host or device source/destination (unified addressing decides the direction).
 static void copy_in(double* dst, const double* src, int N, int s, int ld, cudaStream_t st) {
     HM_CUDA(cudaMemcpy2DAsync(dst, (size_t)N * sizeof(double), src, (size_t)ld * sizeof(double),
-                              (size_t)N * sizeof(double), s, cudaMemcpyDeviceToDevice, st));
+                              (size_t)N * sizeof(double), s, cudaMemcpyDefault, st));
+}
+static void copy_out(double* dst, int ld, const double* src, int N, int s, cudaStream_t st) {
+    HM_CUDA(cudaMemcpy2DAsync(dst, (size_t)ld * sizeof(double), src, (size_t)N * sizeof(double),
+                              (size_t)N * sizeof(double), s, cudaMemcpyDefault, st));
 }
 
 void Engine::multiply_device(const double* dx, int s, int ldx, double* dy, int ldy) {
@@ -931,16 +982,14 @@ void Engine::multiply_device(const double* dx, int s, int ldx, double* dy, int l
     ensure_io(s);
     copy_in(ioX.p, dx, N_, s, ldx, stream_);
     matvec_plan(s).run(stream_, dstatus.p);
-    HM_CUDA(cudaMemcpy2DAsync(dy, (size_t)ldy * sizeof(double), ioY.p, (size_t)N_ * sizeof(double),
-                              (size_t)N_ * sizeof(double), s, cudaMemcpyDeviceToDevice, stream_));
+    copy_out(dy, ldy, ioY.p, N_, s, stream_);
 }
 
 void Engine::solve_fp64(const double* db, int s, int ldb, double* dx, int ldx) {
     ensure_io(s);
     copy_in(ioX.p, db, N_, s, ldb, stream_);
     solve_plan<double>(f64_, s).run(stream_, dstatus.p);
-    HM_CUDA(cudaMemcpy2DAsync(dx, (size_t)ldx * sizeof(double), ioY.p, (size_t)N_ * sizeof(double),
-                              (size_t)N_ * sizeof(double), s, cudaMemcpyDeviceToDevice, stream_));
+    copy_out(dx, ldx, ioY.p, N_, s, stream_);
 }
 
 // Mixed precision: FP32 factor sweeps, refined against the FP64 operator
@@ -948,11 +997,12 @@ void Engine::solve_fp64(const double* db, int s, int ldb, double* dx, int ldx) {
 void Engine::solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st) {
     ensure_io(s);
     cudaStream_t q = stream_;
-    // ioR holds b, ioY x, ioX the matvec input (x), ioYf the correction.
-    DBuf<double> norms(2 * (size_t)s);
-    DBuf<double> bcopy((size_t)N_ * s);
-    copy_in(bcopy.p, db, N_, s, ldb, q);
-    to_float_kernel<<<grid_for((size_t)N_ * s), 256, 0, q>>>(bcopy.p, ioXf.p, (size_t)N_ * s);
+    // ioR = b, ioX = x (also the matvec input), ioY = A x then r, ioXf = float(r),
+    // ioYf = the FP32 correction.
+    double* bcopy = ioR.p;
+    copy_in(bcopy, db, N_, s, ldb, q);
+    to_float_kernel<<<grid_for((size_t)N_ * s), 256, 0, q>>>(bcopy, ioXf.p, (size_t)N_ * s);
+    count_launch();
     Plan& sp = solve_plan<float>(f32_, s);
     Plan& mp = matvec_plan(s);
     std::vector<double> hn(2 * (size_t)s);
@@ -961,11 +1011,13 @@ void Engine::solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, 
     for (; it < std::max(1, opts_.ir_max_iter); ++it) {
         sp.run(q, dstatus.p);                                   // ioYf = A32^{-1} r
         accumulate_kernel<<<grid_for((size_t)N_ * s), 256, 0, q>>>(ioX.p, ioYf.p, (size_t)N_ * s, it == 0);
+        count_launch();
         mp.run(q, dstatus.p);                                   // ioY = A64 x
-        norms.zero(q);
+        HM_CUDA(cudaMemsetAsync(ioNorm.p, 0, 2 * (size_t)s * sizeof(double), q));
         residual_kernel<<<dim3(std::min(64, ceil_div(N_, 256)), s), 256, 0, q>>>(
-            bcopy.p, ioY.p, ioXf.p, N_, s, norms.p, norms.p + s);  // ioY = b - A x, ioXf = float(r)
-        HM_CUDA(cudaMemcpyAsync(hn.data(), norms.p, 2 * s * sizeof(double), cudaMemcpyDeviceToHost, q));
+            bcopy, ioY.p, ioXf.p, N_, s, ioNorm.p, ioNorm.p + s);  // ioY = b - A x, ioXf = float(r)
+        count_launch();
+        HM_CUDA(cudaMemcpyAsync(hn.data(), ioNorm.p, 2 * s * sizeof(double), cudaMemcpyDeviceToHost, q));
         HM_CUDA(cudaStreamSynchronize(q));
         worst = 0.0;
         for (int j = 0; j < s; ++j) {
@@ -976,8 +1028,7 @@ void Engine::solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, 
         if (!(worst == worst)) break;  // NaN
         if (worst <= opts_.ir_tol) { ++it; break; }
     }
-    HM_CUDA(cudaMemcpy2DAsync(dx, (size_t)ldx * sizeof(double), ioX.p, (size_t)N_ * sizeof(double),
-                              (size_t)N_ * sizeof(double), s, cudaMemcpyDeviceToDevice, q));
+    copy_out(dx, ldx, ioX.p, N_, s, q);
     HM_CUDA(cudaStreamSynchronize(q));
     if (st) {
         st->ir_iters = it;

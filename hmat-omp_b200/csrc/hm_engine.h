@@ -34,6 +34,17 @@ struct Node {
 std::vector<Node> hodlr_tree(int N, int leaf);
 std::vector<Node> hss_tree(int N, int leaf);
 
+// Where the operator's entries come from during a build: a dense device matrix, or a
+// kernel generator evaluated from point coordinates (matrix-free).
+struct Source {
+    const double* dA = nullptr;
+    int lda = 0;
+    int gen = GEN_DENSE;
+    GenParams gp;
+    bool dense() const { return gen == GEN_DENSE; }
+    const double* blk(int r0, int c0) const { return dense() ? dA + r0 + (size_t)c0 * lda : nullptr; }
+};
+
 // Per-precision factorization storage.
 template <typename T>
 struct FactorStore {
@@ -55,10 +66,17 @@ class Engine {
     const std::vector<Node>& nodes() const { return nodes_; }
 
     void set_stream(cudaStream_t s) { stream_ = s; }
+    void set_precision(int p) {
+        if (p != opts_.precision) factored_ = false;
+        opts_.precision = p;
+    }
     cudaStream_t stream() const { return stream_; }
 
     // builds
     void build_dense_device(const double* dA, int N, int lda, int leaf);
+    // Matrix-free build: points (host) in the layout GenParams documents.
+    void build_kernel(int gen, const double* pts_host, size_t npts, int dim, int N, double p0, double p1,
+                      int leaf);
     void import_hodlr(int N, int leaf, const int* r12, const int* r21, const double* const* D,
                       const double* const* U, const double* const* V, const double* const* B12,
                       const double* const* B21);
@@ -74,11 +92,12 @@ class Engine {
   protected:
     void plan_levels();
     void alloc_bases();
-    void build_hodlr(const double* dA, int lda);
-    void build_hss(const double* dA, int lda);
-    void finish_build_hodlr(const std::vector<int>& rank12, const std::vector<int>& rank21,
-                            const std::vector<double>& sig12, const std::vector<double>& sig21,
-                            const std::vector<size_t>& sig_off);
+    void begin_build(int N, int leaf);
+    void build_hodlr(const Source& src);
+    void build_hss(const Source& src);
+    // Append steps materialising blocks (dense copy or generator fill).
+    void add_block_fill(Plan& plan, const Source& src,
+                        const std::vector<std::tuple<int, int, int, int, int, double*, int>>& blocks);
     void check_status(const char* what);
     template <typename T> void factor_t(FactorStore<T>& fs);
     template <typename T> Plan& solve_plan(FactorStore<T>& fs, int s);
@@ -98,6 +117,7 @@ class Engine {
     // FP64 operator storage
     DBuf<double> dD, dU, dV, dB;
     DBuf<int> dstatus;
+    DBuf<double> dPts;             // generator points (matrix-free builds)
     bool built_ = false;
     // factorizations
     FactorStore<double> f64_;
@@ -106,7 +126,7 @@ class Engine {
     size_t sizeM_ = 0, sizeP_ = 0;
     bool factored_ = false;
     // I/O staging buffers (ld = N)
-    DBuf<double> ioX, ioY, ioR;
+    DBuf<double> ioX, ioY, ioR, ioNorm;
     DBuf<float> ioXf, ioYf;
     int io_cols_ = 0;
     std::map<int, Plan> mv_plans_, solve64_plans_, solve32_plans_;

@@ -197,6 +197,32 @@ __global__ void zero_regions_kernel(const ZeroRegion<T>* __restrict__ z, int cou
     }
 }
 
+template <int GEN>
+__global__ void gen_fill_kernel(const GenFillDesc* __restrict__ descs, GenParams gp) {
+    const GenFillDesc d = descs[blockIdx.y];
+    const size_t total = (size_t)d.rows * d.cols;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e % d.rows), j = (int)(e / d.rows);
+        d.dst[i + (size_t)j * d.ldd] =
+            d.trans ? gen_entry<GEN>(gp, d.r0 + j, d.c0 + i) : gen_entry<GEN>(gp, d.r0 + i, d.c0 + j);
+    }
+}
+
+void launch_gen_fill(const GenFillDesc* d_descs, int count, int max_elems, int gen, const GenParams& gp,
+                     cudaStream_t s) {
+    if (count <= 0) return;
+    HM_CHECK(count <= 65535, HM_ERR_UNSUPPORTED, "generator fill batch too large");
+    dim3 grid((unsigned)std::min(std::max(1, (max_elems + 255) / 256), 2048), (unsigned)count);
+    switch (gen) {
+        case GEN_CAUCHY: gen_fill_kernel<GEN_CAUCHY><<<grid, 256, 0, s>>>(d_descs, gp); break;
+        case GEN_GAUSSIAN: gen_fill_kernel<GEN_GAUSSIAN><<<grid, 256, 0, s>>>(d_descs, gp); break;
+        case GEN_COULOMB: gen_fill_kernel<GEN_COULOMB><<<grid, 256, 0, s>>>(d_descs, gp); break;
+        default: throw Error(HM_ERR_ARG, "unknown kernel generator");
+    }
+    HM_CUDA(cudaGetLastError());
+}
+
 // ---------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------
@@ -245,9 +271,13 @@ void GemmBatch<T>::add(int m, int n, int k, T alpha, const T* A, int lda, int op
 template <typename T>
 void GemmBatch<T>::finalize(cudaStream_t s) {
     int t = 0;
+    flops_ = bytes_ = 0;
     for (auto& d : h_) {
         d.tile0 = t;
         t += d.tiles_m * d.tiles_n * d.ksplit;
+        flops_ += 2.0 * d.m * (double)d.n * d.k;
+        const double a = (gen_ == GEN_DENSE) ? (double)d.m * d.k : 0.0;
+        bytes_ += sizeof(T) * (a + (double)d.k * d.n + (double)d.m * d.n * (d.beta != T(0) ? 2 : 1));
     }
     total_tiles_ = t;
     if (!h_.empty()) {

@@ -48,6 +48,15 @@ struct GemmDesc {
     int ga_r0, ga_c0;  // generated A: origin of the block in the global operator
 };
 
+// Materialise a block of a generated operator: dst(i,j) = trans ? G(r0+j, c0+i) : G(r0+i, c0+j)
+struct GenFillDesc {
+    int r0, c0, rows, cols, trans;
+    double* dst;
+    int ldd;
+};
+void launch_gen_fill(const GenFillDesc* d_descs, int count, int max_elems, int gen, const GenParams& gp,
+                     cudaStream_t s);
+
 // Tile configurations.
 enum : int { CFG_64x64 = 0, CFG_N_SKINNY = 1 };
 
@@ -66,6 +75,11 @@ class GemmBatch {
     void launch(cudaStream_t s, const GenParams& gp = GenParams()) const;
     void clear();
     int cfg() const { return cfg_; }
+    int gen() const { return gen_; }
+    int nlaunch() const { return h_.empty() ? 0 : (hz_.empty() ? 1 : 2); }
+    // algorithmic work of one launch: 2mnk flops; operand and result bytes
+    double flops() const { return flops_; }
+    double bytes() const { return bytes_; }
 
   private:
     int cfg_, gen_;
@@ -76,6 +90,7 @@ class GemmBatch {
     DBuf<ZeroRegion<T>> dz_;
     int total_tiles_ = 0;
     bool finalized_ = false;
+    double flops_ = 0, bytes_ = 0;
 };
 
 }  // namespace hm

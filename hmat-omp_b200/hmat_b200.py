@@ -73,6 +73,8 @@ def load() -> C.CDLL:
     L.hm_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     for f in ("hm_hodlr_build_from_dense", "hm_hss_build_from_dense"):
         getattr(L, f).argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, C.c_int]
+    L.hm_hodlr_build_from_kernel.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int,
+                                             C.c_int]
     L.hm_hodlr_build_from_dense_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
     PP = C.POINTER(C.c_void_p)
     L.hm_hodlr_import.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip, PP, PP, PP, PP, PP]
@@ -85,8 +87,34 @@ def load() -> C.CDLL:
     L.hm_solve.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_int, C.POINTER(SolveStats)]
     L.hm_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                   C.POINTER(SolveStats)]
+    L.hm_set_precision.argtypes = [C.c_void_p, C.c_int]
+    L.hm_launch_count.argtypes = []
+    L.hm_launch_count.restype = C.c_longlong
+    L.hm_profile_enable.argtypes = [C.c_int]
+    L.hm_profile_enable.restype = None
+    L.hm_profile_report.argtypes = [C.c_char_p, C.c_size_t]
+    L.hm_profile_report.restype = C.c_size_t
     _lib = L
     return L
+
+
+def launch_count() -> int:
+    """Kernels this library has launched in the process."""
+    return int(load().hm_launch_count())
+
+
+def profile_enable(on: bool) -> None:
+    load().hm_profile_enable(1 if on else 0)
+
+
+def profile_report() -> dict:
+    """{step: (launches, ms, algorithmic flops, algorithmic bytes)} since profile_enable(True)."""
+    import json
+    L = load()
+    n = L.hm_profile_report(None, 0)
+    buf = C.create_string_buffer(int(n))
+    L.hm_profile_report(buf, n)
+    return {k: tuple(v) for k, v in json.loads(buf.value.decode()).items()}
 
 
 def header_functions() -> list[str]:
@@ -141,6 +169,10 @@ class _Handle:
             self.close()
         except Exception:
             pass
+
+    def set_precision(self, precision: int):
+        self._check(self._L.hm_set_precision(self._h, precision))
+        self.opts.precision = precision
 
     def set_stream(self, stream_ptr: int):
         self._check(self._L.hm_set_stream(self._h, C.c_void_p(stream_ptr)))
@@ -210,6 +242,21 @@ class HODLRMatrix(_Handle):
     def build_from_dense_device(self, dA: int, N: int, lda: int, leaf_size: int):
         self.N = N
         self._check(self._L.hm_hodlr_build_from_dense_device(self._h, C.c_void_p(dA), N, lda, leaf_size))
+
+    def build_from_kernel(self, kernel: int, points: np.ndarray, params, leaf_size: int, N: int | None = None):
+        """Matrix-free build.  Cauchy: points = concat(x, y) (1-D); Gaussian/Coulomb:
+        points N x dim."""
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        if kernel == KERNEL_CAUCHY:
+            N = pts.size // 2 if N is None else N
+            dim = 1
+        else:
+            pts2 = pts.reshape(pts.shape[0], -1)
+            N, dim = pts2.shape
+        pr = np.ascontiguousarray(params, dtype=np.float64)
+        self.N = N
+        self._check(self._L.hm_hodlr_build_from_kernel(self._h, kernel, _d(pts), dim, N, _d(pr), pr.size,
+                                                       leaf_size))
 
     def import_factors(self, N: int, leaf_size: int, nodes) -> None:
         """Upload a tree of reference factors; ``nodes`` in pre-order with attributes

@@ -97,12 +97,26 @@ HM_API const char* hm_last_error(const hm_handle* h);
 /* Work is enqueued on `stream` (a cudaStream_t); NULL = the handle's own stream. */
 HM_API int hm_set_stream(hm_handle* h, void* stream);
 
+/* Switch the factor/solve precision of an existing operator (HM_FP64 or HM_MIXED); the
+ * next solve refactors.  No counterpart in the reference (FP64 only). */
+HM_API int hm_set_precision(hm_handle* h, int precision);
+
 /* HODLRMatrix::build_from_dense(A, leaf_size) (hodlr_routines.h:20-63): tree split
  * mid=(s+e)/2, leaf iff len <= leaf; A12 -> (left.U, right.V, B_12), A21 -> (right.U,
  * left.V, B_21) by compress_rsvd (compression.h:67-99).  A: host, N x N, column-major. */
 HM_API int hm_hodlr_build_from_dense(hm_handle* h, const double* A, int N, int lda, int leaf_size);
 /* Same, with A already in device memory. */
 HM_API int hm_hodlr_build_from_dense_device(hm_handle* h, const double* dA, int N, int lda, int leaf_size);
+
+/* Matrix-free counterpart of build_from_dense for operators given by a kernel on
+ * points (the reference fills a dense A from include/kernel.h:30-89 and compresses its
+ * blocks; here the blocks' entries are evaluated on the device where the sketch GEMMs
+ * consume them, so A is never stored).  points (host): Cauchy: x[0:N] then y[0:N]
+ * (dim 1); Gaussian/Coulomb: N x dim, point-major.  params[0..1] = p0, p1 of the
+ * HM_KERNEL_* formula.  Same tree, compression rules and sketch stream as
+ * hm_hodlr_build_from_dense. */
+HM_API int hm_hodlr_build_from_kernel(hm_handle* h, int kernel, const double* points, int dim, int N,
+                                      const double* params, int nparams, int leaf_size);
 
 /* HSSMatrix::build_from_dense(A, leaf_size) (hss_routines.h:50-113): build_topo ids,
  * leaf row/column bases of the off-diagonal strips, identity transfers, dense B. */
@@ -143,6 +157,17 @@ HM_API int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x,
              hm_solve_stats* stats);
 HM_API int hm_solve_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx,
                     hm_solve_stats* stats);
+
+/* ---- instrumentation (no counterpart in the reference, which only wall-clocks its
+ *      drivers: main_hodlr.cpp:14-24) ---- */
+/* Count of kernels this library has launched in the process (always on). */
+HM_API long long hm_launch_count(void);
+/* Turn per-step CUDA-event timing on/off (clears recorded steps). */
+HM_API void hm_profile_enable(int on);
+/* JSON {"step": [launches, ms, algorithmic flops, algorithmic bytes], ...} of the steps
+ * recorded since hm_profile_enable(1); synchronises.  Returns the length needed
+ * (including the terminating NUL); writes at most len bytes. */
+HM_API size_t hm_profile_report(char* buf, size_t len);
 
 #ifdef __cplusplus
 }

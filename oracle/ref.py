@@ -62,6 +62,9 @@ def lib(gaussian: bool = False) -> C.CDLL:
         getattr(L, f"hmref_{kind}_multiply").argtypes = [C.c_void_p, _dp, _dp]
         getattr(L, f"hmref_{kind}_solve").argtypes = [C.c_void_p, _dp, C.c_int, _dp]
     L.hmref_hodlr_tree.argtypes = [C.c_void_p] + [_ip] * 6
+    L.hmref_hodlr_solve_omp.argtypes = [C.c_void_p, _dp, C.c_int, _dp]
+    L.hmref_omp_max_threads.argtypes = []
+    L.hmref_omp_max_threads.restype = C.c_int
     L.hmref_hss_tree.argtypes = [C.c_void_p] + [_ip] * 9
     _libs[name] = L
     return L
@@ -152,6 +155,15 @@ class RefHODLR:
         B = np.asfortranarray(b.reshape(self.N, -1))
         X = np.zeros_like(B, order="F")
         self.L.hmref_hodlr_solve(self.h, _d(B), B.shape[1], _d(X))
+        return X.ravel() if vec else X
+
+    def solve_omp(self, b: np.ndarray) -> np.ndarray:
+        """HODLRMatrixOMP::solve on this (serially built) tree."""
+        b = np.asarray(b, dtype=np.float64)
+        vec = b.ndim == 1
+        B = np.asfortranarray(b.reshape(self.N, -1))
+        X = np.zeros_like(B, order="F")
+        self.L.hmref_hodlr_solve_omp(self.h, _d(B), B.shape[1], _d(X))
         return X.ravel() if vec else X
 
     def to_oracle(self):

@@ -206,6 +206,23 @@ void hmref_hodlr_solve(void* h, const double* rhs, int nrhs, double* x) {
     to_ptr(xm, x);
 }
 
+// HODLRMatrixOMP::solve (hodlr_routines_omp.h:137-240) on the tree of a serial build:
+// the OpenMP class is pointed at the serial build's nodes (same HODLRNode type), so
+// the timed solve is the reference's OpenMP path without its OpenMP build, whose tasks
+// copy the whole dense A each (include/hodlr_routines_omp.h:48-56).
+void hmref_hodlr_solve_omp(void* h, const double* rhs, int nrhs, double* x) {
+    auto* b = static_cast<HodlrBox*>(h);
+    HODLRMatrixOMP view(b->ser ? b->ser->tolerance : b->par->tolerance);
+    view.root = b->root();
+    view.N = b->ser ? b->ser->N : b->par->N;
+    Matrix bm = from_ptr(rhs, view.N, nrhs, view.N);
+    Matrix xm = view.solve(bm);
+    to_ptr(xm, x);
+    view.root = nullptr;  // nodes stay owned by the box (view.nodes is empty)
+}
+
+int hmref_omp_max_threads() { return omp_get_max_threads(); }
+
 // ---- HSS (include/hss_routines.h, include/hss_routines_omp.h) ----
 void* hmref_hss_build(const double* A, int N, int lda, int leaf, double tol, int rsvd_rank,
                       unsigned seed, int omp) {
