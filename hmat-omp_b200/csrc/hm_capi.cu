@@ -53,7 +53,7 @@ hm::Engine& built(hm_handle* h) {
 void validate(const hm_opts& o) {
     HM_CHECK(o.tol == o.tol, HM_ERR_ARG, "tol is NaN");
     HM_CHECK(o.rsvd_rank >= 0 && o.oversample >= 0 && o.rsvd_min_dim >= 1, HM_ERR_ARG, "bad rsvd options");
-    HM_CHECK(o.rsvd_rank + o.oversample <= hm::GJ_MAX, HM_ERR_UNSUPPORTED,
+    HM_CHECK(o.rsvd_rank + o.oversample <= hm::SKETCH_MAX, HM_ERR_UNSUPPORTED,
              "rsvd_rank + oversample above the supported sketch width (160)");
     HM_CHECK(o.power_iters >= 0 && o.max_rank >= 0, HM_ERR_ARG, "bad power_iters/max_rank");
     HM_CHECK(o.sketch >= HM_SKETCH_REFERENCE_UNIFORM && o.sketch <= HM_SKETCH_DEVICE_NORMAL, HM_ERR_ARG,

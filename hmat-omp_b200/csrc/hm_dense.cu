@@ -1,7 +1,7 @@
 // Small batched dense kernels for sm_100a: one CTA per problem.
 //
 //  * gj_inverse_kernel  — Gauss-Jordan inversion with partial pivoting, the matrix held
-//                          in shared memory (n <= GJ_MAX).  Larger inverses are built by
+//                          in registers (n <= GJ_MAX).  Larger inverses are built by
 //                          2x2 block elimination over these plus batched GEMMs.
 //  * jacobi_kernel      — cyclic two-sided Jacobi for symmetric positive semi-definite
 //                          Gram matrices, parallel (round-robin) pair ordering, rotation
@@ -86,101 +86,128 @@ void Plan::run(cudaStream_t s, int* status) const {
 }
 
 // ---------------------------------------------------------------------------------
-// Gauss-Jordan inverse
+// Gauss-Jordan inverse, register resident, implicit pivoting
+//
+// Thread (lane, warp) holds rows lane + 32*rr and columns warp + W*cc of an NB x NB
+// tile (the matrix padded with identity).  Step j picks the pivot row p_j among rows not
+// yet used (largest |a[i][j]|, partial pivoting) and applies the in-place Gauss-Jordan
+// exchange on (p_j, j) without moving rows.  Afterwards row p_j holds x_j and column k
+// stands for equation p_k, so A^{-1}[j][p_k] = a[p_j][k]; the result is scattered with
+// that permutation.  The pivot column goes through shared memory (double-buffered, one
+// barrier per step); the pivot row comes from the owning lane by a warp shuffle.
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) gj_inverse_kernel(const GJDesc* __restrict__ descs, int* status) {
-    extern __shared__ double sm[];
+template <int NB, int W>
+__global__ void __launch_bounds__(32 * W, 1) gj_inverse_kernel(const GJDesc* __restrict__ descs, int* status) {
+    constexpr int RT = NB / 32, CT = NB / W;
+    __shared__ double colv[2][NB];
+    __shared__ double s_inv[2];
+    __shared__ int s_p[2];
+    __shared__ int piv[NB];
+    __shared__ int qinv[NB];
+    __shared__ int s_bad;
     const GJDesc d = descs[blockIdx.x];
     const int n = d.n;
     if (n <= 0) return;
-    double* a = sm;                 // n x n, column-major, ld n
-    double* colv = a + n * n;
-    double* rowv = colv + n;
-    int* perm = reinterpret_cast<int*>(rowv + n);
-    __shared__ int s_piv;
-    __shared__ int s_bad;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int e = tid; e < n * n; e += nt) {
-        int i = e % n, j = e / n;
-        a[e] = d.A[i + (size_t)j * d.lda];
-    }
-    if (tid == 0) s_bad = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double a[RT][CT];
+#pragma unroll
+    for (int rr = 0; rr < RT; ++rr)
+#pragma unroll
+        for (int cc = 0; cc < CT; ++cc) {
+            const int i = lane + 32 * rr, c = warp + W * cc;
+            a[rr][cc] = (i < n && c < n) ? d.A[i + (size_t)c * d.lda] : (i == c ? 1.0 : 0.0);
+        }
+    if (threadIdx.x == 0) s_bad = 0;
+    unsigned used = 0;
     __syncthreads();
+    int steps = 0;
     for (int j = 0; j < n; ++j) {
-        if (tid < 32) {
+        const int buf = j & 1;
+        if (warp == j % W) {
+            const int ccj = j / W;
             double best = -1.0;
-            int bi = j;
-            for (int i = j + tid; i < n; i += 32) {
-                double v = fabs(a[i + j * n]);
-                if (v > best) { best = v; bi = i; }
+            int bi = 0x7fffffff;
+#pragma unroll
+            for (int rr = 0; rr < RT; ++rr) {
+                double v = 0.0;
+#pragma unroll
+                for (int cc = 0; cc < CT; ++cc) v = (cc == ccj) ? a[rr][cc] : v;
+                colv[buf][lane + 32 * rr] = v;
+                const int i = lane + 32 * rr;
+                const double av = fabs(v);
+                if (i < n && !((used >> rr) & 1u) && av > best) { best = av; bi = i; }
             }
+#pragma unroll
             for (int off = 16; off > 0; off >>= 1) {
-                double ob = __shfl_down_sync(0xffffffffu, best, off);
-                int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
                 if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
             }
-            if (tid == 0) {
-                s_piv = bi;
-                perm[j] = bi;
-                double pv = a[bi + j * n];
+            __syncwarp();
+            if (lane == 0) {
+                const double pv = (bi < n) ? colv[buf][bi] : 0.0;
                 if (!(pv != 0.0) || !isfinite(pv)) s_bad = 1;
+                s_p[buf] = bi < n ? bi : 0;
+                s_inv[buf] = 1.0 / pv;
+                piv[j] = bi < n ? bi : 0;
             }
         }
         __syncthreads();
         if (s_bad) break;
-        const int p = s_piv;
-        if (p != j)
-            for (int c = tid; c < n; c += nt) {
-                double t = a[j + c * n];
-                a[j + c * n] = a[p + c * n];
-                a[p + c * n] = t;
-            }
-        __syncthreads();
-        for (int i = tid; i < n; i += nt) colv[i] = a[i + j * n];
-        for (int c = tid; c < n; c += nt) rowv[c] = a[j + c * n];
-        __syncthreads();
-        const double inv = 1.0 / rowv[j];
-        for (int e = tid; e < n * n; e += nt) {
-            int i = e % n, c = e / n;
-            double r = (c == j) ? inv : rowv[c] * inv;
-            if (i == j) a[e] = r;
-            else a[e] = ((c == j) ? 0.0 : a[e]) - colv[i] * r;
+        const int p = s_p[buf];
+        const double inv = s_inv[buf];
+        const int prr = p >> 5, plane = p & 31;
+        if (lane == plane) used |= 1u << prr;
+        double rv[CT], cv[RT];
+#pragma unroll
+        for (int cc = 0; cc < CT; ++cc) {
+            double v = 0.0;
+#pragma unroll
+            for (int rr = 0; rr < RT; ++rr) v = (rr == prr) ? a[rr][cc] : v;
+            rv[cc] = __shfl_sync(0xffffffffu, v, plane);
         }
-        __syncthreads();
+#pragma unroll
+        for (int rr = 0; rr < RT; ++rr) cv[rr] = colv[buf][lane + 32 * rr];
+#pragma unroll
+        for (int rr = 0; rr < RT; ++rr) {
+            const int i = lane + 32 * rr;
+#pragma unroll
+            for (int cc = 0; cc < CT; ++cc) {
+                const int c = warp + W * cc;
+                const double r = (c == j) ? inv : rv[cc] * inv;
+                a[rr][cc] = (i == p) ? r : fma(-cv[rr], r, (c == j) ? 0.0 : a[rr][cc]);
+            }
+        }
+        ++steps;
     }
     if (s_bad) {
-        if (tid == 0) atomicOr(status, ST_SINGULAR);
-        for (int e = tid; e < n * n; e += nt) {
-            int i = e % n, j = e / n;
-            d.X[i + (size_t)j * d.ldx] = nan("");
-        }
+        if (threadIdx.x == 0) atomicOr(status, ST_SINGULAR);
+        for (int e = threadIdx.x; e < n * n; e += 32 * W) d.X[(e % n) + (size_t)(e / n) * d.ldx] = nan("");
         return;
     }
-    for (int j = n - 1; j >= 0; --j) {
-        const int p = perm[j];
-        if (p != j)
-            for (int i = tid; i < n; i += nt) {
-                double t = a[i + j * n];
-                a[i + j * n] = a[i + p * n];
-                a[i + p * n] = t;
-            }
-        __syncthreads();
-    }
-    for (int e = tid; e < n * n; e += nt) {
-        int i = e % n, j = e / n;
-        d.X[i + (size_t)j * d.ldx] = a[e];
+    for (int j = threadIdx.x; j < n; j += 32 * W) qinv[piv[j]] = j;
+    __syncthreads();
+#pragma unroll
+    for (int rr = 0; rr < RT; ++rr) {
+        const int i = lane + 32 * rr;
+        if (i >= n) continue;
+        const int row = qinv[i];
+#pragma unroll
+        for (int cc = 0; cc < CT; ++cc) {
+            const int c = warp + W * cc;
+            if (c < n) d.X[row + (size_t)piv[c] * d.ldx] = a[rr][cc];
+        }
     }
 }
 
-void launch_gj(const DevTable<GJDesc>& t, int* status, cudaStream_t s) {
+void launch_gj(const DevTable<GJDesc>& t, int nb, int* status, cudaStream_t s) {
     if (t.h.empty()) return;
-    int nmax = 0;
-    for (auto& d : t.h) nmax = std::max(nmax, d.n);
-    HM_CHECK(nmax <= GJ_MAX, HM_ERR_UNSUPPORTED, "Gauss-Jordan block larger than GJ_MAX");
-    size_t smem = (size_t)nmax * nmax * 8 + 2 * (size_t)nmax * 8 + (size_t)nmax * 4 + 16;
-    static size_t cur = 0;
-    ensure_dyn_smem(gj_inverse_kernel, smem, cur);
-    gj_inverse_kernel<<<t.size(), 256, smem, s>>>(t.d.p, status);
+    switch (nb) {
+        case 32: gj_inverse_kernel<32, 4><<<t.size(), 128, 0, s>>>(t.d.p, status); break;
+        case 64: gj_inverse_kernel<64, 8><<<t.size(), 256, 0, s>>>(t.d.p, status); break;
+        case 128: gj_inverse_kernel<128, 16><<<t.size(), 512, 0, s>>>(t.d.p, status); break;
+        default: throw Error(HM_ERR_UNSUPPORTED, "Gauss-Jordan block size");
+    }
     HM_CUDA(cudaGetLastError());
 }
 
@@ -489,8 +516,8 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
     }
     if (!small.empty()) {
         auto st = std::make_unique<GJStep>();
-        for (auto& p : small) st->t.h.push_back({p.A, p.lda, p.X, p.ldx, p.n});
-        st->t.upload(s);
+        for (auto& p : small) st->t[p.n <= 32 ? 0 : p.n <= 64 ? 1 : 2].h.push_back({p.A, p.lda, p.X, p.ldx, p.n});
+        for (auto& tb : st->t) tb.upload(s);
         plan.add(std::move(st));
     }
     if (large.empty()) return;

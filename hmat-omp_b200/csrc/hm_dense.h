@@ -10,10 +10,11 @@
 
 namespace hm {
 
-// Largest matrix inverted directly in shared memory by Gauss-Jordan.
-constexpr int GJ_MAX = 160;
-// Larger inverses are split 2x2 (block elimination) down to this size.
-constexpr int GJ_SPLIT = 128;
+// Largest matrix inverted directly (in registers) by Gauss-Jordan; larger inverses are
+// split 2x2 (block elimination) down to this size.
+constexpr int GJ_MAX = 128;
+// Widest sketch (rsvd_rank + oversample) and full-SVD block the Jacobi kernels take.
+constexpr int SKETCH_MAX = 160;
 // Largest Gram matrix held in shared memory by the Jacobi eigen-solver.
 constexpr int JAC_SMEM_MAX = 128;
 
@@ -92,7 +93,7 @@ struct DevTable {
     int size() const { return (int)h.size(); }
 };
 
-void launch_gj(const DevTable<GJDesc>& t, int* status, cudaStream_t s);
+void launch_gj(const DevTable<GJDesc>& t, int nb, int* status, cudaStream_t s);
 void launch_jacobi(const DevTable<EigDesc>& t, int* status, cudaStream_t s, int max_sweeps = 40);
 void launch_prep(const DevTable<PrepDesc>& t, double tol, int max_rank, cudaStream_t s);
 void launch_norms(const DevTable<NormDesc>& t, cudaStream_t s);
@@ -179,20 +180,26 @@ struct GemmStep : Plan::Step {
 };
 
 struct GJStep : Plan::Step {
-    DevTable<GJDesc> t;
-    void run(cudaStream_t s, int* st) const override { launch_gj(t, st, s); }
+    DevTable<GJDesc> t[3];   // n <= 32, <= 64, <= 128
+    void run(cudaStream_t s, int* st) const override {
+        launch_gj(t[0], 32, st, s);
+        launch_gj(t[1], 64, st, s);
+        launch_gj(t[2], 128, st, s);
+    }
     const char* name() const override { return "gauss_jordan_inverse"; }
+    int nlaunch() const override { return !t[0].h.empty() + !t[1].h.empty() + !t[2].h.empty(); }
     double flops() const override {
         double f = 0;
-        for (auto& d : t.h) f += 2.0 * d.n * d.n * (double)d.n;
+        for (auto& tb : t)
+            for (auto& d : tb.h) f += 2.0 * d.n * d.n * (double)d.n;
         return f;
     }
     double bytes() const override {
         double b = 0;
-        for (auto& d : t.h) b += 16.0 * d.n * d.n;
+        for (auto& tb : t)
+            for (auto& d : tb.h) b += 16.0 * d.n * d.n;
         return b;
     }
-    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
 };
 struct EigStep : Plan::Step {
     DevTable<EigDesc> t;

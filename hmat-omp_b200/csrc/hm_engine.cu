@@ -234,6 +234,9 @@ void Engine::begin_build(int N, int leaf) {
     leaf_ = leaf;
     built_ = factored_ = false;
     f64_.ready = f32_.ready = false;
+    f64_.planned = f32_.planned = false;
+    f64_.plans.clear();
+    f32_.plans.clear();
     dDinv.release();
     mv_plans_.clear();
     solve64_plans_.clear();
@@ -639,10 +642,10 @@ static CopyDesc flat_copy(const void* src, bool sf, void* dst, bool df, size_t n
 }
 
 template <typename T>
-void Engine::factor_t(FactorStore<T>& fs) {
+void Engine::plan_factor(FactorStore<T>& fs) {
     constexpr bool F32 = std::is_same<T, float>::value;
     cudaStream_t s = stream_;
-    dstatus.zero(s);
+    fs.plans.clear();
     size_t offM = 0, offP = 0;
     for (auto& n : nodes_) {
         if (n.is_leaf) continue;
@@ -662,7 +665,8 @@ void Engine::factor_t(FactorStore<T>& fs) {
         }
         if (n.is_leaf) totD = std::max(totD, n.offD + (size_t)n.len() * n.len());
     }
-    Plan plan;
+    fs.plans.push_back(std::make_unique<Plan>());
+    Plan& plan = *fs.plans.back();
     {   // FP64 leaf inverses
         if (dDinv.n < totD) dDinv.alloc(totD);
         std::vector<InvProblem> inv;
@@ -680,7 +684,7 @@ void Engine::factor_t(FactorStore<T>& fs) {
     const T* Dinv;
     const T* Vt;
     const T* Ut;
-    DBuf<T> Utmp;
+    DBuf<T>& Utmp = fs.Utmp;
     if constexpr (F32) {
         if (fs.Dinv.n < totD) fs.Dinv.alloc(totD);
         if (fs.V.n < totV) fs.V.alloc(totV);
@@ -714,12 +718,9 @@ void Engine::factor_t(FactorStore<T>& fs) {
         g->batch.finalize(s);
         plan.add(std::move(g));
     }
-    plan.run(s, dstatus.p);
-    HM_CUDA(cudaStreamSynchronize(s));
-    check_status("factor: leaf inverses");
-
     for (int d = (int)levels_.size() - 1; d >= 0; --d) {
-        Plan lp;
+        fs.plans.push_back(std::make_unique<Plan>());
+        Plan& lp = *fs.plans.back();
         const auto& lvl = levels_[d];
         auto gK = std::make_unique<GemmStep<T>>();
         auto cvK = std::make_unique<CopyStep>();
@@ -810,10 +811,18 @@ void Engine::factor_t(FactorStore<T>& fs) {
         lp.add(std::move(gD));
         gC->batch.finalize(s);
         lp.add(std::move(gC));
-        lp.run(s, dstatus.p);
-        HM_CUDA(cudaStreamSynchronize(s));
-        check_status("factor: capacitance");
     }
+    fs.planned = true;
+}
+
+// Run the recorded factorization (planned once per operator), then check the status
+// word once: singular pivots anywhere are reported after the last level.
+template <typename T>
+void Engine::factor_t(FactorStore<T>& fs) {
+    if (!fs.planned) plan_factor(fs);
+    dstatus.zero(stream_);
+    for (auto& p : fs.plans) p->run(stream_, dstatus.p);
+    check_status("factor");
     fs.ready = true;
 }
 

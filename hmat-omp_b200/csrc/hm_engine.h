@@ -53,6 +53,9 @@ struct FactorStore {
     DBuf<T> P;      // B^ Minv per internal node
     DBuf<T> Dinv;   // leaf inverses in precision T (FP64: unused)
     bool ready = false;
+    bool planned = false;
+    DBuf<T> Utmp;                              // U in precision T (FP32 only)
+    std::vector<std::unique_ptr<Plan>> plans;  // leaf step, then one per level
 };
 
 class Engine {
@@ -100,6 +103,7 @@ class Engine {
                         const std::vector<std::tuple<int, int, int, int, int, double*, int>>& blocks);
     void check_status(const char* what);
     template <typename T> void factor_t(FactorStore<T>& fs);
+    template <typename T> void plan_factor(FactorStore<T>& fs);
     template <typename T> Plan& solve_plan(FactorStore<T>& fs, int s);
     Plan& matvec_plan(int s);
     void ensure_io(int s);
