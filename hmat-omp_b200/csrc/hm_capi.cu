@@ -220,6 +220,13 @@ int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ld
     });
 }
 
+int hm_multiply_device_noalloc(hm_handle* h, const double* dx, int nrhs, int ldx, double* dy, int ldy) {
+    return guard(h, [&] {
+        hm::Engine& e = built(h);
+        hm::multiply_noalloc(e.view(), dx, nrhs, ldx, dy, ldy, e.stream());
+    });
+}
+
 void hm_profile_enable(int on) {
     hm::Profiler& p = hm::Profiler::get();
     p.enabled = on != 0;

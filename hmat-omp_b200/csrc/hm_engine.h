@@ -31,6 +31,7 @@ struct Node {
     size_t offM = 0, offP = 0;
 };
 
+class Engine;
 std::vector<Node> hodlr_tree(int N, int leaf);
 std::vector<Node> hss_tree(int N, int leaf);
 
@@ -92,6 +93,18 @@ class Engine {
     void export_tree(int* start, int* end, int* is_leaf, int* depth, int* r12, int* r21) const;
     void get_factor(int node, int which, double* out, int* rows, int* cols) const;
 
+    // Read-only view of the FP64 operator storage (for entry points that build their
+    // own launch tables).
+    struct View {
+        const std::vector<Node>* nodes;
+        const std::vector<int>* leaves;
+        const std::vector<std::vector<int>>* levels;
+        const double *D, *U, *V, *B;
+        int N;
+        bool built;
+    };
+    View view() const { return {&nodes_, &leaves_, &levels_, dD.p, dU.p, dV.p, dB.p, N_, built_}; }
+
   protected:
     void plan_levels();
     void alloc_bases();
@@ -136,4 +149,11 @@ class Engine {
     std::map<int, Plan> mv_plans_, solve64_plans_, solve32_plans_;
 };
 
+}  // namespace hm
+
+namespace hm {
+// The multiply of Engine::multiply_device without device allocation: intermediates and
+// launch tables in a fixed file-scope device array (hm_noalloc.cu).
+void multiply_noalloc(const Engine::View& v, const double* dx, int s, int ldx, double* dy, int ldy,
+                      cudaStream_t st);
 }  // namespace hm

@@ -336,6 +336,16 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp) const {
     HM_CUDA(cudaGetLastError());
 }
 
+// Launch a batch whose descriptor and zeroing tables are already in device memory
+// that the caller owns (tile offsets assigned as GemmBatch::packed() does).
+void gemm_launch_tables(const GemmDesc<double>* dtab, int ndesc, int total_tiles,
+                        const ZeroRegion<double>* dzero, int nzero, cudaStream_t s) {
+    if (ndesc <= 0 || total_tiles <= 0) return;
+    if (nzero > 0) zero_regions_kernel<double><<<nzero, 256, 0, s>>>(dzero, nzero);
+    launch_gen<double, 64, 64, 16, 4, 4>(GEN_DENSE, total_tiles, s, dtab, ndesc, GenParams());
+    HM_CUDA(cudaGetLastError());
+}
+
 template class GemmBatch<double>;
 template class GemmBatch<float>;
 

@@ -57,6 +57,11 @@ struct GenFillDesc {
 void launch_gen_fill(const GenFillDesc* d_descs, int count, int max_elems, int gen, const GenParams& gp,
                      cudaStream_t s);
 
+template <typename T> struct GemmDesc;
+template <typename T> struct ZeroRegion;
+void gemm_launch_tables(const GemmDesc<double>* dtab, int ndesc, int total_tiles,
+                        const ZeroRegion<double>* dzero, int nzero, cudaStream_t s);
+
 // Tile configurations.
 enum : int { CFG_64x64 = 0, CFG_N_SKINNY = 1 };
 
@@ -76,6 +81,19 @@ class GemmBatch {
     void clear();
     int cfg() const { return cfg_; }
     int gen() const { return gen_; }
+    // Descriptors with tile offsets assigned (total tile count in *tiles), and the
+    // split-K zeroing regions: for launching from tables the caller places itself.
+    std::vector<GemmDesc<T>> packed(int* tiles) const {
+        std::vector<GemmDesc<T>> out(h_);
+        int t = 0;
+        for (auto& d : out) {
+            d.tile0 = t;
+            t += d.tiles_m * d.tiles_n * d.ksplit;
+        }
+        *tiles = t;
+        return out;
+    }
+    const std::vector<ZeroRegion<T>>& zero_regions() const { return hz_; }
     int nlaunch() const { return h_.empty() ? 0 : (hz_.empty() ? 1 : 2); }
     // algorithmic work of one launch: 2mnk flops; operand and result bytes
     double flops() const { return flops_; }

@@ -158,6 +158,18 @@ HM_API int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x,
 HM_API int hm_solve_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx,
                     hm_solve_stats* stats);
 
+/* multiply(x) like hm_multiply_device, but allocating no device memory: for callers
+ * that may not call cudaMalloc when they multiply (a loop being captured into a CUDA
+ * graph, a real-time or callback thread, an application that owns all device memory
+ * through its own pool).  No counterpart in the reference.  Intermediates and launch
+ * tables live in one fixed 32 MiB device array that every GPU loading the library
+ * keeps until exit; operators needing more fail with HM_ERR_UNSUPPORTED.  The first
+ * call on a device looks up that array's device address (make it before any stream
+ * capture).  All calls share the array: calls whose work overlaps on the GPU race.
+ * dx/dy: device, N x nrhs, column-major, on the handle's stream. */
+HM_API int hm_multiply_device_noalloc(hm_handle* h, const double* dx, int nrhs, int ldx, double* dy,
+                                      int ldy);
+
 /* ---- instrumentation (no counterpart in the reference, which only wall-clocks its
  *      drivers: main_hodlr.cpp:14-24) ---- */
 /* Count of kernels this library has launched in the process (always on). */
