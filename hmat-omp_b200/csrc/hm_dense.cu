@@ -624,7 +624,7 @@ void plan_gram_svd(Plan& plan, const std::vector<SvdProblem>& probs, double tol,
         int* pm = plan.scratch_i(k);
         nrm->t.h.push_back({x.X, x.ldx, m, k, raw});
         prep->t.h.push_back({raw, sig, pm, p.rank, k});
-        perm->t.h.push_back({x.X, x.ldx, p.L, p.ldl, m, k, pm, sig});
+        if (p.L) perm->t.h.push_back({x.X, x.ldx, p.L, p.ldl, m, k, pm, sig});
         if (p.R) perm->t.h.push_back({x.Wt, k, p.R, p.ldr, k, k, pm, nullptr});
     }
     nrm->t.upload(s);

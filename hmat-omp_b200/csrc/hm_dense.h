@@ -274,7 +274,7 @@ struct SvdProblem {
     const double* X;
     int ldx;
     int rows, k;
-    double* L;      // rows x k (may alias X)
+    double* L;      // rows x k (may alias X; nullptr: not needed)
     int ldl;
     double* R;      // k x k (nullptr: not needed, e.g. orthonormalisation only)
     int ldr;

@@ -193,13 +193,23 @@ void Engine::check_status(const char* what) {
 
 // Column capacity of each basis block from the compression rules (compression.h:72-75).
 void Engine::alloc_bases() {
-    size_t offU = 0, offV = 0, offD = 0;
+    alloc_D();
+    alloc_UV();
+}
+
+void Engine::alloc_D() {
+    size_t offD = 0;
     for (auto& n : nodes_) {
         if (n.is_leaf) {
             n.offD = offD;
             offD += (size_t)n.len() * n.len();
         }
     }
+    dD.alloc(std::max<size_t>(offD, 1));
+}
+
+void Engine::alloc_UV() {
+    size_t offU = 0, offV = 0;
     for (auto& n : nodes_) {
         if (n.parent < 0) continue;
         n.offU = offU;
@@ -207,11 +217,40 @@ void Engine::alloc_bases() {
         n.offV = offV;
         offV += (size_t)n.len() * n.capV;
     }
-    dD.alloc(std::max<size_t>(offD, 1));
     dU.alloc(std::max<size_t>(offU, 1));
     dV.alloc(std::max<size_t>(offV, 1));
     dU.zero(stream_);
     dV.zero(stream_);
+}
+
+// blocks: (offset, count) of each sketch in the reference's draw order.
+void Engine::make_sketches(DBuf<double>& dOmega, const std::vector<std::pair<size_t, size_t>>& blocks) {
+    size_t total = 0;
+    for (auto& b : blocks) total = std::max(total, b.first + b.second);
+    dOmega.alloc(std::max<size_t>(total, 1));
+    if (!total) return;
+    if (opts_.sketch == HM_SKETCH_DEVICE_NORMAL) {
+        normal_fill_kernel<<<grid_for(total), 256, 0, stream_>>>(dOmega.p, total, opts_.seed, 0ull);
+        HM_CUDA(cudaGetLastError());
+        count_launch();
+        return;
+    }
+    // Matrix::Random (matrix.h:50-57): one std::mt19937 seeded once, a fresh
+    // distribution per call, column-major fill, calls in build order.
+    std::vector<double> host(total);
+    std::mt19937 gen((std::mt19937::result_type)opts_.seed);
+    for (auto& b : blocks) {
+        double* o = host.data() + b.first;
+        if (opts_.sketch == HM_SKETCH_REFERENCE_NORMAL) {
+            std::normal_distribution<double> dist(0.0, 1.0);
+            for (size_t i = 0; i < b.second; ++i) o[i] = dist(gen);
+        } else {
+            std::uniform_real_distribution<double> dist(0.0, 1.0);
+            for (size_t i = 0; i < b.second; ++i) o[i] = dist(gen);
+        }
+    }
+    HM_CUDA(cudaMemcpyAsync(dOmega.p, host.data(), total * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    HM_CUDA(cudaStreamSynchronize(stream_));
 }
 
 // ---------------------------------------------------------------------------------
@@ -364,33 +403,12 @@ void Engine::build_hodlr(const Source& src) {
     size_t omega_total = 0;
     for (auto& b : blocks)
         if (b.rsvd) { b.omega = omega_total; omega_total += (size_t)b.n * b.k; }
-    DBuf<double> dOmega(std::max<size_t>(omega_total, 1));
-    if (omega_total) {
-        if (opts_.sketch == HM_SKETCH_DEVICE_NORMAL) {
-            normal_fill_kernel<<<grid_for(omega_total), 256, 0, stream_>>>(dOmega.p, omega_total,
-                                                                           opts_.seed, 0ull);
-            HM_CUDA(cudaGetLastError());
-        } else {
-            // Matrix::Random (matrix.h:50-57): one std::mt19937 seeded once, a fresh
-            // distribution per call, column-major fill, calls in build order.
-            std::vector<double> host(omega_total);
-            std::mt19937 gen((std::mt19937::result_type)opts_.seed);
-            for (auto& b : blocks) {
-                if (!b.rsvd) continue;
-                double* o = host.data() + b.omega;
-                size_t cnt = (size_t)b.n * b.k;
-                if (opts_.sketch == HM_SKETCH_REFERENCE_NORMAL) {
-                    std::normal_distribution<double> dist(0.0, 1.0);
-                    for (size_t i = 0; i < cnt; ++i) o[i] = dist(gen);
-                } else {
-                    std::uniform_real_distribution<double> dist(0.0, 1.0);
-                    for (size_t i = 0; i < cnt; ++i) o[i] = dist(gen);
-                }
-            }
-            HM_CUDA(cudaMemcpyAsync(dOmega.p, host.data(), omega_total * sizeof(double),
-                                    cudaMemcpyHostToDevice, stream_));
-            HM_CUDA(cudaStreamSynchronize(stream_));
-        }
+    DBuf<double> dOmega;
+    {
+        std::vector<std::pair<size_t, size_t>> om;
+        for (auto& b : blocks)
+            if (b.rsvd) om.emplace_back(b.omega, (size_t)b.n * b.k);
+        make_sketches(dOmega, om);
     }
     // per-block sigma and rank
     std::vector<size_t> sig_off(blocks.size());
@@ -576,8 +594,287 @@ void Engine::build_hodlr(const Source& src) {
     HM_CUDA(cudaStreamSynchronize(stream_));
 }
 
-void Engine::build_hss(const Source&) {
-    throw Error(HM_ERR_UNSUPPORTED, "HSS build not available in this build");
+// HSS build (hss_routines.h:50-113).  Leaves, in reverse id order, compress their row
+// strip A[leaf, :] and their transposed column strip A[:, leaf]^T, each with the diagonal
+// block zeroed, keeping only the left singular vectors (the leaf's U and V).  Transfers
+// are identities (hss_routines.h:86-90), so a node's basis is the block diagonal of its
+// leaves' bases and B12 = UL^T A12 VR is the set of leaf-pair blocks U_l^T A_lm V_m.
+// Those come from the panels Pt_l = A[l, :]^T U_l (N x rank_U(l)): block (l, m) of B is
+// Pt_l[m rows]^T V_m.  The engine then factors/solves/multiplies this two-block form.
+void Engine::build_hss(const Source& src) {
+    const int N = N_;
+    const int kguess = opts_.rsvd_rank + opts_.oversample;
+    struct Strip {
+        int leaf, which;  // which 0: row strip (U), 1: column strip (V)
+        bool rsvd;
+        int m, k;
+        size_t omega = 0, out = 0;
+    };
+    std::vector<Strip> strips;
+    for (int i = (int)nodes_.size() - 1; i >= 0; --i) {  // reverse id order (hss_routines.h:57)
+        if (!nodes_[i].is_leaf) continue;
+        for (int w = 0; w < 2; ++w) {
+            Strip s;
+            s.leaf = i;
+            s.which = w;
+            s.m = nodes_[i].len();
+            s.rsvd = s.m >= opts_.rsvd_min_dim && N >= opts_.rsvd_min_dim;  // compression.h:72
+            s.k = s.rsvd ? std::min(kguess, std::min(s.m, N)) : std::min(s.m, N);
+            strips.push_back(s);
+        }
+    }
+    size_t omega_total = 0, out_total = 0;
+    for (auto& s : strips) {
+        if (s.rsvd) { s.omega = omega_total; omega_total += (size_t)N * s.k; }
+        s.out = out_total;
+        out_total += (size_t)s.m * s.k;
+    }
+    DBuf<double> dOmega;
+    {
+        std::vector<std::pair<size_t, size_t>> om;
+        for (auto& s : strips)
+            if (s.rsvd) om.emplace_back(s.omega, (size_t)N * s.k);
+        make_sketches(dOmega, om);
+    }
+    alloc_D();
+    {
+        Plan lp;
+        std::vector<std::tuple<int, int, int, int, int, double*, int>> fill;
+        for (int l : leaves_) {
+            const Node& n = nodes_[l];
+            fill.emplace_back(n.start, n.start, n.len(), n.len(), 0, dD.p + n.offD, n.len());
+        }
+        add_block_fill(lp, src, fill);
+        lp.run(stream_, dstatus.p);
+    }
+    dLeafB.alloc(std::max<size_t>(out_total, 1));
+    DBuf<int> dRank(std::max<size_t>(strips.size(), 1));
+    // chunks of strips bounded by a workspace budget
+    const size_t budget = size_t(16) << 30;
+    size_t i0 = 0;
+    while (i0 < strips.size()) {
+        size_t i1 = i0, bytes = 0;
+        while (i1 < strips.size()) {
+            const Strip& s = strips[i1];
+            const size_t b = 8 * ((size_t)s.m * N + 5 * (size_t)N * s.k + 6 * (size_t)s.m * s.k + 8 * (size_t)s.k * s.k);
+            if (i1 > i0 && bytes + b > budget) break;
+            bytes += b;
+            ++i1;
+        }
+        Plan plan;
+        std::vector<std::tuple<int, int, int, int, int, double*, int>> fill;
+        auto zero = std::make_unique<IdentStep>();
+        std::vector<SvdProblem> full;
+        struct R { const Strip* s; double *S, *Y, *Q, *X, *Ub; };
+        std::vector<R> rs;
+        for (size_t i = i0; i < i1; ++i) {
+            const Strip& s = strips[i];
+            const Node& n = nodes_[s.leaf];
+            const int slot = (int)i;
+            if (!s.rsvd) {
+                // tall X = strip^T (N x m); strip = R S L^T, U_strip = R
+                double* X = plan.scratch((size_t)N * s.m);
+                if (s.which == 0) fill.emplace_back(n.start, 0, N, s.m, 1, X, N);
+                else fill.emplace_back(0, n.start, N, s.m, 0, X, N);
+                zero->t.h.push_back({X + n.start, N, s.m, s.m, 0.0});
+                SvdProblem q{};
+                q.X = X; q.ldx = N; q.rows = N; q.k = s.m;
+                q.L = nullptr;
+                q.R = dLeafB.p + s.out; q.ldr = s.m;
+                q.rank = dRank.p + slot;
+                q.sort = true;
+                full.push_back(q);
+            } else {
+                R r{&s, nullptr, nullptr, nullptr, nullptr, nullptr};
+                r.S = plan.scratch((size_t)s.m * N);  // the strip, m x N
+                if (s.which == 0) fill.emplace_back(n.start, 0, s.m, N, 0, r.S, s.m);
+                else fill.emplace_back(0, n.start, s.m, N, 1, r.S, s.m);
+                zero->t.h.push_back({r.S + (size_t)n.start * s.m, s.m, s.m, s.m, 0.0});
+                r.Y = plan.scratch((size_t)s.m * s.k);
+                r.Q = plan.scratch((size_t)s.m * s.k);
+                r.X = plan.scratch((size_t)N * s.k);
+                r.Ub = plan.scratch((size_t)s.k * s.k);
+                rs.push_back(r);
+            }
+        }
+        add_block_fill(plan, src, fill);
+        zero->t.upload(stream_);
+        plan.add(std::move(zero));
+        plan_gram_svd(plan, full, opts_.tol, opts_.max_rank, stream_);
+        if (!rs.empty()) {
+            auto gY = std::make_unique<GemmStep<double>>();
+            for (auto& r : rs)  // Y = S Omega  (compression.h:79)
+                gY->batch.add(r.s->m, r.s->k, N, 1.0, r.S, r.s->m, OP_N, dOmega.p + r.s->omega, N, OP_N, 0.0,
+                              r.Y, r.s->m);
+            gY->batch.finalize(stream_);
+            plan.add(std::move(gY));
+            std::vector<SvdProblem> sq;
+            for (auto& r : rs) {  // Q = orthonormal basis of range(Y)
+                SvdProblem q{};
+                q.X = r.Y; q.ldx = r.s->m; q.rows = r.s->m; q.k = r.s->k;
+                q.L = r.Q; q.ldl = r.s->m;
+                sq.push_back(q);
+            }
+            plan_gram_svd(plan, sq, opts_.tol, 0, stream_);
+            auto gX = std::make_unique<GemmStep<double>>();
+            for (auto& r : rs)  // X = S^T Q
+                gX->batch.add(N, r.s->k, r.s->m, 1.0, r.S, r.s->m, OP_T, r.Q, r.s->m, OP_N, 0.0, r.X, N);
+            gX->batch.finalize(stream_);
+            plan.add(std::move(gX));
+            std::vector<SvdProblem> sv;
+            for (auto& r : rs) {  // SVD of Q^T S: X = V_b diag(S) U_b^T
+                SvdProblem q{};
+                q.X = r.X; q.ldx = N; q.rows = N; q.k = r.s->k;
+                q.L = nullptr;
+                q.R = r.Ub; q.ldr = r.s->k;
+                q.rank = dRank.p + (r.s - strips.data());
+                q.sort = true;
+                sv.push_back(q);
+            }
+            plan_gram_svd(plan, sv, opts_.tol, opts_.max_rank, stream_);
+            auto gU = std::make_unique<GemmStep<double>>();
+            for (auto& r : rs)  // U = Q U_b  (compression.h:94)
+                gU->batch.add(r.s->m, r.s->k, r.s->k, 1.0, r.Q, r.s->m, OP_N, r.Ub, r.s->k, OP_N, 0.0,
+                              dLeafB.p + r.s->out, r.s->m);
+            gU->batch.finalize(stream_);
+            plan.add(std::move(gU));
+        }
+        plan.run(stream_, dstatus.p);
+        HM_CUDA(cudaStreamSynchronize(stream_));
+        check_status("hss build: leaf strips");
+        i0 = i1;
+    }
+    // ranks: leaves from their strips, internal nodes the sums (hss_routines.h:82-83)
+    std::vector<int> rk(strips.size());
+    if (!strips.empty())
+        HM_CUDA(cudaMemcpy(rk.data(), dRank.p, rk.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    leafU_.assign(nodes_.size(), {0, 0});
+    leafV_.assign(nodes_.size(), {0, 0});
+    for (size_t i = 0; i < strips.size(); ++i) {
+        const Strip& s = strips[i];
+        Node& n = nodes_[s.leaf];
+        const int r = std::min(rk[i], s.k);
+        if (s.which == 0) { n.rankU = r; leafU_[s.leaf] = {s.out, r}; }
+        else { n.rankV = r; leafV_[s.leaf] = {s.out, r}; }
+    }
+    for (int i = (int)nodes_.size() - 1; i >= 0; --i) {
+        Node& n = nodes_[i];
+        if (n.is_leaf) continue;
+        n.rankU = nodes_[n.left].rankU + nodes_[n.right].rankU;
+        n.rankV = nodes_[n.left].rankV + nodes_[n.right].rankV;
+    }
+    for (auto& n : nodes_) {
+        n.capU = n.rankU;
+        n.capV = n.rankV;
+    }
+    alloc_UV();
+    // dense bases: block diagonal of the leaf bases (reconstruct_U/V, hss_routines.h:23-45)
+    std::vector<std::vector<int>> under(nodes_.size());  // leaves under each node, left to right
+    for (int i = (int)nodes_.size() - 1; i >= 0; --i) {
+        if (nodes_[i].is_leaf) under[i] = {i};
+        else {
+            under[i] = under[nodes_[i].left];
+            under[i].insert(under[i].end(), under[nodes_[i].right].begin(), under[nodes_[i].right].end());
+        }
+    }
+    {
+        Plan bp;
+        auto cp = std::make_unique<CopyStep>();
+        for (size_t c = 0; c < nodes_.size(); ++c) {
+            const Node& C = nodes_[c];
+            if (C.parent < 0) continue;
+            int cu = 0, cv = 0;
+            for (int l : under[c]) {
+                const Node& L = nodes_[l];
+                const size_t ro = (size_t)(L.start - C.start);
+                if (L.rankU)
+                    cp->t.h.push_back({dLeafB.p + leafU_[l].first, L.len(), dU.p + C.offU + ro + (size_t)cu * C.len(),
+                                       C.len(), L.len(), L.rankU, 0, 0, 0});
+                if (L.rankV)
+                    cp->t.h.push_back({dLeafB.p + leafV_[l].first, L.len(), dV.p + C.offV + ro + (size_t)cv * C.len(),
+                                       C.len(), L.len(), L.rankV, 0, 0, 0});
+                cu += L.rankU;
+                cv += L.rankV;
+                if (cp->t.h.size() >= 60000) {
+                    cp->t.upload(stream_);
+                    bp.add(std::move(cp));
+                    cp = std::make_unique<CopyStep>();
+                }
+            }
+        }
+        if (!cp->t.h.empty()) { cp->t.upload(stream_); bp.add(std::move(cp)); }
+        bp.run(stream_, dstatus.p);
+        HM_CUDA(cudaStreamSynchronize(stream_));
+    }
+    // coupling blocks
+    size_t totB = 0;
+    for (auto& n : nodes_) {
+        if (n.is_leaf) continue;
+        const Node& L = nodes_[n.left];
+        const Node& R = nodes_[n.right];
+        n.offB12 = totB;
+        totB += (size_t)L.rankU * R.rankV;
+        n.offB21 = totB;
+        totB += (size_t)R.rankU * L.rankV;
+    }
+    dB.alloc(std::max<size_t>(totB, 1));
+    dB.zero(stream_);
+    if (!levels_.empty()) {
+        size_t totP = 0;
+        std::vector<size_t> offP(nodes_.size(), 0);
+        for (int l : leaves_) { offP[l] = totP; totP += (size_t)N * nodes_[l].rankU; }
+        DBuf<double> Pt(std::max<size_t>(totP, 1));
+        Plan pp;
+        {   // Pt_l = A[l rows, :]^T U_l
+            auto g = std::make_unique<GemmStep<double>>(CFG_64x64, src.gen);
+            g->gp = src.gp;
+            for (int l : leaves_) {
+                const Node& L = nodes_[l];
+                g->batch.add(N, L.rankU, L.len(), 1.0, src.blk(L.start, 0), src.lda, OP_T,
+                             dLeafB.p + leafU_[l].first, L.len(), OP_N, 0.0, Pt.p + offP[l], N, nullptr, 0,
+                             L.start, 0);
+            }
+            g->batch.finalize(stream_);
+            pp.add(std::move(g));
+        }
+        auto gB = std::make_unique<GemmStep<double>>();
+        auto flush = [&]() {
+            if (gB->batch.empty()) return;
+            gB->batch.finalize(stream_);
+            pp.add(std::move(gB));
+            gB = std::make_unique<GemmStep<double>>();
+        };
+        for (auto& lvl : levels_)
+            for (int id : lvl) {
+                const Node& n = nodes_[id];
+                const int lc = n.left, rc = n.right;
+                const int p1 = nodes_[lc].rankU, p2 = nodes_[rc].rankU;
+                // B12[(l in lc), (m in rc)] = Pt_l[m rows]^T V_m ; B21 likewise with roles swapped
+                for (int side = 0; side < 2; ++side) {
+                    const int rowc = side == 0 ? lc : rc, colc = side == 0 ? rc : lc;
+                    double* Bn = dB.p + (side == 0 ? n.offB12 : n.offB21);
+                    const int ldb = side == 0 ? p1 : p2;
+                    int ro = 0;
+                    for (int l : under[rowc]) {
+                        const Node& L = nodes_[l];
+                        int co = 0;
+                        for (int m : under[colc]) {
+                            const Node& Mn = nodes_[m];
+                            gB->batch.add(L.rankU, Mn.rankV, Mn.len(), 1.0, Pt.p + offP[l] + Mn.start, N, OP_T,
+                                          dLeafB.p + leafV_[m].first, Mn.len(), OP_N, 0.0,
+                                          Bn + ro + (size_t)co * ldb, ldb);
+                            co += Mn.rankV;
+                        }
+                        ro += L.rankU;
+                    }
+                    if (gB->batch.size() > 200000) flush();
+                }
+            }
+        flush();
+        pp.run(stream_, dstatus.p);
+        HM_CUDA(cudaStreamSynchronize(stream_));
+    }
+    check_status("hss build");
 }
 
 // ---------------------------------------------------------------------------------
@@ -1067,8 +1364,12 @@ void Engine::export_tree(int* start, int* end, int* is_leaf, int* depth, int* r1
         if (is_leaf) is_leaf[i] = n.is_leaf;
         if (depth) depth[i] = n.depth;
         int a = 0, b = 0;
-        if (!n.is_leaf) {
-            if (kind_ == HODLR) { a = nodes_[n.left].rankU; b = nodes_[n.right].rankU; }
+        if (kind_ == HSS) {  // rank_U, rank_V (utils.h:41-42)
+            a = n.rankU;
+            b = n.rankV;
+        } else if (!n.is_leaf) {  // B_12, B_21 sizes (hodlr_routines.h:140-141)
+            a = nodes_[n.left].rankU;
+            b = nodes_[n.right].rankU;
         }
         if (r12) r12[i] = a;
         if (r21) r21[i] = b;
@@ -1081,6 +1382,57 @@ void Engine::get_factor(int node, int which, double* out, int* rows, int* cols) 
     const Node& n = nodes_[node];
     const double* src = nullptr;
     int r = 0, c = 0, ld = 0;
+    if (kind_ == HSS) {  // HSSNode fields (utils.h:32-55)
+        std::vector<double> host;
+        switch (which) {
+            case 0: if (n.is_leaf) { src = dD.p + n.offD; r = c = ld = n.len(); } break;
+            case 1: if (n.is_leaf) { src = dLeafB.p + leafU_[node].first; r = ld = n.len(); c = n.rankU; } break;
+            case 2: if (n.is_leaf) { src = dLeafB.p + leafV_[node].first; r = ld = n.len(); c = n.rankV; } break;
+            case 3:  // R = I (hss_routines.h:86-87)
+            case 4: {  // W = I (hss_routines.h:89-90)
+                const int k = which == 3 ? n.rankU : n.rankV;
+                if (n.is_leaf || k == 0) break;
+                r = c = k;
+                if (out)
+                    for (int j = 0; j < k; ++j)
+                        for (int i = 0; i < k; ++i) out[i + (size_t)j * k] = i == j;
+                if (rows) *rows = r;
+                if (cols) *cols = c;
+                return;
+            }
+            case 5: {  // B = [[0, B12], [B21, 0]] at (0, lc.rank_V) and (lc.rank_U, 0) (hss_routines.h:105-107)
+                if (n.is_leaf || n.rankU == 0 || n.rankV == 0) break;
+                const Node& L = nodes_[n.left];
+                const Node& R = nodes_[n.right];
+                r = n.rankU;
+                c = n.rankV;
+                if (out) {
+                    std::fill(out, out + (size_t)r * c, 0.0);
+                    std::vector<double> b12((size_t)L.rankU * R.rankV), b21((size_t)R.rankU * L.rankV);
+                    if (!b12.empty())
+                        HM_CUDA(cudaMemcpy(b12.data(), dB.p + n.offB12, b12.size() * 8, cudaMemcpyDeviceToHost));
+                    if (!b21.empty())
+                        HM_CUDA(cudaMemcpy(b21.data(), dB.p + n.offB21, b21.size() * 8, cudaMemcpyDeviceToHost));
+                    for (int j = 0; j < R.rankV; ++j)
+                        for (int i = 0; i < L.rankU; ++i)
+                            out[i + (size_t)(L.rankV + j) * r] = b12[i + (size_t)j * L.rankU];
+                    for (int j = 0; j < L.rankV; ++j)
+                        for (int i = 0; i < R.rankU; ++i)
+                            out[(L.rankU + i) + (size_t)j * r] = b21[i + (size_t)j * R.rankU];
+                }
+                if (rows) *rows = r;
+                if (cols) *cols = c;
+                return;
+            }
+            default: throw Error(HM_ERR_ARG, "get_factor: bad selector");
+        }
+        if (rows) *rows = r;
+        if (cols) *cols = c;
+        if (out && r * c > 0)
+            HM_CUDA(cudaMemcpy2D(out, (size_t)r * sizeof(double), src, (size_t)ld * sizeof(double),
+                                 (size_t)r * sizeof(double), c, cudaMemcpyDeviceToHost));
+        return;
+    }
     switch (which) {
         case 0: if (n.is_leaf) { src = dD.p + n.offD; r = c = ld = n.len(); } break;
         case 1: if (n.parent >= 0) { src = dU.p + n.offU; r = ld = n.len(); c = n.rankU; } break;

@@ -108,6 +108,10 @@ class Engine {
   protected:
     void plan_levels();
     void alloc_bases();
+    void alloc_D();
+    void alloc_UV();
+    // sketches for RSVD blocks, in draw order: host mt19937 stream or device normals
+    void make_sketches(DBuf<double>& dOmega, const std::vector<std::pair<size_t, size_t>>& blocks);
     void begin_build(int N, int leaf);
     void build_hodlr(const Source& src);
     void build_hss(const Source& src);
@@ -135,6 +139,9 @@ class Engine {
     DBuf<double> dD, dU, dV, dB;
     DBuf<int> dstatus;
     DBuf<double> dPts;             // generator points (matrix-free builds)
+    // HSS: compressed leaf bases (offset into dLeafB, rank) per leaf node
+    DBuf<double> dLeafB;
+    std::vector<std::pair<size_t, int>> leafU_, leafV_;
     bool built_ = false;
     // factorizations
     FactorStore<double> f64_;
