@@ -220,6 +220,27 @@ int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ld
     });
 }
 
+int hm_solve_transpose_device(hm_handle* h, const double* dg, int nrhs, int ldg, double* dl, int ldl) {
+    return guard(h, [&] { built(h).solve_transpose_device(dg, nrhs, ldg, dl, ldl); });
+}
+
+int hm_solve_transpose(hm_handle* h, const double* g, int nrhs, int ldg, double* lam, int ldl) {
+    return guard(h, [&] {
+        built(h).solve_transpose_device(g, nrhs, ldg, lam, ldl);   // host pointers: unified addressing
+        HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int hm_gradients(hm_handle* h, const double* x, int ldx, const double* lam, int ldl, int nrhs, double* dparams) {
+    return guard(h, [&] { built(h).gradients(x, ldx, lam, ldl, nrhs, dparams); });
+}
+
+int hm_get_gradient(const hm_handle* h, int node, int which, double* out, int* rows, int* cols) {
+    return guard(const_cast<hm_handle*>(h), [&] {
+        built(const_cast<hm_handle*>(h)).get_gradient(node, which, out, rows, cols);
+    });
+}
+
 int hm_multiply_device_noalloc(hm_handle* h, const double* dx, int nrhs, int ldx, double* dy, int ldy) {
     return guard(h, [&] {
         hm::Engine& e = built(h);

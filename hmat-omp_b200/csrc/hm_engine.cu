@@ -280,6 +280,10 @@ void Engine::begin_build(int N, int leaf) {
     mv_plans_.clear();
     solve64_plans_.clear();
     solve32_plans_.clear();
+    solveT_plans_.clear();
+    grads_ready_ = false;
+    gen_ = GEN_DENSE;
+    gp_ = GenParams();
     nodes_ = kind_ == HODLR ? hodlr_tree(N, leaf) : hss_tree(N, leaf);
     plan_levels();
     if (!dstatus.p) dstatus.alloc(1);
@@ -326,6 +330,8 @@ void Engine::build_kernel(int gen, const double* pts, size_t npts, int dim, int 
     src.gp.p1 = p1;
     if (kind_ == HODLR) build_hodlr(src);
     else build_hss(src);
+    gen_ = src.gen;
+    gp_ = src.gp;
     built_ = true;
 }
 
@@ -1148,6 +1154,7 @@ void Engine::ensure_io(int s) {
     mv_plans_.clear();
     solve64_plans_.clear();
     solve32_plans_.clear();
+    solveT_plans_.clear();
 }
 
 // y = A x for s columns: in = x (ld N), out = y (ld N)
@@ -1351,6 +1358,173 @@ void Engine::solve_device(const double* db, int s, int ldb, double* dx, int ldx,
     if (st) { st->ir_iters = 0; st->rel_residual = -1.0; }
     if (opts_.precision == HM_MIXED) solve_mixed(db, s, ldb, dx, ldx, st);
     else solve_fp64(db, s, ldb, dx, ldx);
+}
+
+// ---------------------------------------------------------------------------------
+// Adjoint: A^T lam = g with the FP64 factors.  A^{-1} = F_0 ... F_{L-1} Dinv with
+// F_d = I - Q P V~^T per node of level d, so A^{-T} = Dinv^T F_{L-1}^T ... F_0^T:
+// root level first, t = [Q1^T l1; Q2^T l2], gamma = P^T t, l1 -= V1 gamma_1,
+// l2 -= V2 gamma_2; then lam_leaf = Dinv^T l_leaf.
+// ---------------------------------------------------------------------------------
+Plan& Engine::solveT_plan(int s) {
+    auto it = solveT_plans_.find(s);
+    if (it != solveT_plans_.end()) return it->second;
+    Plan& pl = solveT_plans_[s];
+    const int N = N_;
+    double* Z = ioX.p;
+    for (size_t d = 0; d < levels_.size(); ++d) {
+        auto gT = std::make_unique<GemmStep<double>>();
+        auto gG = std::make_unique<GemmStep<double>>();
+        auto gC = std::make_unique<GemmStep<double>>();
+        for (int id : levels_[d]) {
+            const Node& n = nodes_[id];
+            const Node& L = nodes_[n.left];
+            const Node& R = nodes_[n.right];
+            const int p1 = L.rankU, p2 = R.rankU, q1 = L.rankV, q2 = R.rankV;
+            const int p = p1 + p2, q = q1 + q2;
+            double* T = pl.scratch(std::max<size_t>((size_t)p * s, 1));
+            double* G = pl.scratch(std::max<size_t>((size_t)q * s, 1));
+            gT->batch.add(p1, s, L.len(), 1.0, f64_.Q.p + L.offU, L.len(), OP_T, Z + L.start, N, OP_N, 0.0, T, p);
+            gT->batch.add(p2, s, R.len(), 1.0, f64_.Q.p + R.offU, R.len(), OP_T, Z + R.start, N, OP_N, 0.0, T + p1, p);
+            gG->batch.add(q, s, p, 1.0, f64_.P.p + n.offP, p, OP_T, T, p, OP_N, 0.0, G, q);
+            gC->batch.add(L.len(), s, q1, -1.0, dV.p + L.offV, L.len(), OP_N, G, q, OP_N, 1.0, Z + L.start, N);
+            gC->batch.add(R.len(), s, q2, -1.0, dV.p + R.offV, R.len(), OP_N, G + q1, q, OP_N, 1.0, Z + R.start, N);
+        }
+        gT->batch.finalize(stream_);
+        pl.add(std::move(gT));
+        gG->batch.finalize(stream_);
+        pl.add(std::move(gG));
+        gC->batch.finalize(stream_);
+        pl.add(std::move(gC));
+    }
+    auto gL = std::make_unique<GemmStep<double>>();
+    for (int l : leaves_) {
+        const Node& n = nodes_[l];
+        gL->batch.add(n.len(), s, n.len(), 1.0, dDinv.p + n.offD, n.len(), OP_T, Z + n.start, N, OP_N, 0.0,
+                      ioY.p + n.start, N);
+    }
+    gL->batch.finalize(stream_);
+    pl.add(std::move(gL));
+    return pl;
+}
+
+void Engine::solve_transpose_device(const double* dg, int s, int ldg, double* dl, int ldl) {
+    HM_CHECK(built_, HM_ERR_STATE, "solve_transpose before build");
+    HM_CHECK(s >= 1 && ldg >= N_ && ldl >= N_ && dg && dl, HM_ERR_ARG, "solve_transpose: bad arguments");
+    if (!f64_.ready) factor_t<double>(f64_);
+    ensure_io(s);
+    copy_in(ioX.p, dg, N_, s, ldg, stream_);
+    solveT_plan(s).run(stream_, dstatus.p);
+    copy_out(dl, ldl, ioY.p, N_, s, stream_);
+}
+
+// Gradients of a loss L through x = A^{-1} b, given x and lam = A^{-T} dL/dx, so that
+// dL/dA = -lam x^T: per leaf dD = -lam x^T; per node, with A12 = U1 B12 V2^T and
+// A21 = U2 B21 V1^T, dU1 = -lam1 (B12 V2^T x2)^T, dV2 = -x2 (B12^T U1^T lam1)^T,
+// dB12 = -(U1^T lam1)(V2^T x2)^T, and likewise for A21.  For a kernel-generated
+// operator also dL/dp0 and dL/dp1 of the exact kernel (matrix-free, O(N^2 s)).
+void Engine::gradients(const double* dx, int ldx, const double* dl, int ldl, int s, double* dparams) {
+    HM_CHECK(built_, HM_ERR_STATE, "gradients before build");
+    HM_CHECK(s >= 1 && ldx >= N_ && ldl >= N_ && dx && dl, HM_ERR_ARG, "gradients: bad arguments");
+    const int N = N_;
+    ensure_io(s);
+    // stage x in ioX and lam in ioY (ld N)
+    copy_in(ioX.p, dx, N, s, ldx, stream_);
+    copy_in(ioY.p, dl, N, s, ldl, stream_);
+    gD_.alloc(std::max<size_t>(dD.n, 1));
+    gU_.alloc(std::max<size_t>(dU.n, 1));
+    gV_.alloc(std::max<size_t>(dV.n, 1));
+    gB_.alloc(std::max<size_t>(dB.n, 1));
+    gU_.zero(stream_);
+    gV_.zero(stream_);
+    Plan pl;
+    const double *X = ioX.p, *Lm = ioY.p;
+    auto gLeaf = std::make_unique<GemmStep<double>>();
+    for (int l : leaves_) {
+        const Node& n = nodes_[l];
+        gLeaf->batch.add(n.len(), n.len(), s, -1.0, Lm + n.start, N, OP_N, X + n.start, N, OP_T, 0.0,
+                         gD_.p + n.offD, n.len());
+    }
+    auto gProj = std::make_unique<GemmStep<double>>();
+    auto gMid = std::make_unique<GemmStep<double>>();
+    auto gOut = std::make_unique<GemmStep<double>>();
+    for (auto& lvl : levels_)
+        for (int id : lvl) {
+            const Node& n = nodes_[id];
+            const Node& L = nodes_[n.left];
+            const Node& R = nodes_[n.right];
+            const int p1 = L.rankU, p2 = R.rankU, q1 = L.rankV, q2 = R.rankV;
+            double* t1 = pl.scratch(std::max<size_t>((size_t)q1 * s, 1));   // V1^T x1
+            double* t2 = pl.scratch(std::max<size_t>((size_t)q2 * s, 1));   // V2^T x2
+            double* w1 = pl.scratch(std::max<size_t>((size_t)p1 * s, 1));   // U1^T lam1
+            double* w2 = pl.scratch(std::max<size_t>((size_t)p2 * s, 1));   // U2^T lam2
+            double* u1 = pl.scratch(std::max<size_t>((size_t)p1 * s, 1));   // B12 t2
+            double* u2 = pl.scratch(std::max<size_t>((size_t)p2 * s, 1));   // B21 t1
+            double* v2 = pl.scratch(std::max<size_t>((size_t)q2 * s, 1));   // B12^T w1
+            double* v1 = pl.scratch(std::max<size_t>((size_t)q1 * s, 1));   // B21^T w2
+            const double* B12 = dB.p + n.offB12;
+            const double* B21 = dB.p + n.offB21;
+            gProj->batch.add(q1, s, L.len(), 1.0, dV.p + L.offV, L.len(), OP_T, X + L.start, N, OP_N, 0.0, t1, q1);
+            gProj->batch.add(q2, s, R.len(), 1.0, dV.p + R.offV, R.len(), OP_T, X + R.start, N, OP_N, 0.0, t2, q2);
+            gProj->batch.add(p1, s, L.len(), 1.0, dU.p + L.offU, L.len(), OP_T, Lm + L.start, N, OP_N, 0.0, w1, p1);
+            gProj->batch.add(p2, s, R.len(), 1.0, dU.p + R.offU, R.len(), OP_T, Lm + R.start, N, OP_N, 0.0, w2, p2);
+            gMid->batch.add(p1, s, q2, 1.0, B12, p1, OP_N, t2, q2, OP_N, 0.0, u1, p1);
+            gMid->batch.add(p2, s, q1, 1.0, B21, p2, OP_N, t1, q1, OP_N, 0.0, u2, p2);
+            gMid->batch.add(q2, s, p1, 1.0, B12, p1, OP_T, w1, p1, OP_N, 0.0, v2, q2);
+            gMid->batch.add(q1, s, p2, 1.0, B21, p2, OP_T, w2, p2, OP_N, 0.0, v1, q1);
+            // dU1 = -lam1 u1^T, dU2 = -lam2 u2^T, dV2 = -x2 v2^T, dV1 = -x1 v1^T
+            gOut->batch.add(L.len(), p1, s, -1.0, Lm + L.start, N, OP_N, u1, p1, OP_T, 0.0, gU_.p + L.offU, L.len());
+            gOut->batch.add(R.len(), p2, s, -1.0, Lm + R.start, N, OP_N, u2, p2, OP_T, 0.0, gU_.p + R.offU, R.len());
+            gOut->batch.add(R.len(), q2, s, -1.0, X + R.start, N, OP_N, v2, q2, OP_T, 0.0, gV_.p + R.offV, R.len());
+            gOut->batch.add(L.len(), q1, s, -1.0, X + L.start, N, OP_N, v1, q1, OP_T, 0.0, gV_.p + L.offV, L.len());
+            // dB12 = -w1 t2^T, dB21 = -w2 t1^T
+            gOut->batch.add(p1, q2, s, -1.0, w1, p1, OP_N, t2, q2, OP_T, 0.0, gB_.p + n.offB12, p1);
+            gOut->batch.add(p2, q1, s, -1.0, w2, p2, OP_N, t1, q1, OP_T, 0.0, gB_.p + n.offB21, p2);
+        }
+    for (auto* g : {gLeaf.get(), gProj.get(), gMid.get(), gOut.get()}) g->batch.finalize(stream_);
+    pl.add(std::move(gLeaf));
+    pl.add(std::move(gProj));
+    pl.add(std::move(gMid));
+    pl.add(std::move(gOut));
+    pl.run(stream_, dstatus.p);
+    if (dparams) {
+        dparams[0] = dparams[1] = std::nan("");
+        if (gen_ != GEN_DENSE) {
+            DBuf<double> acc(2);
+            acc.zero(stream_);
+            launch_param_grad(gen_, gp_, X, Lm, N, s, acc.p, stream_);
+            count_launch();
+            double h[2];
+            HM_CUDA(cudaMemcpyAsync(h, acc.p, sizeof h, cudaMemcpyDeviceToHost, stream_));
+            HM_CUDA(cudaStreamSynchronize(stream_));
+            dparams[0] = h[0];
+            dparams[1] = h[1];
+        }
+    }
+    HM_CUDA(cudaStreamSynchronize(stream_));
+    grads_ready_ = true;
+}
+
+void Engine::get_gradient(int node, int which, double* out, int* rows, int* cols) const {
+    HM_CHECK(grads_ready_, HM_ERR_STATE, "get_gradient before gradients");
+    HM_CHECK(kind_ == HODLR, HM_ERR_UNSUPPORTED, "factor gradients are for HODLR operators");
+    HM_CHECK(node >= 0 && node < (int)nodes_.size(), HM_ERR_ARG, "get_gradient: bad node");
+    const Node& n = nodes_[node];
+    const double* src = nullptr;
+    int r = 0, c = 0, ld = 0;
+    switch (which) {
+        case 0: if (n.is_leaf) { src = gD_.p + n.offD; r = c = ld = n.len(); } break;
+        case 1: if (n.parent >= 0) { src = gU_.p + n.offU; r = ld = n.len(); c = n.rankU; } break;
+        case 2: if (n.parent >= 0) { src = gV_.p + n.offV; r = ld = n.len(); c = n.rankV; } break;
+        case 3: if (!n.is_leaf) { src = gB_.p + n.offB12; r = ld = nodes_[n.left].rankU; c = nodes_[n.right].rankV; } break;
+        case 4: if (!n.is_leaf) { src = gB_.p + n.offB21; r = ld = nodes_[n.right].rankU; c = nodes_[n.left].rankV; } break;
+        default: throw Error(HM_ERR_ARG, "get_gradient: bad selector");
+    }
+    if (rows) *rows = r;
+    if (cols) *cols = c;
+    if (out && r * c > 0)
+        HM_CUDA(cudaMemcpy2D(out, (size_t)r * sizeof(double), src, (size_t)ld * sizeof(double),
+                             (size_t)r * sizeof(double), c, cudaMemcpyDeviceToHost));
 }
 
 // ---------------------------------------------------------------------------------

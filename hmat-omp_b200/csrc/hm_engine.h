@@ -88,6 +88,10 @@ class Engine {
     void multiply_device(const double* dx, int s, int ldx, double* dy, int ldy);
     void factor();
     void solve_device(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st);
+    // adjoint solve and gradient accumulation
+    void solve_transpose_device(const double* dg, int s, int ldg, double* dl, int ldl);
+    void gradients(const double* dx, int ldx, const double* dl, int ldl, int s, double* dparams);
+    void get_gradient(int node, int which, double* out, int* rows, int* cols) const;
 
     // introspection
     void export_tree(int* start, int* end, int* is_leaf, int* depth, int* r12, int* r21) const;
@@ -123,6 +127,7 @@ class Engine {
     template <typename T> void plan_factor(FactorStore<T>& fs);
     template <typename T> Plan& solve_plan(FactorStore<T>& fs, int s);
     Plan& matvec_plan(int s);
+    Plan& solveT_plan(int s);
     void ensure_io(int s);
     std::vector<int> path_of(int n) const;   // n and its ancestors below the root
     void solve_fp64(const double* db, int s, int ldb, double* dx, int ldx);
@@ -153,7 +158,12 @@ class Engine {
     DBuf<double> ioX, ioY, ioR, ioNorm;
     DBuf<float> ioXf, ioYf;
     int io_cols_ = 0;
-    std::map<int, Plan> mv_plans_, solve64_plans_, solve32_plans_;
+    std::map<int, Plan> mv_plans_, solve64_plans_, solve32_plans_, solveT_plans_;
+    // the build's operator source (kernel generator and its parameters) and gradients
+    int gen_ = GEN_DENSE;
+    GenParams gp_;
+    DBuf<double> gD_, gU_, gV_, gB_;
+    bool grads_ready_ = false;
 };
 
 }  // namespace hm

@@ -224,6 +224,105 @@ void launch_gen_fill(const GenFillDesc* d_descs, int count, int max_elems, int g
 }
 
 // ---------------------------------------------------------------------------------
+// dL/dp of the exact kernel operator: dL/dA = -lam x^T, so
+//   dL/dp0 = -sum_ij dA_ij/dp0 * sum_k lam_ik x_jk,  dL/dp1 = -sum_i sum_k lam_ik x_ik
+// (p1 is the diagonal shift of the Gaussian and Coulomb kernels; for Cauchy the shift is
+// p0 and has no off-diagonal part).  One CTA: 128 rows x PG_COLS columns, both operand
+// panels staged in shared memory as [k][index].
+// ---------------------------------------------------------------------------------
+constexpr int PG_ROWS = 128, PG_COLS = 1024, PG_TILE = 128;
+
+template <int GEN>
+__device__ __forceinline__ double gen_dparam(const GenParams& g, int r, int c) {
+    if constexpr (GEN == GEN_GAUSSIAN) {
+        double d2 = 0.0;
+        for (int t = 0; t < g.dim; ++t) {
+            const double d = g.pts[(size_t)r * g.dim + t] - g.pts[(size_t)c * g.dim + t];
+            d2 += d * d;
+        }
+        const double h = g.p0;
+        return exp(-d2 / (2.0 * h * h)) * d2 / (h * h * h);
+    } else if constexpr (GEN == GEN_COULOMB) {
+        double d2 = 0.0;
+        for (int t = 0; t < g.dim; ++t) {
+            const double d = g.pts[(size_t)r * g.dim + t] - g.pts[(size_t)c * g.dim + t];
+            d2 += d * d;
+        }
+        const double den = sqrt(d2) + g.p0;
+        return -1.0 / (den * den);
+    } else {
+        return r == c ? 1.0 : 0.0;  // Cauchy: p0 is the diagonal shift
+    }
+}
+
+template <int GEN>
+__global__ void __launch_bounds__(PG_ROWS) param_grad_kernel(GenParams gp, const double* __restrict__ X,
+                                                             const double* __restrict__ L, int N, int s,
+                                                             double* acc) {
+    extern __shared__ double sm[];
+    double* Ls = sm;                  // [s][PG_ROWS]
+    double* Xs = sm + (size_t)s * PG_ROWS;  // [s][PG_TILE]
+    const int i0 = blockIdx.x * PG_ROWS, j0 = blockIdx.y * PG_COLS;
+    const int t = threadIdx.x, i = i0 + t;
+    for (int k = 0; k < s; ++k) Ls[k * PG_ROWS + t] = i < N ? L[i + (size_t)k * N] : 0.0;
+    double a0 = 0.0, a1 = 0.0;
+    for (int jt = j0; jt < min(N, j0 + PG_COLS); jt += PG_TILE) {
+        __syncthreads();
+        for (int k = 0; k < s; ++k) {
+            const int j = jt + t;
+            Xs[k * PG_TILE + t] = j < N ? X[j + (size_t)k * N] : 0.0;
+        }
+        __syncthreads();
+        if (i >= N) continue;
+        const int jn = min(PG_TILE, N - jt);
+        for (int jj = 0; jj < jn; ++jj) {
+            const int j = jt + jj;
+            double dot = 0.0;
+            for (int k = 0; k < s; ++k) dot = fma(Ls[k * PG_ROWS + t], Xs[k * PG_TILE + jj], dot);
+            a0 = fma(gen_dparam<GEN>(gp, i, j), dot, a0);
+            if (i == j) a1 += dot;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        a0 += __shfl_down_sync(0xffffffffu, a0, off);
+        a1 += __shfl_down_sync(0xffffffffu, a1, off);
+    }
+    if ((t & 31) == 0) {
+        atomicAdd(&acc[0], -a0);
+        atomicAdd(&acc[1], GEN == GEN_CAUCHY ? 0.0 : -a1);
+    }
+}
+
+void launch_param_grad(int gen, const GenParams& gp, const double* X, const double* L, int N, int s,
+                       double* acc, cudaStream_t st) {
+    HM_CHECK(s >= 1 && s <= 96, HM_ERR_UNSUPPORTED, "kernel-parameter gradient supports 1..96 columns");
+    const size_t smem = (size_t)s * (PG_ROWS + PG_TILE) * sizeof(double);
+    dim3 grid((unsigned)ceil_div(N, PG_ROWS), (unsigned)ceil_div(N, PG_COLS));
+    switch (gen) {
+        case GEN_GAUSSIAN: {
+            static size_t cur = 0;
+            ensure_dyn_smem(param_grad_kernel<GEN_GAUSSIAN>, smem, cur);
+            param_grad_kernel<GEN_GAUSSIAN><<<grid, PG_ROWS, smem, st>>>(gp, X, L, N, s, acc);
+            break;
+        }
+        case GEN_COULOMB: {
+            static size_t cur = 0;
+            ensure_dyn_smem(param_grad_kernel<GEN_COULOMB>, smem, cur);
+            param_grad_kernel<GEN_COULOMB><<<grid, PG_ROWS, smem, st>>>(gp, X, L, N, s, acc);
+            break;
+        }
+        case GEN_CAUCHY: {
+            static size_t cur = 0;
+            ensure_dyn_smem(param_grad_kernel<GEN_CAUCHY>, smem, cur);
+            param_grad_kernel<GEN_CAUCHY><<<grid, PG_ROWS, smem, st>>>(gp, X, L, N, s, acc);
+            break;
+        }
+        default: throw Error(HM_ERR_ARG, "parameter gradient needs a kernel-generated operator");
+    }
+    HM_CUDA(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------
 struct CfgShape { int BM, BN, BK; };

@@ -57,6 +57,11 @@ struct GenFillDesc {
 void launch_gen_fill(const GenFillDesc* d_descs, int count, int max_elems, int gen, const GenParams& gp,
                      cudaStream_t s);
 
+// acc[0] += dL/dp0, acc[1] += dL/dp1 of the exact kernel operator, given x and
+// lam = A^{-T} dL/dx (both N x s, ld N); dL/dA = -lam x^T.
+void launch_param_grad(int gen, const GenParams& gp, const double* X, const double* L, int N, int s,
+                       double* acc, cudaStream_t st);
+
 template <typename T> struct GemmDesc;
 template <typename T> struct ZeroRegion;
 void gemm_launch_tables(const GemmDesc<double>* dtab, int ndesc, int total_tiles,

@@ -87,6 +87,10 @@ def load() -> C.CDLL:
     L.hm_solve.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_int, C.POINTER(SolveStats)]
     L.hm_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                   C.POINTER(SolveStats)]
+    L.hm_solve_transpose.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_int]
+    L.hm_solve_transpose_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]
+    L.hm_gradients.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, _dp]
+    L.hm_get_gradient.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _ip, _ip]
     L.hm_set_precision.argtypes = [C.c_void_p, C.c_int]
     L.hm_launch_count.argtypes = []
     L.hm_launch_count.restype = C.c_longlong
@@ -206,6 +210,33 @@ class _Handle:
         self._check(self._L.hm_solve_device(self._h, C.c_void_p(db), nrhs, ldb, C.c_void_p(dx), ldx,
                                             C.byref(st)))
         return st
+
+    def solve_transpose(self, g: np.ndarray) -> np.ndarray:
+        """lam = A^{-T} g (the adjoint solve)."""
+        g = np.asarray(g, dtype=np.float64)
+        vec = g.ndim == 1
+        G = np.asfortranarray(g.reshape(self.N, -1))
+        Lm = np.zeros_like(G, order="F")
+        self._check(self._L.hm_solve_transpose(self._h, _d(G), G.shape[1], self.N, _d(Lm), self.N))
+        return Lm.ravel() if vec else Lm
+
+    def gradients(self, x: np.ndarray, lam: np.ndarray) -> np.ndarray:
+        """Accumulate dL/d(factors) from x and lam = A^{-T} dL/dx; returns [dL/dp0, dL/dp1]
+        of the kernel (NaN for dense builds)."""
+        X = np.asfortranarray(np.asarray(x, dtype=np.float64).reshape(self.N, -1))
+        Lm = np.asfortranarray(np.asarray(lam, dtype=np.float64).reshape(self.N, -1))
+        out = np.zeros(2)
+        self._check(self._L.hm_gradients(self._h, X.ctypes.data, self.N, Lm.ctypes.data, self.N, X.shape[1],
+                                         _d(out)))
+        return out
+
+    def get_gradient(self, node: int, which: int) -> np.ndarray:
+        r, c = C.c_int(), C.c_int()
+        self._check(self._L.hm_get_gradient(self._h, node, which, None, C.byref(r), C.byref(c)))
+        out = np.zeros(r.value * c.value)
+        if out.size:
+            self._check(self._L.hm_get_gradient(self._h, node, which, _d(out), C.byref(r), C.byref(c)))
+        return out.reshape(c.value, r.value).T.copy()
 
     def num_nodes(self) -> int:
         return self._L.hm_num_nodes(self._h)

@@ -158,6 +158,22 @@ HM_API int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x,
 HM_API int hm_solve_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx,
                     hm_solve_stats* stats);
 
+/* ---- adjoint (no counterpart in the reference) ----
+ * A^T lam = g with the FP64 factorization run transposed in reverse level order
+ * (the transpose of the Woodbury recursion of hodlr_routines.h:112-175); factors in FP64
+ * on demand.  Host or device g/lam; the _device form does not synchronise. */
+HM_API int hm_solve_transpose(hm_handle* h, const double* g, int nrhs, int ldg, double* lam, int ldl);
+HM_API int hm_solve_transpose_device(hm_handle* h, const double* dg, int nrhs, int ldg, double* dlam, int ldl);
+/* Gradients of a loss L through x = A^{-1} b given x and lam = A^{-T} dL/dx (so dL/db = lam
+ * and dL/dA = -lam x^T), accumulated into the factors of the HODLR representation
+ * (leaf D, U, V, B_12, B_21; read with hm_get_gradient, same selectors as
+ * hm_get_factor) and, for operators built by hm_hodlr_build_from_kernel, dparams[0..1] =
+ * dL/dp0, dL/dp1 of the exact kernel (Gaussian: p0 = length-scale h; NaN for dense
+ * builds).  dparams may be NULL. */
+HM_API int hm_gradients(hm_handle* h, const double* x, int ldx, const double* lam, int ldl, int nrhs,
+                        double* dparams);
+HM_API int hm_get_gradient(const hm_handle* h, int node, int which, double* out, int* rows, int* cols);
+
 /* multiply(x) like hm_multiply_device, but allocating no device memory: for callers
  * that may not call cudaMalloc when they multiply (a loop being captured into a CUDA
  * graph, a real-time or callback thread, an application that owns all device memory

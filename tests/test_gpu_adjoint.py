@@ -1,0 +1,143 @@
+"""Adjoint solve and gradients (the differentiation configuration: Gaussian kernel
+h = 0.05 + 1e-2 I on sorted uniform points, HODLR leaf 128, ranks <= 64, FP64;
+L = ||A^{-1} b - t||^2).  Checked against a dense FP64 gradient, central finite
+differences of the whole pipeline (rebuild at h +- eps), and finite differences of the
+factors."""
+import numpy as np
+import pytest
+
+import hmat_b200 as H
+import hmat_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+H0, SHIFT, LEAF, RANK = 0.05, 1e-2, 128, 64
+
+
+def points(N, seed=5):
+    return np.sort(np.random.default_rng(seed).random(N))
+
+
+def build(N, h=H0, tol=1e-12, pts=None):
+    pts = points(N) if pts is None else pts
+    m = H.HODLRMatrix(tol, rsvd_rank=RANK, max_rank=RANK, oversample=10, power_iters=1,
+                      sketch=H.SKETCH_DEVICE_NORMAL, seed=1)
+    m.build_from_kernel(H.KERNEL_GAUSSIAN, pts.reshape(-1, 1), [h, SHIFT], LEAF)
+    return m
+
+
+def loss_and_grad(m, b, t):
+    x = m.solve(b)
+    g = 2.0 * (x - t)
+    lam = m.solve_transpose(g)
+    dp = m.gradients(x, lam)
+    return float(((x - t) ** 2).sum()), x, lam, dp
+
+
+def test_transpose_solve_is_the_adjoint():
+    N = 4096
+    m = build(N)
+    rng = np.random.default_rng(0)
+    u, v = rng.standard_normal((N, 3)), rng.standard_normal((N, 3))
+    lhs = np.sum(m.solve(u) * v)
+    rhs = np.sum(u * m.solve_transpose(v))
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+def test_gradients_against_dense_fp64():
+    N = 4096
+    pts = points(N)
+    m = build(N, pts=pts)
+    rng = np.random.default_rng(1)
+    b, t = rng.standard_normal(N), rng.standard_normal(N)
+    L, x, lam, dp = loss_and_grad(m, b, t)
+    A = O.gaussian_matrix(pts, H0, SHIFT)
+    xd = np.linalg.solve(A, b)
+    lamd = np.linalg.solve(A.T, 2.0 * (xd - t))
+    d = pts[:, None] - pts[None, :]
+    dA = np.exp(-d * d / (2 * H0 * H0)) * d * d / H0 ** 3
+    dh_dense = -lamd @ dA @ xd
+    assert O.rel_err(lamd, lam) < 1e-6          # dL/db
+    assert abs(dp[0] - dh_dense) <= 1e-6 * abs(dh_dense)   # dL/dh
+    assert abs(dp[1] - (-lamd @ xd)) <= 1e-6 * abs(lamd @ xd)  # dL/d(shift)
+
+
+def test_dh_against_central_differences():
+    N = 8192
+    pts = points(N)
+    rng = np.random.default_rng(2)
+    b, t = rng.standard_normal(N), rng.standard_normal(N)
+    # L ~ 8e7 while dL/dh ~ 7.6e6: the rebuilds' rounding noise in L (~1e-12 relative at
+    # cond ~1e4) is amplified by L / (eps dL/dh), so the step must be large (eps = 1e-4,
+    # noise ~3e-7) and Richardson extrapolation removes the eps^2 truncation (1e-5 at
+    # this eps).  A dense FP64 check of the same loss gives FD vs adjoint 1.4e-7.
+    tol = 1e-14
+    m = build(N, pts=pts, tol=tol)
+    L, x, lam, dp = loss_and_grad(m, b, t)
+
+    def central(eps):
+        Lp = loss_and_grad(build(N, H0 + eps, pts=pts, tol=tol), b, t)[0]
+        Lm = loss_and_grad(build(N, H0 - eps, pts=pts, tol=tol), b, t)[0]
+        return (Lp - Lm) / (2 * eps)
+
+    # Richardson extrapolation of two central differences removes the O(eps^2) term
+    e = 2e-3 * H0
+    fd = (4.0 * central(e / 2) - central(e)) / 3.0
+    assert abs(dp[0] - fd) <= 1e-6 * abs(fd), (dp[0], fd)
+
+
+def test_db_through_autograd_against_central_differences():
+    torch = pytest.importorskip("torch")
+    from hodlr_autograd import HodlrSolve
+
+    N = 4096
+    m = build(N)
+    rng = np.random.default_rng(3)
+    b = torch.tensor(rng.standard_normal(N), requires_grad=True)
+    t = torch.tensor(rng.standard_normal(N))
+    L = ((HodlrSolve.apply(b, m) - t) ** 2).sum()
+    L.backward()
+    for i in (0, 1234, N - 1):
+        e = np.zeros(N)
+        e[i] = 1e-3
+        bp, bm = b.detach().numpy() + e, b.detach().numpy() - e
+        fd = (((m.solve(bp) - t.numpy()) ** 2).sum() - ((m.solve(bm) - t.numpy()) ** 2).sum()) / 2e-3
+        assert abs(b.grad[i].item() - fd) <= 1e-6 * max(1.0, abs(fd))
+
+
+def test_factor_gradients_against_finite_differences():
+    """dL/dD, dL/dU, dL/dV, dL/dB12 of the HODLR representation, by perturbing one entry
+    of each imported factor."""
+    N = 2048
+    pts = points(N)
+    A = O.gaussian_matrix(pts, H0, SHIFT)
+    o = O.HodlrOracle(1e-12, RANK)
+    o.build_from_dense(A, LEAF, O.SketchSource(4, "normal"))
+    rng = np.random.default_rng(4)
+    b, t = rng.standard_normal(N), rng.standard_normal(N)
+
+    def handle():
+        m = H.HODLRMatrix(1e-12)
+        m.import_factors(N, LEAF, o.nodes)
+        return m
+
+    m = handle()
+    L, x, lam, _ = loss_and_grad(m, b, t)
+    leaf = next(n for n in o.nodes if n.is_leaf)
+    inner = o.nodes[0]
+    child = o.nodes[1]
+    checks = [(leaf, "D", H.HODLRMatrix.D, (3, 5)), (child, "U", H.HODLRMatrix.U, (7, 0)),
+              (child, "V", H.HODLRMatrix.V, (11, 1)), (inner, "B12", H.HODLRMatrix.B12, (0, 0))]
+    for node, attr, which, (i, j) in checks:
+        G = m.get_gradient(node.index, which)
+        M0 = getattr(node, attr)
+        eps = 1e-6 * max(1.0, abs(M0[i, j]))
+        vals = []
+        for sgn in (1, -1):
+            Mp = M0.copy()
+            Mp[i, j] += sgn * eps
+            setattr(node, attr, Mp)
+            vals.append(loss_and_grad(handle(), b, t)[0])
+        setattr(node, attr, M0)
+        fd = (vals[0] - vals[1]) / (2 * eps)
+        assert abs(G[i, j] - fd) <= 1e-5 * max(abs(fd), 1e-3 * abs(L)), (attr, G[i, j], fd)
