@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--nrhs", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="one profiled step, no timing")
+    ap.add_argument("--workload", default="headline", choices=["headline", "batched"])
+    ap.add_argument("--systems", type=int, default=512)
+    ap.add_argument("--refine", type=int, default=1, help="FP64 refinement steps (batched workload)")
     return ap.parse_args()
 
 
@@ -326,6 +329,69 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batched(args):
+    """Configuration 4: 512 independent HODLR systems (seed 4): N log-uniform integer in
+    [1024, 32768], Gaussian kernel with h log-uniform in [0.01, 0.2] and shift 1e-2 on
+    sorted uniform points, leaf 64, ranks <= 48, 1-64 right-hand sides each (uniform
+    integer), FP64.  A step = factor + solve of every system; all systems share every
+    launch.  Prints one JSON line (not the headline metric)."""
+    import torch
+    import hmat_b200 as H
+    import hmat_oracle as O
+
+    rng = np.random.default_rng(4)
+    nsys = args.systems
+    Ns = np.exp(rng.uniform(np.log(1024), np.log(32768), nsys)).astype(int)
+    hs = np.exp(rng.uniform(np.log(0.01), np.log(0.2), nsys))
+    ss = rng.integers(1, 65, nsys)
+    pts = [np.sort(rng.random(n)) for n in Ns]
+    B = H.HODLRBatch(1e-10, rsvd_rank=48, max_rank=48, oversample=10, sketch=H.SKETCH_DEVICE_NORMAL, seed=0,
+                     refine_steps=args.refine)
+    stream = torch.cuda.current_stream()
+    B.set_stream(stream.cuda_stream)
+    t0 = time.perf_counter()
+    B.build_from_kernel(H.KERNEL_GAUSSIAN, pts, [[h, 1e-2] for h in hs], 64)
+    t_build = time.perf_counter() - t0
+    bs = [rng.standard_normal((n, s)) for n, s in zip(Ns, ss)]
+    cols, packed = B._packed(bs)
+    db = torch.from_numpy(packed).cuda()
+    dx = torch.empty_like(db)
+    cp = cols.ctypes.data_as(H._ip)
+    import ctypes
+
+    def step():
+        B.factor()
+        B._check(B._L.hm_batch_solve(B._h, ctypes.c_void_p(db.data_ptr()), cp, ctypes.c_void_p(dx.data_ptr())))
+
+    for _ in range(args.warmup):
+        step()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    n0 = H.launch_count()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    launches = (H.launch_count() - n0) // args.steps
+    xs = B._unpack(dx.cpu().numpy(), cols)
+    ys = B.multiply(xs)
+    back = [O.rel_err(b, y) for b, y in zip(bs, ys)]
+    small = np.argsort(Ns)[:6]
+    fwd = [O.rel_err(np.linalg.solve(O.gaussian_matrix(pts[k], hs[k], 1e-2), bs[k]), xs[k]) for k in small]
+    total_rhs = int(ss.sum())
+    print(json.dumps({
+        "metric": "batched HODLR factor+solve RHS/s (512 systems, N in [1024, 32768])", "value": total_rhs / (ms / 1e3),
+        "unit": "RHS/s", "systems_per_s": nsys / (ms / 1e3), "ms_per_step": ms, "steps": args.steps,
+        "warmup": args.warmup, "dtype": "f64", "data": "synthetic", "gpu_launches": int(launches),
+        "config": {"workload": "batched_gaussian_hodlr", "systems": nsys, "rows_total": int(Ns.sum()),
+                   "rhs_total": total_rhs, "leaf": 64, "max_rank": 48},
+        "build_s": t_build, "backward_error_max": max(back),
+        "forward_error_vs_dense_smallest6": fwd,
+    }))
+
+
 def roofline(prof: dict):
     peaks = {}
     try:
@@ -346,6 +412,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched":
+        run_batched(args)
     else:
         run_ours(args)
 

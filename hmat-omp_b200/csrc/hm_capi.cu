@@ -79,6 +79,7 @@ void hm_opts_default(hm_opts* o) {
     o->precision = HM_FP64;
     o->ir_tol = 1e-10;
     o->ir_max_iter = 30;
+    o->refine_steps = 0;
 }
 
 int hm_create(const hm_opts* o, hm_handle** out) {
@@ -218,6 +219,29 @@ int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ld
         built(h).solve_device(b, nrhs, ldb, x, ldx, st);    // host pointers: unified addressing
         HM_CUDA(cudaStreamSynchronize(h->stream));
     });
+}
+
+int hm_batch_build_from_kernel(hm_handle* h, int kernel, const double* points, int dim, int nsys, const int* N,
+                               const double* params, int leaf) {
+    return guard(h, [&] {
+        HM_CHECK(params && nsys >= 1, HM_ERR_ARG, "batch build: bad arguments");
+        const int gen = kernel == HM_KERNEL_GAUSSIAN ? hm::GEN_GAUSSIAN : kernel == HM_KERNEL_COULOMB ? hm::GEN_COULOMB : -1;
+        HM_CHECK(gen > 0, HM_ERR_ARG, "batch build: Gaussian or Coulomb kernel");
+        std::vector<double> p0(nsys), p1(nsys);
+        for (int k = 0; k < nsys; ++k) { p0[k] = params[2 * k]; p1[k] = params[2 * k + 1]; }
+        engine(h, hm::Engine::HODLR).build_batch_kernel(gen, points, dim, nsys, N, p0.data(), p1.data(), leaf);
+        HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int hm_num_systems(const hm_handle* h) { return (h && h->eng) ? h->eng->num_systems() : 0; }
+
+int hm_batch_solve(hm_handle* h, const double* b, const int* nrhs, double* x) {
+    return guard(h, [&] { built(h).batch_solve(b, nrhs, x); });
+}
+
+int hm_batch_multiply(hm_handle* h, const double* x, const int* nrhs, double* y) {
+    return guard(h, [&] { built(h).batch_multiply(x, nrhs, y); });
 }
 
 int hm_solve_transpose_device(hm_handle* h, const double* dg, int nrhs, int ldg, double* dl, int ldl) {

@@ -248,10 +248,24 @@ __global__ void __launch_bounds__(256) jacobi_kernel(const EigDesc* __restrict__
         int i = e % k, j = e / k;
         W[i + (size_t)j * ldw] = (i == j) ? 1.0 : 0.0;
     }
+    // Rotation test: |a_pq| > eps sqrt(a_pp a_qq), relative, so graded matrices keep their
+    // small eigenvalues to high relative accuracy.  Columns whose diagonal is at most 1e-30
+    // of the largest (singular values below 1e-15 sigma_0: rounding, not signal) are dead:
+    // they are not rotated, and the caller turns them into zero columns.  Orthogonalising
+    // noise among itself to relative precision would take tens of sweeps (and never ends
+    // once entries reach the denormal range) without changing any result above 1e-15.
+    __shared__ double s_dmax;
+    if (tid == 0) {
+        double dm = 0.0;
+        for (int i = 0; i < k; ++i) dm = fmax(dm, fabs(g[i + i * ld]));
+        s_dmax = dm;
+    }
     __syncthreads();
+    const double dead = 1e-30 * s_dmax;
+    const double floor_abs = 1e-290;
     const double eps = 4.0 * 2.220446049250313e-16;
     int sweep = 0;
-    bool converged = (k == 1);
+    bool converged = (k == 1) || s_dmax == 0.0;
     for (; sweep < max_sweeps && !converged; ++sweep) {
         if (tid == 0) s_rot = 0;
         __syncthreads();
@@ -263,7 +277,7 @@ __global__ void __launch_bounds__(256) jacobi_kernel(const EigDesc* __restrict__
                 if (q < k) {
                     const double app = g[p + p * ld], aqq = g[q + q * ld], apq = g[p + q * ld];
                     const double thr = eps * sqrt(fabs(app)) * sqrt(fabs(aqq));
-                    if (fabs(apq) > thr && apq != 0.0) {
+                    if (app > dead && aqq > dead && fabs(apq) > thr && fabs(apq) > floor_abs) {
                         const double tau = (aqq - app) / (2.0 * apq);
                         const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + hypot(1.0, tau));
                         c = 1.0 / sqrt(1.0 + tt * tt);
@@ -406,9 +420,13 @@ __global__ void __launch_bounds__(256) prep_kernel(const PrepDesc* __restrict__ 
         perm[pos] = i;
     }
     __syncthreads();
+    // singular values at or below 1e-15 of the largest are rounding (dead Jacobi columns):
+    // zero, so the permute step writes zero columns for them
+    const double smax = sg[perm[0]];
     for (int c = tid; c < k; c += nt) {
         d.perm[c] = perm[c];
-        if (d.sigma) d.sigma[c] = sg[perm[c]];
+        const double v = sg[perm[c]];
+        if (d.sigma) d.sigma[c] = v > 1e-15 * smax ? v : 0.0;
     }
     if (d.rank && tid == 0) {
         // compression.h:42-46: #{S_i > tol*S_0} when S_0 > 1e-15, at least 1
@@ -431,11 +449,12 @@ void launch_prep(const DevTable<PrepDesc>& t, double tol, int max_rank, cudaStre
     HM_CUDA(cudaGetLastError());
 }
 
+// Table kernels: blockIdx.x = problem (no 65535 limit), blockIdx.y = slice of its elements.
 __global__ void permute_kernel(const PermDesc* __restrict__ descs) {
-    const PermDesc d = descs[blockIdx.y];
+    const PermDesc d = descs[blockIdx.x];
     const size_t total = (size_t)d.rows * d.k;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
-         e += (size_t)gridDim.x * blockDim.x) {
+    for (size_t e = blockIdx.y * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.y * blockDim.x) {
         const int i = (int)(e % d.rows), c = (int)(e / d.rows);
         const int src = d.perm[c];
         double v = d.src[i + (size_t)src * d.lds];
@@ -452,8 +471,7 @@ void launch_permute(const DevTable<PermDesc>& t, cudaStream_t s) {
     size_t mx = 0;
     for (auto& d : t.h) mx = std::max(mx, (size_t)d.rows * d.k);
     int gx = (int)std::min<size_t>(std::max<size_t>(1, (mx + 255) / 256), 1024);
-    HM_CHECK(t.size() <= 65535, HM_ERR_UNSUPPORTED, "permute batch too large");
-    permute_kernel<<<dim3(gx, t.size()), 256, 0, s>>>(t.d.p);
+    permute_kernel<<<dim3(t.size(), gx), 256, 0, s>>>(t.d.p);
     HM_CUDA(cudaGetLastError());
 }
 
@@ -461,10 +479,10 @@ void launch_permute(const DevTable<PermDesc>& t, cudaStream_t s) {
 // Copies (optionally transposed, optionally to FP32) and identity fills
 // ---------------------------------------------------------------------------------
 __global__ void copy_kernel(const CopyDesc* __restrict__ descs) {
-    const CopyDesc d = descs[blockIdx.y];
+    const CopyDesc d = descs[blockIdx.x];
     const size_t total = (size_t)d.rows * d.cols;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
-         e += (size_t)gridDim.x * blockDim.x) {
+    for (size_t e = blockIdx.y * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.y * blockDim.x) {
         const int i = (int)(e % d.rows), j = (int)(e / d.rows);
         const size_t si = d.trans ? j + (size_t)i * d.lds : i + (size_t)j * d.lds;
         const double v = d.src_f32 ? (double)static_cast<const float*>(d.src)[si]
@@ -480,16 +498,15 @@ void launch_copy(const DevTable<CopyDesc>& t, cudaStream_t s) {
     size_t mx = 0;
     for (auto& d : t.h) mx = std::max(mx, (size_t)d.rows * d.cols);
     int gx = (int)std::min<size_t>(std::max<size_t>(1, (mx + 255) / 256), 2048);
-    HM_CHECK(t.size() <= 65535, HM_ERR_UNSUPPORTED, "copy batch too large");
-    copy_kernel<<<dim3(gx, t.size()), 256, 0, s>>>(t.d.p);
+    copy_kernel<<<dim3(t.size(), gx), 256, 0, s>>>(t.d.p);
     HM_CUDA(cudaGetLastError());
 }
 
 __global__ void ident_kernel(const IdentDesc* __restrict__ descs) {
-    const IdentDesc d = descs[blockIdx.y];
+    const IdentDesc d = descs[blockIdx.x];
     const size_t total = (size_t)d.rows * d.cols;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
-         e += (size_t)gridDim.x * blockDim.x) {
+    for (size_t e = blockIdx.y * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.y * blockDim.x) {
         const int i = (int)(e % d.rows), j = (int)(e / d.rows);
         d.X[i + (size_t)j * d.ldx] = (i == j) ? d.diag : 0.0;
     }
@@ -500,8 +517,7 @@ void launch_ident(const DevTable<IdentDesc>& t, cudaStream_t s) {
     size_t mx = 0;
     for (auto& d : t.h) mx = std::max(mx, (size_t)d.rows * d.cols);
     int gx = (int)std::min<size_t>(std::max<size_t>(1, (mx + 255) / 256), 1024);
-    HM_CHECK(t.size() <= 65535, HM_ERR_UNSUPPORTED, "identity batch too large");
-    ident_kernel<<<dim3(gx, t.size()), 256, 0, s>>>(t.d.p);
+    ident_kernel<<<dim3(t.size(), gx), 256, 0, s>>>(t.d.p);
     HM_CUDA(cudaGetLastError());
 }
 

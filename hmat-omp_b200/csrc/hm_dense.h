@@ -94,7 +94,7 @@ struct DevTable {
 };
 
 void launch_gj(const DevTable<GJDesc>& t, int nb, int* status, cudaStream_t s);
-void launch_jacobi(const DevTable<EigDesc>& t, int* status, cudaStream_t s, int max_sweeps = 40);
+void launch_jacobi(const DevTable<EigDesc>& t, int* status, cudaStream_t s, int max_sweeps = 60);
 void launch_prep(const DevTable<PrepDesc>& t, double tol, int max_rank, cudaStream_t s);
 void launch_norms(const DevTable<NormDesc>& t, cudaStream_t s);
 void launch_permute(const DevTable<PermDesc>& t, cudaStream_t s);

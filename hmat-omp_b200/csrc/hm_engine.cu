@@ -25,6 +25,9 @@
 
 namespace hm {
 
+template <> Plan& Engine::solve_plan<double>(FactorStore<double>& fs, const std::vector<int>& sc);
+template <> Plan& Engine::solve_plan<float>(FactorStore<float>& fs, const std::vector<int>& sc);
+
 // ---------------------------------------------------------------------------------
 // Trees
 // ---------------------------------------------------------------------------------
@@ -131,6 +134,12 @@ __global__ void residual_kernel(const double* __restrict__ b, double* __restrict
         atomicAdd(&nr2[j], a2);
         atomicAdd(&nb2[j], c2);
     }
+}
+
+// out = a*x + b*y (out may alias x or y)
+__global__ void axpby_kernel(double* out, const double* x, double a, const double* y, double b, size_t n) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+        out[e] = a * x[e] + b * y[e];
 }
 
 // x += double(d)
@@ -285,6 +294,8 @@ void Engine::begin_build(int N, int leaf) {
     gen_ = GEN_DENSE;
     gp_ = GenParams();
     nodes_ = kind_ == HODLR ? hodlr_tree(N, leaf) : hss_tree(N, leaf);
+    sys_N_ = {N};
+    sys_off_ = {0};
     plan_levels();
     if (!dstatus.p) dstatus.alloc(1);
     dstatus.zero(stream_);
@@ -310,6 +321,151 @@ void Engine::build_dense_device(const double* dA, int N, int lda, int leaf) {
     if (kind_ == HODLR) build_hodlr(src);
     else build_hss(src);
     built_ = true;
+}
+
+void Engine::build_batch_kernel(int gen, const double* pts, int dim, int nsys, const int* Ns, const double* p0s,
+                                const double* p1s, int leaf) {
+    HM_CHECK(kind_ == HODLR, HM_ERR_UNSUPPORTED, "batches are HODLR systems");
+    HM_CHECK(gen == GEN_GAUSSIAN || gen == GEN_COULOMB, HM_ERR_ARG, "batch kernel: Gaussian or Coulomb");
+    HM_CHECK(nsys >= 1 && Ns && p0s && p1s && pts && dim >= 1 && dim <= 3 && leaf > 0, HM_ERR_ARG,
+             "batch build: bad arguments");
+    std::vector<int> off(nsys + 1, 0);
+    for (int k = 0; k < nsys; ++k) {
+        HM_CHECK(Ns[k] > 0, HM_ERR_ARG, "batch build: system sizes must be positive");
+        HM_CHECK((long long)off[k] + Ns[k] < (1LL << 31), HM_ERR_UNSUPPORTED, "batch too large");
+        off[k + 1] = off[k] + Ns[k];
+    }
+    const int Ntot = off[nsys];
+    for (size_t i = 0; i < (size_t)Ntot * dim; ++i)
+        HM_CHECK(std::isfinite(pts[i]), HM_ERR_NONFINITE, "batch build: non-finite point");
+    begin_build(Ntot, leaf);
+    // forest: each system's pre-order tree on its own rows
+    nodes_.clear();
+    for (int k = 0; k < nsys; ++k) {
+        std::vector<Node> t = hodlr_tree(Ns[k], leaf);
+        const int base = (int)nodes_.size();
+        for (auto& n : t) {
+            n.start += off[k];
+            n.end += off[k];
+            n.sys = k;
+            if (n.parent >= 0) n.parent += base;
+            if (n.left >= 0) n.left += base;
+            if (n.right >= 0) n.right += base;
+            nodes_.push_back(n);
+        }
+    }
+    sys_N_.assign(Ns, Ns + nsys);
+    sys_off_.assign(off.begin(), off.end() - 1);
+    plan_levels();
+    std::vector<int> rs(Ntot);
+    for (int k = 0; k < nsys; ++k)
+        for (int i = off[k]; i < off[k + 1]; ++i) rs[i] = k;
+    dPts.alloc((size_t)Ntot * dim);
+    dRowSys.alloc(Ntot);
+    dSysP0.alloc(nsys);
+    dSysP1.alloc(nsys);
+    HM_CUDA(cudaMemcpyAsync(dPts.p, pts, (size_t)Ntot * dim * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    HM_CUDA(cudaMemcpyAsync(dRowSys.p, rs.data(), rs.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
+    HM_CUDA(cudaMemcpyAsync(dSysP0.p, p0s, nsys * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    HM_CUDA(cudaMemcpyAsync(dSysP1.p, p1s, nsys * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    HM_CUDA(cudaStreamSynchronize(stream_));
+    Source src;
+    src.gen = gen;
+    src.gp.pts = dPts.p;
+    src.gp.N = Ntot;
+    src.gp.dim = dim;
+    src.gp.row_sys = dRowSys.p;
+    src.gp.p0v = dSysP0.p;
+    src.gp.p1v = dSysP1.p;
+    build_hodlr(src);
+    built_ = true;  // no kernel-parameter gradient for batches (gen_ stays dense)
+}
+
+// packed (system k: N_k x s_k at offset sum_{j<k} N_j s_j) <-> staging (rows global, ld N)
+static std::vector<CopyDesc> packed_copies(const std::vector<int>& Ns, const std::vector<int>& off,
+                                           const std::vector<int>& sc, double* packed, double* staging, int N,
+                                           bool to_staging, size_t* total) {
+    std::vector<CopyDesc> out;
+    size_t p = 0;
+    for (size_t k = 0; k < Ns.size(); ++k) {
+        if (sc[k] > 0) {
+            CopyDesc c{};
+            if (to_staging) {
+                c.src = packed + p; c.lds = Ns[k]; c.dst = staging + off[k]; c.ldd = N;
+            } else {
+                c.src = staging + off[k]; c.lds = N; c.dst = packed + p; c.ldd = Ns[k];
+            }
+            c.rows = Ns[k];
+            c.cols = sc[k];
+            out.push_back(c);
+        }
+        p += (size_t)Ns[k] * sc[k];
+    }
+    *total = p;
+    return out;
+}
+
+void Engine::batch_solve(const double* b, const int* nrhs, double* x) {
+    HM_CHECK(built_, HM_ERR_STATE, "batch solve before build");
+    HM_CHECK(b && nrhs && x, HM_ERR_ARG, "batch solve: bad arguments");
+    HM_CHECK(opts_.precision == HM_FP64, HM_ERR_UNSUPPORTED, "batched solves run in FP64");
+    std::vector<int> sc(nrhs, nrhs + sys_N_.size());
+    int smax = 0;
+    for (int s : sc) {
+        HM_CHECK(s >= 0, HM_ERR_ARG, "batch solve: negative column count");
+        smax = std::max(smax, s);
+    }
+    if (smax == 0) return;
+    if (!factored_) factor();
+    ensure_io(smax);
+    size_t total = 0;
+    auto in = packed_copies(sys_N_, sys_off_, sc, nullptr, ioX.p, N_, true, &total);
+    if (ioPacked.n < total) ioPacked.alloc(total);
+    const bool refine = opts_.refine_steps > 0;
+    if (refine && ioAcc.n < (size_t)N_ * smax) ioAcc.alloc((size_t)N_ * smax);
+    in = packed_copies(sys_N_, sys_off_, sc, ioPacked.p, refine ? ioR.p : ioX.p, N_, true, &total);
+    auto outc = packed_copies(sys_N_, sys_off_, sc, ioPacked.p, refine ? ioAcc.p : ioY.p, N_, false, &total);
+    HM_CUDA(cudaMemcpyAsync(ioPacked.p, b, total * sizeof(double), cudaMemcpyDefault, stream_));
+    CopyStep cin, cout;
+    cin.t.h = in;
+    cout.t.h = outc;
+    cin.t.upload(stream_);
+    cout.t.upload(stream_);
+    cin.run(stream_, dstatus.p);
+    count_launch();
+    if (refine) refined_fp64(sc, smax);
+    else solve_plan<double>(f64_, sc).run(stream_, dstatus.p);
+    cout.run(stream_, dstatus.p);
+    count_launch();
+    HM_CUDA(cudaMemcpyAsync(x, ioPacked.p, total * sizeof(double), cudaMemcpyDefault, stream_));
+    HM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::batch_multiply(const double* xin, const int* nrhs, double* y) {
+    HM_CHECK(built_, HM_ERR_STATE, "batch multiply before build");
+    HM_CHECK(xin && nrhs && y, HM_ERR_ARG, "batch multiply: bad arguments");
+    std::vector<int> sc(nrhs, nrhs + sys_N_.size());
+    int smax = 0;
+    for (int s : sc) smax = std::max(smax, s);
+    if (smax == 0) return;
+    ensure_io(smax);
+    size_t total = 0;
+    packed_copies(sys_N_, sys_off_, sc, nullptr, ioX.p, N_, true, &total);
+    if (ioPacked.n < total) ioPacked.alloc(total);
+    auto in = packed_copies(sys_N_, sys_off_, sc, ioPacked.p, ioX.p, N_, true, &total);
+    auto outc = packed_copies(sys_N_, sys_off_, sc, ioPacked.p, ioY.p, N_, false, &total);
+    HM_CUDA(cudaMemcpyAsync(ioPacked.p, xin, total * sizeof(double), cudaMemcpyDefault, stream_));
+    CopyStep cin, cout;
+    cin.t.h = in;
+    cout.t.h = outc;
+    cin.t.upload(stream_);
+    cout.t.upload(stream_);
+    cin.run(stream_, dstatus.p);
+    matvec_plan(sc).run(stream_, dstatus.p);
+    cout.run(stream_, dstatus.p);
+    count_launch(2);
+    HM_CUDA(cudaMemcpyAsync(y, ioPacked.p, total * sizeof(double), cudaMemcpyDefault, stream_));
+    HM_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void Engine::build_kernel(int gen, const double* pts, size_t npts, int dim, int N, double p0, double p1,
@@ -384,7 +540,8 @@ void Engine::build_hodlr(const Source& src) {
             blocks.push_back(b);
         }
     };
-    post(0);
+    for (size_t r = 0; r < nodes_.size(); ++r)  // every system's root, system after system
+        if (nodes_[r].parent < 0) post((int)r);
     HM_CHECK((int)blocks.size() <= 1 << 26, HM_ERR_UNSUPPORTED, "tree too large");
     // capacities
     for (auto& b : blocks) {
@@ -1158,13 +1315,15 @@ void Engine::ensure_io(int s) {
 }
 
 // y = A x for s columns: in = x (ld N), out = y (ld N)
+// sc[k]: right-hand-side columns of system k (rows of all systems share ld N)
 static void add_matvec(Plan& pl, const std::vector<Node>& nodes, const std::vector<int>& leaves,
                        const std::vector<std::vector<int>>& levels, const double* dD, const double* dU,
-                       const double* dV, const double* dB, const double* X, double* Y, int N, int s,
-                       cudaStream_t st) {
+                       const double* dV, const double* dB, const double* X, double* Y, int N,
+                       const std::vector<int>& sc, cudaStream_t st) {
     auto gLeaf = std::make_unique<GemmStep<double>>();
     for (int l : leaves) {
         const Node& n = nodes[l];
+        const int s = sc[n.sys];
         gLeaf->batch.add(n.len(), s, n.len(), 1.0, dD + n.offD, n.len(), OP_N, X + n.start, N, OP_N,
                          0.0, Y + n.start, N);
     }
@@ -1178,6 +1337,8 @@ static void add_matvec(Plan& pl, const std::vector<Node>& nodes, const std::vect
             const Node& L = nodes[n.left];
             const Node& R = nodes[n.right];
             const int p1 = L.rankU, p2 = R.rankU, q1 = L.rankV, q2 = R.rankV;
+            const int s = sc[n.sys];
+            if (s == 0) continue;
             double* T = pl.scratch(std::max<size_t>((size_t)(q1 + q2) * s, 1));
             double* Dl = pl.scratch(std::max<size_t>((size_t)(p1 + p2) * s, 1));
             // T1 = V1^T x1, T2 = V2^T x2
@@ -1206,11 +1367,11 @@ static void add_matvec(Plan& pl, const std::vector<Node>& nodes, const std::vect
     }
 }
 
-Plan& Engine::matvec_plan(int s) {
-    auto it = mv_plans_.find(s);
+Plan& Engine::matvec_plan(const std::vector<int>& sc) {
+    auto it = mv_plans_.find(sc);
     if (it != mv_plans_.end()) return it->second;
-    Plan& pl = mv_plans_[s];
-    add_matvec(pl, nodes_, leaves_, levels_, dD.p, dU.p, dV.p, dB.p, ioX.p, ioY.p, N_, s, stream_);
+    Plan& pl = mv_plans_[sc];
+    add_matvec(pl, nodes_, leaves_, levels_, dD.p, dU.p, dV.p, dB.p, ioX.p, ioY.p, N_, sc, stream_);
     return pl;
 }
 
@@ -1218,11 +1379,13 @@ Plan& Engine::matvec_plan(int s) {
 template <typename T>
 static void add_solve(Plan& pl, const std::vector<Node>& nodes, const std::vector<int>& leaves,
                       const std::vector<std::vector<int>>& levels, const T* Dinv, const T* Vt,
-                      const T* Q, const T* P, const T* X, T* Z, int N, int s, cudaStream_t st) {
+                      const T* Q, const T* P, const T* X, T* Z, int N, const std::vector<int>& sc,
+                      cudaStream_t st) {
     constexpr bool F32 = std::is_same<T, float>::value;
     auto gLeaf = std::make_unique<GemmStep<T>>();
     for (int l : leaves) {
         const Node& n = nodes[l];
+        const int s = sc[n.sys];
         gLeaf->batch.add(n.len(), s, n.len(), T(1), Dinv + n.offD, n.len(), OP_N, X + n.start, N, OP_N,
                          T(0), Z + n.start, N);
     }
@@ -1238,6 +1401,8 @@ static void add_solve(Plan& pl, const std::vector<Node>& nodes, const std::vecto
             const Node& R = nodes[n.right];
             const int p1 = L.rankU, p2 = R.rankU, q1 = L.rankV, q2 = R.rankV;
             const int p = p1 + p2, q = q1 + q2;
+            const int s = sc[n.sys];
+            if (s == 0) continue;
             T* Tt = F32 ? reinterpret_cast<T*>(pl.scratch_f(std::max<size_t>((size_t)q * s, 1)))
                         : reinterpret_cast<T*>(pl.scratch(std::max<size_t>((size_t)q * s, 1)));
             T* Dt = F32 ? reinterpret_cast<T*>(pl.scratch_f(std::max<size_t>((size_t)p * s, 1)))
@@ -1260,22 +1425,22 @@ static void add_solve(Plan& pl, const std::vector<Node>& nodes, const std::vecto
 }
 
 template <>
-Plan& Engine::solve_plan<double>(FactorStore<double>& fs, int s) {
-    auto it = solve64_plans_.find(s);
+Plan& Engine::solve_plan<double>(FactorStore<double>& fs, const std::vector<int>& sc) {
+    auto it = solve64_plans_.find(sc);
     if (it != solve64_plans_.end()) return it->second;
-    Plan& pl = solve64_plans_[s];
-    add_solve<double>(pl, nodes_, leaves_, levels_, dDinv.p, dV.p, fs.Q.p, fs.P.p, ioX.p, ioY.p, N_, s,
+    Plan& pl = solve64_plans_[sc];
+    add_solve<double>(pl, nodes_, leaves_, levels_, dDinv.p, dV.p, fs.Q.p, fs.P.p, ioX.p, ioY.p, N_, sc,
                       stream_);
     return pl;
 }
 
 template <>
-Plan& Engine::solve_plan<float>(FactorStore<float>& fs, int s) {
-    auto it = solve32_plans_.find(s);
+Plan& Engine::solve_plan<float>(FactorStore<float>& fs, const std::vector<int>& sc) {
+    auto it = solve32_plans_.find(sc);
     if (it != solve32_plans_.end()) return it->second;
-    Plan& pl = solve32_plans_[s];
+    Plan& pl = solve32_plans_[sc];
     add_solve<float>(pl, nodes_, leaves_, levels_, fs.Dinv.p, fs.V.p, fs.Q.p, fs.P.p, ioXf.p, ioYf.p,
-                     N_, s, stream_);
+                     N_, sc, stream_);
     return pl;
 }
 
@@ -1294,15 +1459,41 @@ void Engine::multiply_device(const double* dx, int s, int ldx, double* dy, int l
     HM_CHECK(s >= 1 && ldx >= N_ && ldy >= N_ && dx && dy, HM_ERR_ARG, "multiply: bad arguments");
     ensure_io(s);
     copy_in(ioX.p, dx, N_, s, ldx, stream_);
-    matvec_plan(s).run(stream_, dstatus.p);
+    matvec_plan(uniform(s)).run(stream_, dstatus.p);
     copy_out(dy, ldy, ioY.p, N_, s, stream_);
 }
 
 void Engine::solve_fp64(const double* db, int s, int ldb, double* dx, int ldx) {
     ensure_io(s);
-    copy_in(ioX.p, db, N_, s, ldb, stream_);
-    solve_plan<double>(f64_, s).run(stream_, dstatus.p);
-    copy_out(dx, ldx, ioY.p, N_, s, stream_);
+    if (opts_.refine_steps <= 0) {
+        copy_in(ioX.p, db, N_, s, ldb, stream_);
+        solve_plan<double>(f64_, uniform(s)).run(stream_, dstatus.p);
+        copy_out(dx, ldx, ioY.p, N_, s, stream_);
+        return;
+    }
+    copy_in(ioR.p, db, N_, s, ldb, stream_);
+    copy_out(dx, ldx, refined_fp64(uniform(s), s), N_, s, stream_);
+}
+
+// b in ioR (staging, ld N); returns the staging buffer holding x after the direct solve
+// and opts_.refine_steps steps of x += A^{-1}(b - A x), all in FP64 with one factorization.
+const double* Engine::refined_fp64(const std::vector<int>& sc, int smax) {
+    const size_t n = (size_t)N_ * smax;
+    if (ioAcc.n < n) ioAcc.alloc(n);
+    Plan& sp = solve_plan<double>(f64_, sc);
+    HM_CUDA(cudaMemcpyAsync(ioX.p, ioR.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    sp.run(stream_, dstatus.p);
+    HM_CUDA(cudaMemcpyAsync(ioAcc.p, ioY.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    Plan& mp = matvec_plan(sc);
+    for (int it = 0; it < opts_.refine_steps; ++it) {
+        HM_CUDA(cudaMemcpyAsync(ioX.p, ioAcc.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        mp.run(stream_, dstatus.p);                                   // ioY = A x
+        axpby_kernel<<<grid_for(n), 256, 0, stream_>>>(ioX.p, ioR.p, 1.0, ioY.p, -1.0, n);  // r = b - A x
+        sp.run(stream_, dstatus.p);                                   // ioY = A^{-1} r
+        axpby_kernel<<<grid_for(n), 256, 0, stream_>>>(ioAcc.p, ioAcc.p, 1.0, ioY.p, 1.0, n);
+        count_launch(2);
+    }
+    return ioAcc.p;
 }
 
 // Mixed precision: FP32 factor sweeps, refined against the FP64 operator
@@ -1316,8 +1507,8 @@ void Engine::solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, 
     copy_in(bcopy, db, N_, s, ldb, q);
     to_float_kernel<<<grid_for((size_t)N_ * s), 256, 0, q>>>(bcopy, ioXf.p, (size_t)N_ * s);
     count_launch();
-    Plan& sp = solve_plan<float>(f32_, s);
-    Plan& mp = matvec_plan(s);
+    Plan& sp = solve_plan<float>(f32_, uniform(s));
+    Plan& mp = matvec_plan(uniform(s));
     std::vector<double> hn(2 * (size_t)s);
     double worst = 0.0;
     int it = 0;

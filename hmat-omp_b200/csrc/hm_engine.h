@@ -16,6 +16,7 @@ struct Node {
     int start = 0, end = 0, depth = 0;
     int is_leaf = 0;
     int left = -1, right = -1, parent = -1;
+    int sys = 0;   // independent system this node belongs to (batches); rows are global
     int len() const { return end - start; }
     int mid() const { return (start + end) / 2; }
     // Basis blocks owned by a non-root node (rows of this node):
@@ -81,6 +82,14 @@ class Engine {
     // Matrix-free build: points (host) in the layout GenParams documents.
     void build_kernel(int gen, const double* pts_host, size_t npts, int dim, int N, double p0, double p1,
                       int leaf);
+    // Many independent HODLR systems built from one kernel with per-system parameters
+    // (points concatenated system after system); all share every launch.
+    void build_batch_kernel(int gen, const double* pts_host, int dim, int nsys, const int* Ns,
+                            const double* p0s, const double* p1s, int leaf);
+    // Packed right-hand sides: system k's N_k x s_k block at offset sum_{j<k} N_j s_j.
+    void batch_solve(const double* b, const int* nrhs, double* x);
+    void batch_multiply(const double* x, const int* nrhs, double* y);
+    int num_systems() const { return (int)sys_N_.size(); }
     void import_hodlr(int N, int leaf, const int* r12, const int* r21, const double* const* D,
                       const double* const* U, const double* const* V, const double* const* B12,
                       const double* const* B21);
@@ -125,12 +134,14 @@ class Engine {
     void check_status(const char* what);
     template <typename T> void factor_t(FactorStore<T>& fs);
     template <typename T> void plan_factor(FactorStore<T>& fs);
-    template <typename T> Plan& solve_plan(FactorStore<T>& fs, int s);
-    Plan& matvec_plan(int s);
+    template <typename T> Plan& solve_plan(FactorStore<T>& fs, const std::vector<int>& sc);
+    Plan& matvec_plan(const std::vector<int>& sc);
+    std::vector<int> uniform(int s) const { return std::vector<int>(sys_N_.size(), s); }
     Plan& solveT_plan(int s);
     void ensure_io(int s);
     std::vector<int> path_of(int n) const;   // n and its ancestors below the root
     void solve_fp64(const double* db, int s, int ldb, double* dx, int ldx);
+    const double* refined_fp64(const std::vector<int>& sc, int smax);
     void solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st);
 
     hm_opts opts_;
@@ -155,10 +166,15 @@ class Engine {
     size_t sizeM_ = 0, sizeP_ = 0;
     bool factored_ = false;
     // I/O staging buffers (ld = N)
-    DBuf<double> ioX, ioY, ioR, ioNorm;
+    DBuf<double> ioX, ioY, ioR, ioNorm, ioAcc;
     DBuf<float> ioXf, ioYf;
     int io_cols_ = 0;
-    std::map<int, Plan> mv_plans_, solve64_plans_, solve32_plans_, solveT_plans_;
+    std::map<std::vector<int>, Plan> mv_plans_, solve64_plans_, solve32_plans_;
+    std::map<int, Plan> solveT_plans_;
+    // independent systems sharing the launches: size and first global row of each
+    std::vector<int> sys_N_{0}, sys_off_{0};
+    DBuf<int> dRowSys;
+    DBuf<double> dSysP0, dSysP1, ioPacked;
     // the build's operator source (kernel generator and its parameters) and gradients
     int gen_ = GEN_DENSE;
     GenParams gp_;

@@ -18,26 +18,28 @@ namespace hm {
 // ---------------------------------------------------------------------------------
 template <int GEN>
 __device__ __forceinline__ double gen_entry(const GenParams& g, int r, int c) {
+    const double p0 = g.p0v ? g.p0v[g.row_sys[r]] : g.p0;
+    const double p1 = g.p1v ? g.p1v[g.row_sys[r]] : g.p1;
     if constexpr (GEN == GEN_CAUCHY) {
         double x = g.pts[r], y = g.pts[g.N + c];
         double v = 1.0 / (x - y);
-        return r == c ? v + g.p0 : v;
+        return r == c ? v + p0 : v;
     } else if constexpr (GEN == GEN_GAUSSIAN) {
         double d2 = 0.0;
         for (int t = 0; t < g.dim; ++t) {
             double d = g.pts[(size_t)r * g.dim + t] - g.pts[(size_t)c * g.dim + t];
             d2 += d * d;
         }
-        double v = exp(-d2 / (2.0 * g.p0 * g.p0));
-        return r == c ? v + g.p1 : v;
+        double v = exp(-d2 / (2.0 * p0 * p0));
+        return r == c ? v + p1 : v;
     } else if constexpr (GEN == GEN_COULOMB) {
         double d2 = 0.0;
         for (int t = 0; t < g.dim; ++t) {
             double d = g.pts[(size_t)r * g.dim + t] - g.pts[(size_t)c * g.dim + t];
             d2 += d * d;
         }
-        double v = 1.0 / (sqrt(d2) + g.p0);
-        return r == c ? v + g.p1 : v;
+        double v = 1.0 / (sqrt(d2) + p0);
+        return r == c ? v + p1 : v;
     } else {
         return 0.0;
     }
@@ -199,10 +201,10 @@ __global__ void zero_regions_kernel(const ZeroRegion<T>* __restrict__ z, int cou
 
 template <int GEN>
 __global__ void gen_fill_kernel(const GenFillDesc* __restrict__ descs, GenParams gp) {
-    const GenFillDesc d = descs[blockIdx.y];
+    const GenFillDesc d = descs[blockIdx.x];
     const size_t total = (size_t)d.rows * d.cols;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
-         e += (size_t)gridDim.x * blockDim.x) {
+    for (size_t e = blockIdx.y * (size_t)blockDim.x + threadIdx.x; e < total;
+         e += (size_t)gridDim.y * blockDim.x) {
         const int i = (int)(e % d.rows), j = (int)(e / d.rows);
         d.dst[i + (size_t)j * d.ldd] =
             d.trans ? gen_entry<GEN>(gp, d.r0 + j, d.c0 + i) : gen_entry<GEN>(gp, d.r0 + i, d.c0 + j);
@@ -212,8 +214,7 @@ __global__ void gen_fill_kernel(const GenFillDesc* __restrict__ descs, GenParams
 void launch_gen_fill(const GenFillDesc* d_descs, int count, int max_elems, int gen, const GenParams& gp,
                      cudaStream_t s) {
     if (count <= 0) return;
-    HM_CHECK(count <= 65535, HM_ERR_UNSUPPORTED, "generator fill batch too large");
-    dim3 grid((unsigned)std::min(std::max(1, (max_elems + 255) / 256), 2048), (unsigned)count);
+    dim3 grid((unsigned)count, (unsigned)std::min(std::max(1, (max_elems + 255) / 256), 2048));
     switch (gen) {
         case GEN_CAUCHY: gen_fill_kernel<GEN_CAUCHY><<<grid, 256, 0, s>>>(d_descs, gp); break;
         case GEN_GAUSSIAN: gen_fill_kernel<GEN_GAUSSIAN><<<grid, 256, 0, s>>>(d_descs, gp); break;

@@ -24,6 +24,11 @@ struct GenParams {
     int N = 0;
     int dim = 1;
     double p0 = 0, p1 = 0;        // kernel parameters (see hmat_b200.h HM_KERNEL_*)
+    // Batches of independent systems: row -> system, and per-system p0/p1 (override
+    // p0/p1 when set).  Blocks never couple two systems.
+    const int* row_sys = nullptr;
+    const double* p0v = nullptr;
+    const double* p1v = nullptr;
 };
 
 template <typename T>

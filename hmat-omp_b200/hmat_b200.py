@@ -44,6 +44,7 @@ class Opts(C.Structure):
         ("precision", C.c_int),
         ("ir_tol", C.c_double),
         ("ir_max_iter", C.c_int),
+        ("refine_steps", C.c_int),
     ]
 
 
@@ -87,6 +88,10 @@ def load() -> C.CDLL:
     L.hm_solve.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_int, C.POINTER(SolveStats)]
     L.hm_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                   C.POINTER(SolveStats)]
+    L.hm_batch_build_from_kernel.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _ip, _dp, C.c_int]
+    L.hm_num_systems.argtypes = [C.c_void_p]
+    L.hm_batch_solve.argtypes = [C.c_void_p, C.c_void_p, _ip, C.c_void_p]
+    L.hm_batch_multiply.argtypes = [C.c_void_p, C.c_void_p, _ip, C.c_void_p]
     L.hm_solve_transpose.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_int]
     L.hm_solve_transpose_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]
     L.hm_gradients.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, _dp]
@@ -327,3 +332,48 @@ class HSSMatrix(_Handle):
         A = np.asfortranarray(A, dtype=np.float64)
         self.N = A.shape[0]
         self._check(self._L.hm_hss_build_from_dense(self._h, _d(A), self.N, self.N, leaf_size))
+
+
+class HODLRBatch(_Handle):
+    """Many independent HODLR systems sharing every launch (hm_batch_*)."""
+
+    def __init__(self, tol: float = 1e-10, **kw):
+        super().__init__(tol, **kw)
+        self.sizes: list[int] = []
+
+    def build_from_kernel(self, kernel: int, points: list, params: list, leaf_size: int):
+        pts = [np.asarray(p, dtype=np.float64).reshape(len(p), -1) for p in points]
+        dim = pts[0].shape[1]
+        self.sizes = [p.shape[0] for p in pts]
+        allp = np.ascontiguousarray(np.vstack(pts))
+        Ns = np.array(self.sizes, dtype=np.int32)
+        pr = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
+        self.N = int(Ns.sum())
+        self._check(self._L.hm_batch_build_from_kernel(self._h, kernel, _d(allp), dim, len(pts),
+                                                       Ns.ctypes.data_as(_ip), _d(pr), leaf_size))
+
+    def _packed(self, blocks):
+        cols = np.array([0 if b is None else (1 if np.ndim(b) == 1 else np.shape(b)[1]) for b in blocks],
+                        dtype=np.int32)
+        parts = [np.asarray(b, dtype=np.float64).reshape(n, -1, order="F").ravel(order="F")
+                 for b, n in zip(blocks, self.sizes) if b is not None]
+        return cols, np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(0))
+
+    def _unpack(self, flat, cols):
+        out, p = [], 0
+        for n, c in zip(self.sizes, cols):
+            out.append(flat[p:p + n * c].reshape(c, n).T.copy() if c else None)
+            p += n * c
+        return out
+
+    def solve(self, blocks: list) -> list:
+        cols, b = self._packed(blocks)
+        x = np.zeros_like(b)
+        self._check(self._L.hm_batch_solve(self._h, b.ctypes.data, cols.ctypes.data_as(_ip), x.ctypes.data))
+        return self._unpack(x, cols)
+
+    def multiply(self, blocks: list) -> list:
+        cols, xin = self._packed(blocks)
+        y = np.zeros_like(xin)
+        self._check(self._L.hm_batch_multiply(self._h, xin.ctypes.data, cols.ctypes.data_as(_ip), y.ctypes.data))
+        return self._unpack(y, cols)

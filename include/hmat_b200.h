@@ -74,6 +74,9 @@ typedef struct hm_opts {
     int precision;       /* HM_FP64, or HM_MIXED (FP32 bulk + FP64 LUs + FP64-residual refinement) */
     double ir_tol;       /* HM_MIXED: target max_j ||b_j - A x_j|| / ||b_j|| */
     int ir_max_iter;     /* HM_MIXED: refinement iteration limit */
+    int refine_steps;    /* HM_FP64: steps of x += A^{-1}(b - A x) with the same factors after the
+                            direct solve (0 = the reference's single solve); restores the backward
+                            error of ill-conditioned operators */
 } hm_opts;
 
 typedef struct hm_handle hm_handle;
@@ -157,6 +160,21 @@ HM_API int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x,
              hm_solve_stats* stats);
 HM_API int hm_solve_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx,
                     hm_solve_stats* stats);
+
+/* ---- many independent systems in shared launches (no counterpart in the reference,
+ *      whose classes hold one operator each) ----
+ * nsys HODLR operators, system k of size N[k] with kernel parameters
+ * params[2k], params[2k+1] (p0, p1 of HM_KERNEL_GAUSSIAN / HM_KERNEL_COULOMB) on
+ * points[sum_{j<k} N[j] .. +N[k]) (N x dim, point-major, concatenated).  Each system
+ * gets the reference's tree and compression rules; every level of every system shares
+ * one launch per step in the build, the factorization and the solve. */
+HM_API int hm_batch_build_from_kernel(hm_handle* h, int kernel, const double* points, int dim, int nsys,
+                                      const int* N, const double* params, int leaf_size);
+HM_API int hm_num_systems(const hm_handle* h);
+/* Packed right-hand sides (host or device): system k's N[k] x nrhs[k] column-major
+ * block at offset sum_{j<k} N[j] nrhs[j]; nrhs[k] may be 0.  FP64; synchronises. */
+HM_API int hm_batch_solve(hm_handle* h, const double* b, const int* nrhs, double* x);
+HM_API int hm_batch_multiply(hm_handle* h, const double* x, const int* nrhs, double* y);
 
 /* ---- adjoint (no counterpart in the reference) ----
  * A^T lam = g with the FP64 factorization run transposed in reverse level order
