@@ -168,9 +168,14 @@ template <typename T>
 struct GemmStep : Plan::Step {
     GemmBatch<T> batch;
     GenParams gp;
+    std::string label;   // optional profile label (which step of which phase)
     explicit GemmStep(int cfg = CFG_64x64, int gen = GEN_DENSE) : batch(cfg, gen) {}
+    GemmStep(const char* lbl) : batch(CFG_64x64, GEN_DENSE) {
+        label = std::string(sizeof(T) == 8 ? "gemm_f64:" : "gemm_f32:") + lbl;
+    }
     void run(cudaStream_t s, int*) const override { batch.launch(s, gp); }
     const char* name() const override {
+        if (!label.empty()) return label.c_str();
         if (batch.gen() != GEN_DENSE) return "gemm_kernel_gen_f64";
         return sizeof(T) == 8 ? "gemm_f64" : "gemm_f32";
     }

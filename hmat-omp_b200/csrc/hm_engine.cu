@@ -1164,7 +1164,7 @@ void Engine::plan_factor(FactorStore<T>& fs) {
         Ut = reinterpret_cast<const T*>(dU.p);
     }
     {   // Q_c[rows of leaf] = Dinv U_c[rows of leaf] for every basis block on the path
-        auto g = std::make_unique<GemmStep<T>>();
+        auto g = std::make_unique<GemmStep<T>>("factor.leaf_apply");
         for (int l : leaves_) {
             const Node& n = nodes_[l];
             for (int c : path_of(l)) {
@@ -1182,16 +1182,16 @@ void Engine::plan_factor(FactorStore<T>& fs) {
         fs.plans.push_back(std::make_unique<Plan>());
         Plan& lp = *fs.plans.back();
         const auto& lvl = levels_[d];
-        auto gK = std::make_unique<GemmStep<T>>();
+        auto gK = std::make_unique<GemmStep<T>>("factor.K");
         auto cvK = std::make_unique<CopyStep>();
         auto ident = std::make_unique<IdentStep>();
-        auto gM = std::make_unique<GemmStep<double>>();
+        auto gM = std::make_unique<GemmStep<double>>("factor.M");
         std::vector<InvProblem> inv;
-        auto gP = std::make_unique<GemmStep<double>>();
+        auto gP = std::make_unique<GemmStep<double>>("factor.P");
         auto cvP = std::make_unique<CopyStep>();
-        auto gT = std::make_unique<GemmStep<T>>();
-        auto gD = std::make_unique<GemmStep<T>>();
-        auto gC = std::make_unique<GemmStep<T>>();
+        auto gT = std::make_unique<GemmStep<T>>("factor.update_project");
+        auto gD = std::make_unique<GemmStep<T>>("factor.update_small");
+        auto gC = std::make_unique<GemmStep<T>>("factor.update_correct");
         for (int id : lvl) {
             const Node& n = nodes_[id];
             const Node& L = nodes_[n.left];
@@ -1320,17 +1320,17 @@ static void add_matvec(Plan& pl, const std::vector<Node>& nodes, const std::vect
                        const std::vector<std::vector<int>>& levels, const double* dD, const double* dU,
                        const double* dV, const double* dB, const double* X, double* Y, int N,
                        const std::vector<int>& sc, cudaStream_t st) {
-    auto gLeaf = std::make_unique<GemmStep<double>>();
+    auto gLeaf = std::make_unique<GemmStep<double>>("matvec.leaf");
     for (int l : leaves) {
         const Node& n = nodes[l];
         const int s = sc[n.sys];
         gLeaf->batch.add(n.len(), s, n.len(), 1.0, dD + n.offD, n.len(), OP_N, X + n.start, N, OP_N,
                          0.0, Y + n.start, N);
     }
-    auto gT = std::make_unique<GemmStep<double>>();
-    auto gD = std::make_unique<GemmStep<double>>();
+    auto gT = std::make_unique<GemmStep<double>>("matvec.project");
+    auto gD = std::make_unique<GemmStep<double>>("matvec.couple");
     std::vector<std::unique_ptr<GemmStep<double>>> gE(levels.size());
-    for (size_t d = 0; d < levels.size(); ++d) gE[d] = std::make_unique<GemmStep<double>>();
+    for (size_t d = 0; d < levels.size(); ++d) gE[d] = std::make_unique<GemmStep<double>>("matvec.expand");
     for (size_t d = 0; d < levels.size(); ++d) {
         for (int id : levels[d]) {
             const Node& n = nodes[id];
@@ -1382,7 +1382,7 @@ static void add_solve(Plan& pl, const std::vector<Node>& nodes, const std::vecto
                       const T* Q, const T* P, const T* X, T* Z, int N, const std::vector<int>& sc,
                       cudaStream_t st) {
     constexpr bool F32 = std::is_same<T, float>::value;
-    auto gLeaf = std::make_unique<GemmStep<T>>();
+    auto gLeaf = std::make_unique<GemmStep<T>>("solve.leaf");
     for (int l : leaves) {
         const Node& n = nodes[l];
         const int s = sc[n.sys];
@@ -1392,9 +1392,9 @@ static void add_solve(Plan& pl, const std::vector<Node>& nodes, const std::vecto
     gLeaf->batch.finalize(st);
     pl.add(std::move(gLeaf));
     for (int d = (int)levels.size() - 1; d >= 0; --d) {
-        auto gT = std::make_unique<GemmStep<T>>();
-        auto gD = std::make_unique<GemmStep<T>>();
-        auto gC = std::make_unique<GemmStep<T>>();
+        auto gT = std::make_unique<GemmStep<T>>("solve.project");
+        auto gD = std::make_unique<GemmStep<T>>("solve.small");
+        auto gC = std::make_unique<GemmStep<T>>("solve.correct");
         for (int id : levels[d]) {
             const Node& n = nodes[id];
             const Node& L = nodes[n.left];

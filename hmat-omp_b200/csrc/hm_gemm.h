@@ -119,6 +119,7 @@ class GemmBatch {
     int total_tiles_ = 0;
     bool finalized_ = false;
     double flops_ = 0, bytes_ = 0;
+    int pipe_bn_ = 0, pipe_tiles_ = 0;   // pipelined dense kernel: tile width and tile count
 };
 
 }  // namespace hm
