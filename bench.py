@@ -241,11 +241,17 @@ def run_ours(args):
         return ms, out
 
     if args.profile_only:
-        step()
-        H.profile_enable(True)
-        step()
-        torch.cuda.synchronize()
-        print(json.dumps({"profile": H.profile_report()}))
+        out = {}
+        for name, prec in (("mixed", H.MIXED), ("fp64", H.FP64)):
+            h.set_precision(prec)
+            step()
+            H.profile_enable(True)
+            step()
+            torch.cuda.synchronize()
+            out[name] = H.profile_report()
+            H.profile_enable(False)
+        h.set_precision(H.MIXED)
+        print(json.dumps({"profile": out}))
         return
 
     # ---- mixed precision (headline) ----
