@@ -1106,6 +1106,8 @@ void Engine::plan_factor(FactorStore<T>& fs) {
     constexpr bool F32 = std::is_same<T, float>::value;
     cudaStream_t s = stream_;
     fs.plans.clear();
+    fs.setup.reset();
+    fs.setup_done = false;
     size_t offM = 0, offP = 0;
     for (auto& n : nodes_) {
         if (n.is_leaf) continue;
@@ -1149,10 +1151,15 @@ void Engine::plan_factor(FactorStore<T>& fs) {
         if (fs.Dinv.n < totD) fs.Dinv.alloc(totD);
         if (fs.V.n < totV) fs.V.alloc(totV);
         Utmp.alloc(totU);
+        // the bases depend on the built operator only: converted once per build
+        auto cb = std::make_unique<CopyStep>();
+        cb->t.h.push_back(flat_copy(dV.p, false, fs.V.p, true, totV));
+        cb->t.h.push_back(flat_copy(dU.p, false, Utmp.p, true, totU));
+        cb->t.upload(s);
+        fs.setup = std::make_unique<Plan>();
+        fs.setup->add(std::move(cb));
         auto cp = std::make_unique<CopyStep>();
         cp->t.h.push_back(flat_copy(dDinv.p, false, fs.Dinv.p, true, totD));
-        cp->t.h.push_back(flat_copy(dV.p, false, fs.V.p, true, totV));
-        cp->t.h.push_back(flat_copy(dU.p, false, Utmp.p, true, totU));
         cp->t.upload(s);
         plan.add(std::move(cp));
         Dinv = fs.Dinv.p;
@@ -1281,6 +1288,10 @@ template <typename T>
 void Engine::factor_t(FactorStore<T>& fs) {
     if (!fs.planned) plan_factor(fs);
     dstatus.zero(stream_);
+    if (fs.setup && !fs.setup_done) {
+        fs.setup->run(stream_, dstatus.p);
+        fs.setup_done = true;
+    }
     for (auto& p : fs.plans) p->run(stream_, dstatus.p);
     check_status("factor");
     fs.ready = true;

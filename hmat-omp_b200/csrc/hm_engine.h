@@ -58,6 +58,8 @@ struct FactorStore {
     bool planned = false;
     DBuf<T> Utmp;                              // U in precision T (FP32 only)
     std::vector<std::unique_ptr<Plan>> plans;  // leaf step, then one per level
+    std::unique_ptr<Plan> setup;               // once per build: bases converted to T
+    bool setup_done = false;
 };
 
 class Engine {

@@ -186,145 +186,7 @@ gemm_batched_kernel(const GemmDesc<T>* __restrict__ descs, int ndesc, GenParams 
     }
 }
 
-// ---------------------------------------------------------------------------------
-// Pipelined dense variant: ST-stage cp.async staging of the A and B tiles (element-
-// granular copies with zero fill, because leading dimensions and block offsets are
-// arbitrary), BM x BN tiles on a 16 x 16 thread grid (thread owns rows tx + 16 i and
-// columns ty + 16 j, conflict-free shared reads), padded k-major shared layout.
-// ---------------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem, bool valid) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    const int n = valid ? (int)sizeof(T) : 0;
-    if constexpr (sizeof(T) == 4)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-template <typename T, int BM, int BN, int BK, int ST>
-__global__ void __launch_bounds__(256) gemm_pipe_kernel(const GemmDesc<T>* __restrict__ descs, int ndesc) {
-    constexpr int TM = BM / 16, TN = BN / 16;
-    constexpr int PA = BM + 4, PB = BN + 4;
-    constexpr int LA = BM * BK / 256, LB = BN * BK / 256;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    T* As = reinterpret_cast<T*>(smraw);
-    T* Bs = As + ST * BK * PA;
-
-    const int tile = blockIdx.x;
-    int lo = 0, hi = ndesc - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (descs[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
-    }
-    const GemmDesc<T>& D = descs[lo];
-    const int m = D.m, n = D.n, k = D.k, lda = D.lda, ldb = D.ldb;
-    const bool ta = D.opA == OP_T, tb = D.opB == OP_T;
-    const T* __restrict__ A = D.A;
-    const T* __restrict__ B = D.B;
-    int t = tile - D.tile0;
-    const int tm = t % D.tiles_m;
-    t /= D.tiles_m;
-    const int tn = t % D.tiles_n;
-    const int kslice = t / D.tiles_n;
-    const int m0 = tm * BM, n0 = tn * BN;
-    int kper = (k + D.ksplit - 1) / D.ksplit;
-    kper = (kper + BK - 1) / BK * BK;
-    const int kb = kslice * kper;
-    const int ke = min(k, kb + kper);
-    const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
-
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    auto load_stage = [&](int stage, int k0) {
-        T* as = As + stage * BK * PA;
-        T* bs = Bs + stage * BK * PB;
-#pragma unroll
-        for (int q = 0; q < LA; ++q) {
-            const int e = tid + 256 * q;
-            int i, kk;
-            if (!ta) { i = e % BM; kk = e / BM; } else { kk = e % BK; i = e / BK; }
-            const int gi = m0 + i, gk = k0 + kk;
-            const bool v = gi < m && gk < ke;
-            const T* src = v ? (ta ? A + gk + (size_t)gi * lda : A + gi + (size_t)gk * lda) : A;
-            cp_async_elem(as + kk * PA + i, src, v);
-        }
-#pragma unroll
-        for (int q = 0; q < LB; ++q) {
-            const int e = tid + 256 * q;
-            int j, kk;
-            if (!tb) { kk = e % BK; j = e / BK; } else { j = e % BN; kk = e / BN; }
-            const int gj = n0 + j, gk = k0 + kk;
-            const bool v = gj < n && gk < ke;
-            const T* src = v ? (tb ? B + gj + (size_t)gk * ldb : B + gk + (size_t)gj * ldb) : B;
-            cp_async_elem(bs + kk * PB + j, src, v);
-        }
-    };
-
-    T acc[TM][TN];
-#pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-        for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
-
-#pragma unroll
-    for (int s = 0; s < ST - 1; ++s) {
-        if (s < nk) load_stage(s, kb + s * BK);
-        cp_async_commit();
-    }
-    for (int it = 0; it < nk; ++it) {
-        cp_async_wait<ST - 2>();
-        __syncthreads();
-        const int nxt = it + ST - 1;
-        if (nxt < nk) load_stage(nxt % ST, kb + nxt * BK);
-        cp_async_commit();
-        const T* as = As + (it % ST) * BK * PA;
-        const T* bs = Bs + (it % ST) * BK * PB;
-#pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            T a[TM], b[TN];
-#pragma unroll
-            for (int i = 0; i < TM; ++i) a[i] = as[kk * PA + tx + 16 * i];
-#pragma unroll
-            for (int j = 0; j < TN; ++j) b[j] = bs[kk * PB + ty + 16 * j];
-#pragma unroll
-            for (int i = 0; i < TM; ++i)
-#pragma unroll
-                for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-    }
-    cp_async_wait<0>();
-
-    T* __restrict__ C = D.C;
-    const int ldc = D.ldc;
-    const T alpha = D.alpha, beta = D.beta;
-    const bool split = D.ksplit > 1;
-#pragma unroll
-    for (int i = 0; i < TM; ++i) {
-        const int gi = m0 + tx + 16 * i;
-        if (gi >= m) continue;
-#pragma unroll
-        for (int j = 0; j < TN; ++j) {
-            const int gj = n0 + ty + 16 * j;
-            if (gj >= n) continue;
-            const T v = alpha * acc[i][j];
-            T* c = C + gi + (size_t)gj * ldc;
-            if (split) atomicAdd(c, v);
-            else *c = (beta == T(0)) ? v : fma(beta, *c, v);
-        }
-    }
-}
-
-template <typename T, int BM, int BN>
-static void launch_pipe(int tiles, cudaStream_t s, const GemmDesc<T>* d, int nd) {
-    constexpr int BK = 16, ST = 3;
-    constexpr size_t smem = (size_t)ST * BK * ((BM + 4) + (BN + 4)) * sizeof(T);
-    static size_t cur = 0;
-    ensure_dyn_smem(gemm_pipe_kernel<T, BM, BN, BK, ST>, smem, cur);
-    gemm_pipe_kernel<T, BM, BN, BK, ST><<<tiles, 256, smem, s>>>(d, nd);
-}
+#include "hm_gemm_tile.cuh"
 
 template <typename T>
 __global__ void zero_regions_kernel(const ZeroRegion<T>* __restrict__ z, int count) {
@@ -520,7 +382,7 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         bytes_ += sizeof(T) * (a + (double)d.k * d.n + (double)d.m * d.n * (d.beta != T(0) ? 2 : 1));
     }
     total_tiles_ = t;
-    // dense batches run the pipelined kernel: tile counts for its shape in a device-side
+    // dense batches run the warp-tiled kernel: tile counts for its shape in a device-side
     // copy of the table (BN fitted to the widest problem: ranks are usually <= 96)
     pipe_bn_ = 0;
     if (gen_ == GEN_DENSE && cfg_ == CFG_64x64 && !h_.empty()) {
@@ -533,7 +395,7 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         if (!any_scale) pipe_bn_ = nmax <= 32 ? 32 : nmax <= 64 ? 64 : nmax <= 96 ? 96 : 128;
     }
     if (pipe_bn_) {
-        const int BM = sizeof(T) == 4 ? 128 : 64;
+        const int BM = tile::bm_for(sizeof(T), pipe_bn_);
         std::vector<GemmDesc<T>> dv(h_);
         int tt = 0;
         for (auto& d : dv) {
@@ -543,9 +405,17 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
             tt += d.tiles_m * d.tiles_n * d.ksplit;
         }
         pipe_tiles_ = tt;
+        std::vector<int> tp((size_t)tt);
+        for (size_t i = 0; i < dv.size(); ++i) {
+            const auto& d = dv[i];
+            std::fill(tp.begin() + d.tile0, tp.begin() + d.tile0 + d.tiles_m * d.tiles_n * d.ksplit, (int)i);
+        }
         d_.alloc(dv.size());
+        tmap_.alloc(std::max<size_t>(tp.size(), 1));
         HM_CUDA(cudaMemcpyAsync(d_.p, dv.data(), dv.size() * sizeof(GemmDesc<T>), cudaMemcpyHostToDevice, s));
-        HM_CUDA(cudaStreamSynchronize(s));  // dv is a local vector
+        if (!tp.empty())
+            HM_CUDA(cudaMemcpyAsync(tmap_.p, tp.data(), tp.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        HM_CUDA(cudaStreamSynchronize(s));  // dv and tp are local vectors
     } else if (!h_.empty()) {
         d_.alloc(h_.size());
         HM_CUDA(cudaMemcpyAsync(d_.p, h_.data(), h_.size() * sizeof(GemmDesc<T>),
@@ -566,6 +436,7 @@ void GemmBatch<T>::clear() {
     hz_.clear();
     d_.release();
     dz_.release();
+    tmap_.release();
     total_tiles_ = 0;
     finalized_ = false;
 }
@@ -595,11 +466,10 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp) const {
     HM_CHECK(finalized_, HM_ERR_STATE, "GemmBatch::launch before finalize");
     if (!hz_.empty())
         zero_regions_kernel<T><<<(int)hz_.size(), 256, 0, s>>>(dz_.p, (int)hz_.size());
-    constexpr int PBM = sizeof(T) == 4 ? 128 : 64;
-    if (pipe_bn_ == 32) launch_pipe<T, PBM, 32>(pipe_tiles_, s, d_.p, (int)h_.size());
-    else if (pipe_bn_ == 64) launch_pipe<T, PBM, 64>(pipe_tiles_, s, d_.p, (int)h_.size());
-    else if (pipe_bn_ == 96) launch_pipe<T, PBM, 96>(pipe_tiles_, s, d_.p, (int)h_.size());
-    else if (pipe_bn_ == 128) launch_pipe<T, PBM, 128>(pipe_tiles_, s, d_.p, (int)h_.size());
+    if (pipe_bn_ == 32) tile::launch<T, 32>(pipe_tiles_, s, d_.p, tmap_.p);
+    else if (pipe_bn_ == 64) tile::launch<T, 64>(pipe_tiles_, s, d_.p, tmap_.p);
+    else if (pipe_bn_ == 96) tile::launch<T, 96>(pipe_tiles_, s, d_.p, tmap_.p);
+    else if (pipe_bn_ == 128) tile::launch<T, 128>(pipe_tiles_, s, d_.p, tmap_.p);
     else if (cfg_ == CFG_N_SKINNY)
         launch_gen<T, 128, 16, 16, 4, 2>(gen_, total_tiles_, s, d_.p, (int)h_.size(), gp);
     else

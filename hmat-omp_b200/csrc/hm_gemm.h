@@ -119,7 +119,8 @@ class GemmBatch {
     int total_tiles_ = 0;
     bool finalized_ = false;
     double flops_ = 0, bytes_ = 0;
-    int pipe_bn_ = 0, pipe_tiles_ = 0;   // pipelined dense kernel: tile width and tile count
+    int pipe_bn_ = 0, pipe_tiles_ = 0;   // warp-tiled dense kernel: tile width and tile count
+    DBuf<int> tmap_;                     // its tile -> problem table
 };
 
 }  // namespace hm
