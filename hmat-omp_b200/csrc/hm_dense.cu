@@ -90,21 +90,30 @@ void Plan::run(cudaStream_t s, int* status) const {
 //
 // Thread (lane, warp) holds rows lane + 32*rr and columns warp + W*cc of an NB x NB
 // tile (the matrix padded with identity).  Step j picks the pivot row p_j among rows not
-// yet used (largest |a[i][j]|, partial pivoting) and applies the in-place Gauss-Jordan
-// exchange on (p_j, j) without moving rows.  Afterwards row p_j holds x_j and column k
-// stands for equation p_k, so A^{-1}[j][p_k] = a[p_j][k]; the result is scattered with
-// that permutation.  The pivot column goes through shared memory (double-buffered, one
-// barrier per step); the pivot row comes from the owning lane by a warp shuffle.
+// yet used (partial pivoting) and applies the in-place Gauss-Jordan update
+//     a[p][c] <- a[p][c] / a[p][j]   (c != j),   a[p][j] <- 1 / a[p][j],
+//     a[i][c] <- a[i][c] - a[i][j] a[p][c]      (i != p, c != j),
+//     a[i][j] <- -a[i][j] / a[p][j]  (i != p),
+// without swapping rows: at the end X[q[r], p[c]] = B[r, c] (q = inverse of the pivot
+// sequence).  Each step is one fused multiply-add per element: column j is zeroed by its
+// owner first (so the same FMA yields -a[i][j]/a[p][j]) and the pivot row's multiplier
+// is zero (its scaled values are written afterwards by the owning lane).
+//
+// The owner of column j+1 searches its pivot right after its own update of step j, while
+// the other warps still update, and publishes it (one CTA barrier per step).  The search
+// key is the high word of |a[i][j]| with its low 8 bits replaced by 255 - i: one warp
+// max-reduction picks a pivot within a relative 2^-12 of the largest candidate (ties to
+// the lowest row), which keeps partial pivoting's stability bound.
 // ---------------------------------------------------------------------------------
 template <int NB, int W>
 __global__ void __launch_bounds__(32 * W, 1) gj_inverse_kernel(const GJDesc* __restrict__ descs, int* status) {
     constexpr int RT = NB / 32, CT = NB / W;
+    static_assert(NB % 32 == 0 && NB % W == 0 && NB <= 256, "Gauss-Jordan tile");
     __shared__ double colv[2][NB];
     __shared__ double s_inv[2];
     __shared__ int s_p[2];
     __shared__ int piv[NB];
     __shared__ int qinv[NB];
-    __shared__ int s_bad;
     const GJDesc d = descs[blockIdx.x];
     const int n = d.n;
     if (n <= 0) return;
@@ -117,70 +126,87 @@ __global__ void __launch_bounds__(32 * W, 1) gj_inverse_kernel(const GJDesc* __r
             const int i = lane + 32 * rr, c = warp + W * cc;
             a[rr][cc] = (i < n && c < n) ? d.A[i + (size_t)c * d.lda] : (i == c ? 1.0 : 0.0);
         }
-    if (threadIdx.x == 0) s_bad = 0;
-    unsigned used = 0;
-    __syncthreads();
-    int steps = 0;
-    for (int j = 0; j < n; ++j) {
-        const int buf = j & 1;
-        if (warp == j % W) {
-            const int ccj = j / W;
-            double best = -1.0;
-            int bi = 0x7fffffff;
+    unsigned used = 0;   // bit rr: row lane + 32 rr is already a pivot row
+
+    // pivot search of column j by its owning warp: colv[buf], s_p[buf], s_inv[buf]
+    // (s_p = -1 marks a zero or non-finite pivot)
+    auto search = [&](int j, int buf) {
+        const int ccj = j / W;
+        unsigned best = 0;
+#pragma unroll
+        for (int cc = 0; cc < CT; ++cc) {
+            if (cc != ccj) continue;
 #pragma unroll
             for (int rr = 0; rr < RT; ++rr) {
-                double v = 0.0;
-#pragma unroll
-                for (int cc = 0; cc < CT; ++cc) v = (cc == ccj) ? a[rr][cc] : v;
-                colv[buf][lane + 32 * rr] = v;
                 const int i = lane + 32 * rr;
-                const double av = fabs(v);
-                if (i < n && !((used >> rr) & 1u) && av > best) { best = av; bi = i; }
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double ob = __shfl_xor_sync(0xffffffffu, best, off);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-            }
-            __syncwarp();
-            if (lane == 0) {
-                const double pv = (bi < n) ? colv[buf][bi] : 0.0;
-                if (!(pv != 0.0) || !isfinite(pv)) s_bad = 1;
-                s_p[buf] = bi < n ? bi : 0;
-                s_inv[buf] = 1.0 / pv;
-                piv[j] = bi < n ? bi : 0;
+                const double v = a[rr][cc];
+                colv[buf][i] = v;
+                if (i < n && !((used >> rr) & 1u)) {
+                    const unsigned hi = (unsigned)((unsigned long long)__double_as_longlong(fabs(v)) >> 32);
+                    best = max(best, (hi & 0xFFFFFF00u) | (unsigned)(255 - i));
+                }
             }
         }
-        __syncthreads();
-        if (s_bad) break;
+        best = __reduce_max_sync(0xffffffffu, best);
+        __syncwarp();
+        if (lane == 0) {
+            const int p = 255 - (int)(best & 0xFFu);
+            const double pv = best ? colv[buf][p] : 0.0;
+            const bool ok = best != 0 && pv != 0.0 && isfinite(pv);
+            s_p[buf] = ok ? p : -1;
+            s_inv[buf] = ok ? 1.0 / pv : 0.0;
+        }
+    };
+
+    if (warp == 0) search(0, 0);
+    __syncthreads();
+    bool bad = false;
+    for (int j = 0; j < n; ++j) {
+        const int buf = j & 1;
         const int p = s_p[buf];
+        if (p < 0) { bad = true; break; }   // uniform: every thread read the same word
         const double inv = s_inv[buf];
+        if (threadIdx.x == 0) piv[j] = p;
         const int prr = p >> 5, plane = p & 31;
         if (lane == plane) used |= 1u << prr;
-        double rv[CT], cv[RT];
+        // scaled pivot row, broadcast from its owning lane
+        double r[CT];
 #pragma unroll
         for (int cc = 0; cc < CT; ++cc) {
             double v = 0.0;
 #pragma unroll
-            for (int rr = 0; rr < RT; ++rr) v = (rr == prr) ? a[rr][cc] : v;
-            rv[cc] = __shfl_sync(0xffffffffu, v, plane);
+            for (int rr = 0; rr < RT; ++rr)
+                if (rr == prr) v = a[rr][cc];
+            r[cc] = __shfl_sync(0xffffffffu, v, plane) * inv;
         }
-#pragma unroll
-        for (int rr = 0; rr < RT; ++rr) cv[rr] = colv[buf][lane + 32 * rr];
-#pragma unroll
-        for (int rr = 0; rr < RT; ++rr) {
-            const int i = lane + 32 * rr;
+        // column j: zeroed by its owner, its pivot-row entry becomes 1 / a[p][j]
+        if (warp == j % W) {
+            const int ccj = j / W;
 #pragma unroll
             for (int cc = 0; cc < CT; ++cc) {
-                const int c = warp + W * cc;
-                const double r = (c == j) ? inv : rv[cc] * inv;
-                a[rr][cc] = (i == p) ? r : fma(-cv[rr], r, (c == j) ? 0.0 : a[rr][cc]);
+                if (cc != ccj) continue;
+                r[cc] = inv;
+#pragma unroll
+                for (int rr = 0; rr < RT; ++rr) a[rr][cc] = 0.0;
             }
         }
-        ++steps;
+        double cv[RT];
+#pragma unroll
+        for (int rr = 0; rr < RT; ++rr) cv[rr] = (rr == prr && lane == plane) ? 0.0 : colv[buf][lane + 32 * rr];
+#pragma unroll
+        for (int rr = 0; rr < RT; ++rr)
+#pragma unroll
+            for (int cc = 0; cc < CT; ++cc) a[rr][cc] = fma(-cv[rr], r[cc], a[rr][cc]);
+#pragma unroll
+        for (int rr = 0; rr < RT; ++rr) {
+            if (rr != prr) continue;
+#pragma unroll
+            for (int cc = 0; cc < CT; ++cc) a[rr][cc] = (lane == plane) ? r[cc] : a[rr][cc];
+        }
+        if (j + 1 < n && warp == (j + 1) % W) search(j + 1, buf ^ 1);
+        __syncthreads();
     }
-    if (s_bad) {
+    if (bad) {
         if (threadIdx.x == 0) atomicOr(status, ST_SINGULAR);
         for (int e = threadIdx.x; e < n * n; e += 32 * W) d.X[(e % n) + (size_t)(e / n) * d.ldx] = nan("");
         return;
@@ -205,6 +231,7 @@ void launch_gj(const DevTable<GJDesc>& t, int nb, int* status, cudaStream_t s) {
     switch (nb) {
         case 32: gj_inverse_kernel<32, 4><<<t.size(), 128, 0, s>>>(t.d.p, status); break;
         case 64: gj_inverse_kernel<64, 8><<<t.size(), 256, 0, s>>>(t.d.p, status); break;
+        case 96: gj_inverse_kernel<96, 12><<<t.size(), 384, 0, s>>>(t.d.p, status); break;
         case 128: gj_inverse_kernel<128, 16><<<t.size(), 512, 0, s>>>(t.d.p, status); break;
         default: throw Error(HM_ERR_UNSUPPORTED, "Gauss-Jordan block size");
     }
@@ -532,7 +559,8 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
     }
     if (!small.empty()) {
         auto st = std::make_unique<GJStep>();
-        for (auto& p : small) st->t[p.n <= 32 ? 0 : p.n <= 64 ? 1 : 2].h.push_back({p.A, p.lda, p.X, p.ldx, p.n});
+        for (auto& p : small)
+            st->t[p.n <= 32 ? 0 : p.n <= 64 ? 1 : p.n <= 96 ? 2 : 3].h.push_back({p.A, p.lda, p.X, p.ldx, p.n});
         for (auto& tb : st->t) tb.upload(s);
         plan.add(std::move(st));
     }

@@ -185,14 +185,17 @@ struct GemmStep : Plan::Step {
 };
 
 struct GJStep : Plan::Step {
-    DevTable<GJDesc> t[3];   // n <= 32, <= 64, <= 128
+    DevTable<GJDesc> t[4];   // n <= 32, <= 64, <= 96, <= 128
     void run(cudaStream_t s, int* st) const override {
         launch_gj(t[0], 32, st, s);
         launch_gj(t[1], 64, st, s);
-        launch_gj(t[2], 128, st, s);
+        launch_gj(t[2], 96, st, s);
+        launch_gj(t[3], 128, st, s);
     }
     const char* name() const override { return "gauss_jordan_inverse"; }
-    int nlaunch() const override { return !t[0].h.empty() + !t[1].h.empty() + !t[2].h.empty(); }
+    int nlaunch() const override {
+        return !t[0].h.empty() + !t[1].h.empty() + !t[2].h.empty() + !t[3].h.empty();
+    }
     double flops() const override {
         double f = 0;
         for (auto& tb : t)

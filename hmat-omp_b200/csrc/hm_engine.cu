@@ -1193,6 +1193,9 @@ void Engine::plan_factor(FactorStore<T>& fs) {
         auto cvK = std::make_unique<CopyStep>();
         auto ident = std::make_unique<IdentStep>();
         auto gM = std::make_unique<GemmStep<double>>("factor.M");
+        auto gS = std::make_unique<GemmStep<double>>("factor.M");
+        auto gZ = std::make_unique<GemmStep<double>>("factor.M");
+        auto gTop = std::make_unique<GemmStep<double>>("factor.M");
         std::vector<InvProblem> inv;
         auto gP = std::make_unique<GemmStep<double>>("factor.P");
         auto cvP = std::make_unique<CopyStep>();
@@ -1221,15 +1224,30 @@ void Engine::plan_factor(FactorStore<T>& fs) {
                           OP_N, T(0), Kt, q1);
             gK->batch.add(q2, p2, R.len(), T(1), Vt + R.offV, R.len(), OP_T, fs.Q.p + R.offU, R.len(),
                           OP_N, T(0), Kt + (size_t)q1 * p1, q2);
-            // M = [[I, K1 B12], [K2 B21, I]]
+            // M = [[I, X], [Y, I]] with X = K1 B12, Y = K2 B21.  Its inverse through the
+            // Schur complement of the identity block, S = I - Y X:
+            //   Minv[q1:, :] = [-S^-1 Y, S^-1],   Minv[:q1, :] = [I, 0] - X Minv[q1:, :]
+            // (one inversion of order q2 instead of one of order q1 + q2).
             double* M = lp.scratch(std::max<size_t>((size_t)q * q, 1));
             double* Minv = dMinv.p + n.offM;
-            if (q) ident->t.h.push_back({M, q, q, q, 1.0});
             const double* B12 = dB.p + n.offB12;
             const double* B21 = dB.p + n.offB21;
-            gM->batch.add(q1, q2, p1, 1.0, K64, q1, OP_N, B12, p1, OP_N, 0.0, M + (size_t)q1 * q, q);
-            gM->batch.add(q2, q1, p2, 1.0, K64 + (size_t)q1 * p1, q2, OP_N, B21, p2, OP_N, 0.0, M + q1, q);
-            if (q) inv.push_back({M, q, Minv, q, q});
+            double* X = M + (size_t)q1 * q;
+            double* Y = M + q1;
+            gM->batch.add(q1, q2, p1, 1.0, K64, q1, OP_N, B12, p1, OP_N, 0.0, X, q);
+            gM->batch.add(q2, q1, p2, 1.0, K64 + (size_t)q1 * p1, q2, OP_N, B21, p2, OP_N, 0.0, Y, q);
+            double* Sinv = Minv + q1 + (size_t)q1 * q;
+            if (q2) {
+                double* S = lp.scratch((size_t)q2 * q2);
+                ident->t.h.push_back({S, q2, q2, q2, 1.0});
+                gS->batch.add(q2, q2, q1, -1.0, Y, q, OP_N, X, q, OP_N, 1.0, S, q2);
+                inv.push_back({S, q2, Sinv, q, q2});
+                gZ->batch.add(q2, q1, q2, -1.0, Sinv, q, OP_N, Y, q, OP_N, 0.0, Minv + q1, q);
+            }
+            if (q1) {
+                ident->t.h.push_back({Minv, q, q1, q, 1.0});
+                if (q2) gTop->batch.add(q1, q, q2, -1.0, X, q, OP_N, Minv + q1, q, OP_N, 1.0, Minv, q);
+            }
             // P = B^ Minv: P[0:p1,:] = B12 Minv[q1:,:], P[p1:,:] = B21 Minv[0:q1,:]
             double* P64;
             if constexpr (F32) {
@@ -1268,7 +1286,13 @@ void Engine::plan_factor(FactorStore<T>& fs) {
         lp.add(std::move(ident));
         gM->batch.finalize(s);
         lp.add(std::move(gM));
+        gS->batch.finalize(s);
+        lp.add(std::move(gS));
         plan_inverse(lp, inv, s);
+        gZ->batch.finalize(s);
+        lp.add(std::move(gZ));
+        gTop->batch.finalize(s);
+        lp.add(std::move(gTop));
         gP->batch.finalize(s);
         lp.add(std::move(gP));
         if (!cvP->t.h.empty()) { cvP->t.upload(s); lp.add(std::move(cvP)); }
