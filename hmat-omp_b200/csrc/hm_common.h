@@ -39,6 +39,7 @@ enum : int {
     ST_SINGULAR = 1,        // zero / non-finite pivot in an inversion
     ST_NO_CONVERGE = 2,     // Jacobi sweeps hit their limit
     ST_NONFINITE = 4,       // non-finite value met where a finite one is required
+    ST_TIMEOUT = 8,         // a kernel's bounded wait on its own pipeline gave up
 };
 
 // A typed device allocation with RAII.

@@ -2,6 +2,8 @@
 // them with the batched GEMM: inverses, Gram/Jacobi SVDs, copies.
 #pragma once
 
+#include <cstdlib>
+
 #include <algorithm>
 #include <memory>
 #include <string>
@@ -164,17 +166,39 @@ class Plan {
     size_t used_ = 0, cap_ = 0;
 };
 
+// Which labelled FP32 steps may run on the tensor cores.  By default the three bulk
+// updates of the factorization (leaf_apply, update_project, update_small).  The rest of
+// the mixed-precision path feeds the refinement more directly: on the tensor cores the
+// projection K = V^T Q (amplified by the capacitance matrices) or the solve sweeps
+// weaken the refinement contraction (measured at N = 2^18, 64 right-hand sides: residual
+// after two sweeps 5.4e-11 with the default set, 2.6e-10 with K added, 1.1e-10 with the
+// solve's leaf step added; 1.3e-11 with no tensor cores).  HM_FP32_TENSOR_CORES
+// overrides: "0" none, "1" every eligible step, otherwise a comma-separated label list.
+inline bool tensor_cores_allowed(const char* label) {
+    const char* e = std::getenv("HM_FP32_TENSOR_CORES");
+    const std::string l(label);
+    if (!e || !*e) return l == "factor.leaf_apply" || l == "factor.update_project" || l == "factor.update_small";
+    if (e[0] == '1' && e[1] == 0) return true;
+    if (e[0] == '0' && e[1] == 0) return false;
+    const std::string list = std::string(",") + e + ",";
+    return list.find("," + l + ",") != std::string::npos;
+}
+
 template <typename T>
 struct GemmStep : Plan::Step {
     GemmBatch<T> batch;
     GenParams gp;
-    std::string label;   // optional profile label (which step of which phase)
+    std::string label;      // optional profile label (which step of which phase)
+    std::string label_tc;   // the same when the batch runs on the tensor cores
     explicit GemmStep(int cfg = CFG_64x64, int gen = GEN_DENSE) : batch(cfg, gen) {}
     GemmStep(const char* lbl) : batch(CFG_64x64, GEN_DENSE) {
         label = std::string(sizeof(T) == 8 ? "gemm_f64:" : "gemm_f32:") + lbl;
+        label_tc = std::string("tc_tf32x4:") + lbl;
+        batch.allow_tensor_cores(tensor_cores_allowed(lbl));
     }
-    void run(cudaStream_t s, int*) const override { batch.launch(s, gp); }
+    void run(cudaStream_t s, int* st) const override { batch.launch(s, gp, st); }
     const char* name() const override {
+        if (batch.on_tensor_cores()) return label.empty() ? "tc_tf32x4" : label_tc.c_str();
         if (!label.empty()) return label.c_str();
         if (batch.gen() != GEN_DENSE) return "gemm_kernel_gen_f64";
         return sizeof(T) == 8 ? "gemm_f64" : "gemm_f32";

@@ -196,6 +196,7 @@ void Engine::check_status(const char* what) {
     HM_CUDA(cudaStreamSynchronize(stream_));
     if (st & ST_SINGULAR) throw Error(HM_ERR_SINGULAR, std::string(what) + ": singular pivot");
     if (st & ST_NONFINITE) throw Error(HM_ERR_NONFINITE, std::string(what) + ": non-finite values");
+    if (st & ST_TIMEOUT) throw Error(HM_ERR_CUDA, std::string(what) + ": tensor-core pipeline wait timed out");
     if (st & ST_NO_CONVERGE)
         throw Error(HM_ERR_NO_CONVERGE, std::string(what) + ": Jacobi sweep limit reached");
 }
@@ -1430,6 +1431,7 @@ static void add_solve(Plan& pl, const std::vector<Node>& nodes, const std::vecto
         auto gT = std::make_unique<GemmStep<T>>("solve.project");
         auto gD = std::make_unique<GemmStep<T>>("solve.small");
         auto gC = std::make_unique<GemmStep<T>>("solve.correct");
+
         for (int id : levels[d]) {
             const Node& n = nodes[id];
             const Node& L = nodes[n.left];
@@ -1573,8 +1575,11 @@ void Engine::solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, 
         st->ir_iters = it;
         st->rel_residual = worst;
     }
-    if (!(worst <= opts_.ir_tol))
-        throw Error(HM_ERR_IR, "iterative refinement stopped at relative residual " + std::to_string(worst));
+    if (!(worst <= opts_.ir_tol)) {
+        char msg[128];
+        snprintf(msg, sizeof msg, "iterative refinement stopped at relative residual %.3e after %d sweeps", worst, it);
+        throw Error(HM_ERR_IR, msg);
+    }
 }
 
 void Engine::solve_device(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st) {

@@ -6,10 +6,14 @@
 // prefetch of the next k-tile; each thread owns a TM x TN block of the tile strided by
 // the thread grid so that shared-memory reads and global stores are conflict-free and
 // coalesced along the column-major row index.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "hm_gemm.h"
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 namespace hm {
 
@@ -187,6 +191,7 @@ gemm_batched_kernel(const GemmDesc<T>* __restrict__ descs, int ndesc, GenParams 
 }
 
 #include "hm_gemm_tile.cuh"
+#include "hm_gemm_tc.cuh"
 
 template <typename T>
 __global__ void zero_regions_kernel(const ZeroRegion<T>* __restrict__ z, int count) {
@@ -421,6 +426,10 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         HM_CUDA(cudaMemcpyAsync(d_.p, h_.data(), h_.size() * sizeof(GemmDesc<T>),
                                 cudaMemcpyHostToDevice, s));
     }
+    use_tc_ = false;
+    if constexpr (std::is_same<T, float>::value) {
+        if (pipe_bn_ && tc_allowed_) finalize_tc(s);
+    }
     if (!hz_.empty()) {
         dz_.alloc(hz_.size());
         HM_CUDA(cudaMemcpyAsync(dz_.p, hz_.data(), hz_.size() * sizeof(ZeroRegion<T>),
@@ -430,6 +439,55 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
     finalized_ = true;
 }
 
+// FP32 batches whose tiles average at least 4 k-blocks of 32 (k >= 128) and whose
+// operands the TMA can address run on the tensor cores (3xTF32); short-k batches keep
+// the FMA kernel, which is as fast there.
+template <typename T>
+void GemmBatch<T>::finalize_tc(cudaStream_t s) {
+    if constexpr (std::is_same<T, float>::value) {
+        std::vector<GemmDesc<float>> dv(h_);
+        long long kblocks = 0;
+        int tt = 0;
+        for (auto& d : dv) {
+            if (!tc::tma_ok(d)) return;
+            d.tiles_m = ceil_div(d.m, tc::BM);
+            d.tiles_n = ceil_div(d.n, pipe_bn_);
+            d.tile0 = tt;
+            const int tiles = d.tiles_m * d.tiles_n * d.ksplit;
+            tt += tiles;
+            kblocks += (long long)d.tiles_m * d.tiles_n * ceil_div(std::max(d.k, 1), tc::BK);
+        }
+        if (tt == 0 || kblocks < 4LL * tt) return;
+        std::vector<CUtensorMap> maps;
+        if (!tc::encode_maps(dv, pipe_bn_, maps)) return;
+        std::vector<int> tp((size_t)tt);
+        for (size_t i = 0; i < dv.size(); ++i)
+            std::fill(tp.begin() + dv[i].tile0, tp.begin() + dv[i].tile0 + dv[i].tiles_m * dv[i].tiles_n * dv[i].ksplit,
+                      (int)i);
+        tcd_.alloc(dv.size());
+        tct_.alloc(tp.size());
+        tcmaps_.alloc(maps.size() * sizeof(CUtensorMap));
+        tcstatus_.alloc(1);
+        tcstatus_.zero(s);
+        HM_CUDA(cudaMemcpyAsync(tcd_.p, dv.data(), dv.size() * sizeof(GemmDesc<float>), cudaMemcpyHostToDevice, s));
+        HM_CUDA(cudaMemcpyAsync(tct_.p, tp.data(), tp.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        HM_CUDA(cudaMemcpyAsync(tcmaps_.p, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s));
+        HM_CUDA(cudaStreamSynchronize(s));   // the host vectors are locals
+        tc_tiles_ = tt;
+        use_tc_ = true;
+    }
+}
+
+static int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        HM_CUDA(cudaGetDevice(&dev));
+        HM_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return n;
+}
+
 template <typename T>
 void GemmBatch<T>::clear() {
     h_.clear();
@@ -437,6 +495,10 @@ void GemmBatch<T>::clear() {
     d_.release();
     dz_.release();
     tmap_.release();
+    tcd_.release();
+    tct_.release();
+    tcmaps_.release();
+    use_tc_ = false;
     total_tiles_ = 0;
     finalized_ = false;
 }
@@ -461,11 +523,24 @@ static void launch_gen(int gen, int grid, cudaStream_t s, const GemmDesc<T>* d, 
 }
 
 template <typename T>
-void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp) const {
+void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) const {
     if (h_.empty()) return;
     HM_CHECK(finalized_, HM_ERR_STATE, "GemmBatch::launch before finalize");
     if (!hz_.empty())
         zero_regions_kernel<T><<<(int)hz_.size(), 256, 0, s>>>(dz_.p, (int)hz_.size());
+    if constexpr (std::is_same<T, float>::value) {
+        if (use_tc_) {
+            const auto* maps = reinterpret_cast<const CUtensorMap*>(tcmaps_.p);
+            int* st = status ? status : tcstatus_.p;
+            const int sms = sm_count();
+            if (pipe_bn_ == 32) tc::launch<32>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
+            else if (pipe_bn_ == 64) tc::launch<64>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
+            else if (pipe_bn_ == 96) tc::launch<96>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
+            else tc::launch<128>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
+            HM_CUDA(cudaGetLastError());
+            return;
+        }
+    }
     if (pipe_bn_ == 32) tile::launch<T, 32>(pipe_tiles_, s, d_.p, tmap_.p);
     else if (pipe_bn_ == 64) tile::launch<T, 64>(pipe_tiles_, s, d_.p, tmap_.p);
     else if (pipe_bn_ == 96) tile::launch<T, 96>(pipe_tiles_, s, d_.p, tmap_.p);

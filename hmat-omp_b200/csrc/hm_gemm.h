@@ -87,7 +87,13 @@ class GemmBatch {
     size_t size() const { return h_.size(); }
     // Upload the table (once); later launches reuse it (and may be graph-captured).
     void finalize(cudaStream_t s);
-    void launch(cudaStream_t s, const GenParams& gp = GenParams()) const;
+    void finalize_tc(cudaStream_t s);
+    bool on_tensor_cores() const { return use_tc_; }
+    // whether finalize may put this (FP32) batch on the tensor cores
+    void allow_tensor_cores(bool on) { tc_allowed_ = on; }
+    // status: device status word for the tensor-core kernel's bounded waits (may be null
+    // for batches that never take that kernel)
+    void launch(cudaStream_t s, const GenParams& gp = GenParams(), int* status = nullptr) const;
     void clear();
     int cfg() const { return cfg_; }
     int gen() const { return gen_; }
@@ -121,6 +127,13 @@ class GemmBatch {
     double flops_ = 0, bytes_ = 0;
     int pipe_bn_ = 0, pipe_tiles_ = 0;   // warp-tiled dense kernel: tile width and tile count
     DBuf<int> tmap_;                     // its tile -> problem table
+    // FP32 batches with long k on the tensor cores: tile count, tables, tensor maps
+    bool use_tc_ = false, tc_allowed_ = true;
+    int tc_tiles_ = 0;
+    DBuf<GemmDesc<T>> tcd_;
+    DBuf<int> tct_;
+    DBuf<unsigned char> tcmaps_;
+    DBuf<int> tcstatus_;
 };
 
 }  // namespace hm
