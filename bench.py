@@ -34,9 +34,20 @@ UNIT = "RHS/s"
 
 
 def morton_points(N: int, seed: int) -> np.ndarray:
-    import hmat_oracle as O  # point ordering helper only (not the measured path)
+    import hmat_b200 as H
     p = np.random.default_rng(seed).random((N, 2))
-    return np.ascontiguousarray(p[O.morton_order(p)])
+    return np.ascontiguousarray(p[H.morton_order(p)])
+
+
+def rel_err(ref: np.ndarray, val: np.ndarray) -> float:
+    den = np.linalg.norm(ref)
+    return 0.0 if den == 0 else float(np.linalg.norm(ref - val) / den)
+
+
+def gaussian_dense(x: np.ndarray, h: float, shift: float) -> np.ndarray:
+    """Dense exp(-(x_i - x_j)^2 / 2h^2) + shift I on 1-D points (the batched workload's kernel)."""
+    d = x[:, None] - x[None, :]
+    return np.exp(-d * d / (2.0 * h * h)) + shift * np.eye(len(x))
 
 
 def parse():
@@ -147,20 +158,58 @@ def workload_config(args):
 # Clock sampling during the timed region
 # --------------------------------------------------------------------------------------
 class Clocks:
+    """SM clock and clock-event reasons of this process's GPU, sampled every 10 ms by NVML
+    (read-only queries) on a background thread while the timed region runs; nvidia-smi
+    polling when NVML is unavailable."""
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+
     def __init__(self, dev: int):
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        import threading
+        self.samples, self.max_mhz, self.p = [], None, None
+        self.stop_evt = threading.Event()
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={dev}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml as N
+            import torch
+            N.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(dev).uuid)
+            h = N.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop_evt.is_set():
+                    try:
+                        self.samples.append((N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM),
+                                             N.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                    except Exception:
+                        pass
+                    self.stop_evt.wait(0.01)
+
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            self.mode = "nvml"
         except Exception:
-            self.p = None
+            self.mode = "smi"
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            try:
+                self.p = subprocess.Popen(["nvidia-smi", f"--id={dev}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                           "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            except Exception:
+                self.p = None
 
     def stop(self):
+        if self.mode == "nvml":
+            self.stop_evt.set()
+            self.t.join()
+            sm = [c for c, _ in self.samples]
+            reasons = sorted({nm for _, r in self.samples for nm, bit in self.REASONS.items() if r & bit})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(sm), "source": "nvml 10 ms"}
         if self.p is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         self.p.terminate()
         self.p.wait()
         self.f.flush()
@@ -175,7 +224,7 @@ class Clocks:
                 if len(r) > 5 + i and "Active" in r[5 + i] and "Not" not in r[5 + i]:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+                "reasons": sorted(reasons), "samples": len(rows), "source": "nvidia-smi 100 ms"}
 
 
 # --------------------------------------------------------------------------------------
@@ -343,7 +392,6 @@ def run_batched(args):
     launch.  Prints one JSON line (not the headline metric)."""
     import torch
     import hmat_b200 as H
-    import hmat_oracle as O
 
     rng = np.random.default_rng(4)
     nsys = args.systems
@@ -383,9 +431,9 @@ def run_batched(args):
     launches = (H.launch_count() - n0) // args.steps
     xs = B._unpack(dx.cpu().numpy(), cols)
     ys = B.multiply(xs)
-    back = [O.rel_err(b, y) for b, y in zip(bs, ys)]
+    back = [rel_err(b, y) for b, y in zip(bs, ys)]
     small = np.argsort(Ns)[:6]
-    fwd = [O.rel_err(np.linalg.solve(O.gaussian_matrix(pts[k], hs[k], 1e-2), bs[k]), xs[k]) for k in small]
+    fwd = [rel_err(np.linalg.solve(gaussian_dense(pts[k], hs[k], 1e-2), bs[k]), xs[k]) for k in small]
     total_rhs = int(ss.sum())
     print(json.dumps({
         "metric": "batched HODLR factor+solve RHS/s (512 systems, N in [1024, 32768])", "value": total_rhs / (ms / 1e3),

@@ -139,6 +139,30 @@ def default_opts() -> Opts:
     return o
 
 
+def morton_order(points: np.ndarray, bits: int = 16) -> np.ndarray:
+    """Permutation that sorts 2-D points of [0,1)^2 along the Z-order (Morton) curve.
+
+    A kernel operator over points in this order has numerically low-rank off-diagonal
+    blocks at every level of the bisection tree (the ordering the 2-D Coulomb workload
+    uses); quantises each coordinate to `bits` bits and interleaves them (x in the even
+    bits)."""
+    p = np.asarray(points, dtype=np.float64)
+    q = np.clip((p * (1 << bits)).astype(np.uint64), 0, (1 << bits) - 1)
+
+    def spread(v):   # bit i of v -> bit 2i (magic-number interleave of a 16-bit value)
+        v = v & np.uint64(0xFFFF)
+        v = (v | (v << np.uint64(8))) & np.uint64(0x00FF00FF)
+        v = (v | (v << np.uint64(4))) & np.uint64(0x0F0F0F0F)
+        v = (v | (v << np.uint64(2))) & np.uint64(0x33333333)
+        v = (v | (v << np.uint64(1))) & np.uint64(0x55555555)
+        return v
+
+    if bits > 16:
+        raise ValueError("morton_order: at most 16 bits per coordinate")
+    key = spread(q[:, 0]) | (spread(q[:, 1]) << np.uint64(1))
+    return np.argsort(key, kind="stable")
+
+
 def _d(a: np.ndarray):
     return a.ctypes.data_as(_dp)
 
