@@ -50,6 +50,22 @@ def gaussian_dense(x: np.ndarray, h: float, shift: float) -> np.ndarray:
     return np.exp(-d * d / (2.0 * h * h)) + shift * np.eye(len(x))
 
 
+def shard_indices(n: int, rank: int, world: int) -> list:
+    """Systems this rank owns when independent systems are dealt round-robin to ranks."""
+    return list(range(rank, n, world))
+
+
+def reduce_over_ranks(value: float, op: str, world: int, device) -> float:
+    """max / sum of a per-rank scalar over all ranks (identity for one rank)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -389,16 +405,30 @@ def run_batched(args):
     [1024, 32768], Gaussian kernel with h log-uniform in [0.01, 0.2] and shift 1e-2 on
     sorted uniform points, leaf 64, ranks <= 48, 1-64 right-hand sides each (uniform
     integer), FP64.  A step = factor + solve of every system; all systems share every
-    launch.  Prints one JSON line (not the headline metric)."""
+    launch.  With N GPUs (torchrun) the systems are dealt round-robin to the ranks (no
+    collective in the data path: the total work is fixed, strong scaling); the step time
+    is the max over ranks.  Prints one JSON line (not the headline metric)."""
     import torch
+    import torch.distributed as dist
     import hmat_b200 as H
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     rng = np.random.default_rng(4)
-    nsys = args.systems
-    Ns = np.exp(rng.uniform(np.log(1024), np.log(32768), nsys)).astype(int)
-    hs = np.exp(rng.uniform(np.log(0.01), np.log(0.2), nsys))
-    ss = rng.integers(1, 65, nsys)
-    pts = [np.sort(rng.random(n)) for n in Ns]
+    nall = args.systems
+    Ns_all = np.exp(rng.uniform(np.log(1024), np.log(32768), nall)).astype(int)
+    hs_all = np.exp(rng.uniform(np.log(0.01), np.log(0.2), nall))
+    ss_all = rng.integers(1, 65, nall)
+    pts_all = [np.sort(rng.random(n)) for n in Ns_all]
+    mine = shard_indices(nall, rank, world)
+    Ns, hs, ss = Ns_all[mine], hs_all[mine], ss_all[mine]
+    pts = [pts_all[i] for i in mine]
+    nsys = len(mine)
     B = H.HODLRBatch(1e-10, rsvd_rank=48, max_rank=48, oversample=10, sketch=H.SKETCH_DEVICE_NORMAL, seed=0,
                      refine_steps=args.refine)
     stream = torch.cuda.current_stream()
@@ -406,7 +436,8 @@ def run_batched(args):
     t0 = time.perf_counter()
     B.build_from_kernel(H.KERNEL_GAUSSIAN, pts, [[h, 1e-2] for h in hs], 64)
     t_build = time.perf_counter() - t0
-    bs = [rng.standard_normal((n, s)) for n, s in zip(Ns, ss)]
+    bs_all = [np.random.default_rng(1000 + i).standard_normal((n, s)) for i, (n, s) in enumerate(zip(Ns_all, ss_all))]
+    bs = [bs_all[i] for i in mine]
     cols, packed = B._packed(bs)
     db = torch.from_numpy(packed).cuda()
     dx = torch.empty_like(db)
@@ -420,6 +451,8 @@ def run_batched(args):
     for _ in range(args.warmup):
         step()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
     torch.cuda.synchronize()
     n0 = H.launch_count()
     ev0.record(stream)
@@ -427,22 +460,30 @@ def run_batched(args):
         step()
     ev1.record(stream)
     torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        dist.barrier()
+    ms = reduce_over_ranks(ev0.elapsed_time(ev1) / args.steps, "max", world, dev)
     launches = (H.launch_count() - n0) // args.steps
     xs = B._unpack(dx.cpu().numpy(), cols)
     ys = B.multiply(xs)
     back = [rel_err(b, y) for b, y in zip(bs, ys)]
     small = np.argsort(Ns)[:6]
     fwd = [rel_err(np.linalg.solve(gaussian_dense(pts[k], hs[k], 1e-2), bs[k]), xs[k]) for k in small]
-    total_rhs = int(ss.sum())
+    total_rhs = int(ss_all.sum())
+    back_max = reduce_over_ranks(max(back) if back else 0.0, "max", world, dev)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
     print(json.dumps({
-        "metric": "batched HODLR factor+solve RHS/s (512 systems, N in [1024, 32768])", "value": total_rhs / (ms / 1e3),
-        "unit": "RHS/s", "systems_per_s": nsys / (ms / 1e3), "ms_per_step": ms, "steps": args.steps,
+        "metric": f"batched HODLR factor+solve RHS/s ({nall} systems, N in [1024, 32768])",
+        "value": total_rhs / (ms / 1e3), "unit": "RHS/s", "n_gpus": world, "scaling": "strong",
+        "systems_per_s": nall / (ms / 1e3), "ms_per_step": ms, "steps": args.steps,
         "warmup": args.warmup, "dtype": "f64", "data": "synthetic", "gpu_launches": int(launches),
-        "config": {"workload": "batched_gaussian_hodlr", "systems": nsys, "rows_total": int(Ns.sum()),
-                   "rhs_total": total_rhs, "leaf": 64, "max_rank": 48},
-        "build_s": t_build, "backward_error_max": max(back),
-        "forward_error_vs_dense_smallest6": fwd,
+        "config": {"workload": "batched_gaussian_hodlr", "systems": nall, "rows_total": int(Ns_all.sum()),
+                   "rhs_total": total_rhs, "leaf": 64, "max_rank": 48, "systems_on_rank0": nsys},
+        "build_s": t_build, "backward_error_max": back_max,
+        "forward_error_vs_dense_smallest6_rank0": fwd,
     }))
 
 
