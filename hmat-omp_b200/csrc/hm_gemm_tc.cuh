@@ -205,6 +205,12 @@ __device__ __forceinline__ bool wait_bar_warp(uint32_t b, uint32_t parity, volat
     return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
+// C goes through the TMA (load for beta != 0, store / reduce-add) only when aligned;
+// otherwise the epilogue reads and writes it row by row
+__host__ __device__ inline bool c_tma_ok(const float* C, int ldc) {
+    return (reinterpret_cast<uintptr_t>(C) & 15) == 0 && ldc % 4 == 0;
+}
+
 // Tile of this CTA -> problem, origin and k-range (same split rules as the FMA kernel).
 struct TileInfo {
     int p, m0, n0, kb, ke, nk;
@@ -448,13 +454,14 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
             // ends inside one is written back row by row instead (it must not touch the
             // rows that follow C in memory)
             const int m = D.m;
-            const bool via_tma = (m % 4 == 0) || (ti.m0 + BM <= m);
+            const bool c_tma = c_tma_ok(D.C, D.ldc);
+            const bool via_tma = c_tma && ((m % 4 == 0) || (ti.m0 + BM <= m));
             const int gi = ti.m0 + row;
             float* crow = D.C + gi + (size_t)ti.n0 * D.ldc;
             if (leader) {
                 // the previous tile's store has read the buffer: it may be reloaded / rewritten
                 bulk_wait_read();
-                if (rd) {
+                if (rd && c_tma) {
                     mbar_expect(cfull, (uint32_t)S::C_BYTES);
                     tma2d(smem_u32(cbuf), mc, ti.m0, ti.n0, cfull);
                     c_pending = true;
@@ -464,7 +471,7 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
             const int acc = accn & 1;
             if (!wait_bar_warp(tfull(acc), (accn >> 1) & 1, abort_flag, status)) break;
             if (!wait_bar_warp(cfree, accn & 1, abort_flag, status)) break;
-            if (rd) {
+            if (rd && c_tma) {
                 if (!wait_bar_warp(cfull, rdn & 1, abort_flag, status)) break;
                 if (leader) c_pending = false;
             }
@@ -484,9 +491,13 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
 #pragma unroll
                     for (int j = 0; j < 16; ++j) v[j] = w[j] = 0.f;
                 }
-                if (rd) {
+                if (rd && c_tma) {
 #pragma unroll
                     for (int j = 0; j < 16; ++j) cc[j] = lds_f32(cb0 + 4u * BM * (16 * c + j));
+                } else if (rd) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        cc[j] = (gi < m && 16 * c + j < nt) ? crow[(size_t)(16 * c + j) * D.ldc] : 0.f;
                 }
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
@@ -513,7 +524,7 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
                     bulk_commit();
                 }
             }
-            if (rd) ++rdn;
+            if (rd && c_tma) ++rdn;
             ++accn;
         }
         if (leader) {
@@ -544,8 +555,7 @@ void launch(int tiles, int sms, cudaStream_t s, const GemmDesc<float>* d, const 
 // and leading dimensions that are multiples of 4 floats.
 inline bool tma_ok(const GemmDesc<float>& d) {
     return (reinterpret_cast<uintptr_t>(d.A) & 15) == 0 && (reinterpret_cast<uintptr_t>(d.B) & 15) == 0 &&
-           (reinterpret_cast<uintptr_t>(d.C) & 15) == 0 && d.lda % 4 == 0 && d.ldb % 4 == 0 && d.ldc % 4 == 0 &&
-           d.kscale == nullptr;
+           d.lda % 4 == 0 && d.ldb % 4 == 0 && d.kscale == nullptr;
 }
 
 // Tensor maps of every problem's operands (3 per problem: A, B, C), in the box shapes
@@ -579,7 +589,7 @@ inline bool encode_maps(const std::vector<GemmDesc<float>>& probs, int bn, std::
                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
             if (r != CUDA_SUCCESS) return false;
         }
-        {   // C (m x n, column-major), box BM x bn, no swizzle: [column][row] in shared memory
+        if (c_tma_ok(d.C, d.ldc)) {   // C (m x n, column-major), box BM x bn, no swizzle
             cuuint64_t dims[2] = {(cuuint64_t)d.m, (cuuint64_t)d.n}, strides[1] = {(cuuint64_t)d.ldc * 4};
             cuuint32_t box[2] = {(cuuint32_t)BM, (cuuint32_t)bn}, es[2] = {1, 1};
             const CUresult r = enc(&out[3 * i + 2], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, d.C, dims, strides, box, es,
