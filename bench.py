@@ -314,6 +314,7 @@ def run_ours(args):
             step()
             torch.cuda.synchronize()
             out[name] = H.profile_report()
+            out[name + "_sequence"] = H.profile_sequence()
             H.profile_enable(False)
         h.set_precision(H.MIXED)
         print(json.dumps({"profile": out}))
@@ -487,6 +488,16 @@ def run_batched(args):
     }))
 
 
+# DRAM bytes / algorithmic bytes per step label, measured by ncu on the same step at
+# N = 65536 (profiles/traffic_factor_solve_coulomb_n65536.md); traffic grows with the
+# units processed, so the N = 2^18 traffic is the algorithmic bytes times this ratio.
+TRAFFIC_RATIO = {
+    "gemm_f32:factor.update_correct": 0.61, "gemm_f64:matvec.expand": 0.73, "gemm_f64:matvec.project": 0.79,
+    "tc_tf32x4:factor.update_project": 0.65, "gemm_f32:solve.correct": 0.72, "gemm_f32:solve.project": 0.98,
+    "tc_tf32x4:factor.leaf_apply": 0.45, "gemm_f32:factor.K": 0.98, "gauss_jordan_inverse": 0.51,
+}
+
+
 def roofline(prof: dict):
     peaks = {}
     try:
@@ -497,10 +508,13 @@ def roofline(prof: dict):
     hbm = peaks.get("hbm_gbs", 6650.0)
     name, (n, ms, fl, by) = max(prof.items(), key=lambda kv: kv[1][1])
     achieved = by / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+    ratio = TRAFFIC_RATIO.get(name)
     return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "traffic": None, "peak_source": src,
-            "achieved_tflops": fl / (ms / 1e3) / 1e12 if ms > 0 else 0.0,
-            "note": "SIMT FMA GEMM: the FMA pipe, not HBM, bounds it; see achieved_tflops"}
+            "frac": achieved / hbm, "traffic": by * ratio if ratio else None, "launches": n,
+            "traffic_source": "ncu dram bytes at N=65536 scaled by units (profiles/traffic_factor_solve_coulomb_n65536.md)",
+            "peak_source": src, "achieved_tflops": fl / (ms / 1e3) / 1e12 if ms > 0 else 0.0,
+            "note": "algorithmic bytes of the step's launches / their CUDA-event time; an FMA-pipe GEMM "
+                    "(24-48 flop/byte), so the FMA pipe, not HBM, bounds it: see achieved_tflops"}
 
 
 def main():

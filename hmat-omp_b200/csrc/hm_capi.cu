@@ -280,6 +280,15 @@ void hm_profile_enable(int on) {
 
 long long hm_launch_count(void) { return hm::Profiler::get().launches; }
 
+static size_t copy_out_text(const std::string& r, char* buf, size_t len) {
+    if (buf && len) {
+        size_t n = std::min(len - 1, r.size());
+        std::memcpy(buf, r.data(), n);
+        buf[n] = 0;
+    }
+    return r.size() + 1;
+}
+
 size_t hm_profile_report(char* buf, size_t len) {
     std::string r;
     try {
@@ -287,12 +296,17 @@ size_t hm_profile_report(char* buf, size_t len) {
     } catch (const std::exception& e) {
         r = std::string("{\"error\": \"") + e.what() + "\"}";
     }
-    if (buf && len) {
-        size_t n = std::min(len - 1, r.size());
-        std::memcpy(buf, r.data(), n);
-        buf[n] = 0;
+    return copy_out_text(r, buf, len);
+}
+
+size_t hm_profile_sequence(char* buf, size_t len) {
+    std::string r;
+    try {
+        r = hm::Profiler::get().sequence();
+    } catch (const std::exception& e) {
+        r = std::string("[[\"error: ") + e.what() + "\", 0, 0, 0, 0]]";
     }
-    return r.size() + 1;
+    return copy_out_text(r, buf, len);
 }
 
 }  // extern "C"

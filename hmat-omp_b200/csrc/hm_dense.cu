@@ -68,6 +68,21 @@ std::string Profiler::report() {
     return out + "}";
 }
 
+std::string Profiler::sequence() {
+    std::string out = "[";
+    char buf[320];
+    for (size_t i = 0; i < recs.size(); ++i) {
+        const Rec& r = recs[i];
+        HM_CUDA(cudaEventSynchronize(r.b));
+        float ms = 0;
+        HM_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        snprintf(buf, sizeof buf, "%s[\"%s\", %d, %.6f, %.6e, %.6e]", i ? ", " : "", r.name.c_str(), r.launches, ms,
+                 r.flops, r.bytes);
+        out += buf;
+    }
+    return out + "]";
+}
+
 void Plan::run(cudaStream_t s, int* status) const {
     Profiler& P = Profiler::get();
     for (auto& st : steps_) {

@@ -120,6 +120,8 @@ struct Profiler {
     void reset();
     // {"name": [launches, ms, flops, bytes], ...} (synchronises)
     std::string report();
+    // [["name", launches, ms, flops, bytes], ...] in record order (synchronises)
+    std::string sequence();
 };
 inline void count_launch(int n = 1) { Profiler::get().launches += n; }
 

@@ -101,8 +101,9 @@ def load() -> C.CDLL:
     L.hm_launch_count.restype = C.c_longlong
     L.hm_profile_enable.argtypes = [C.c_int]
     L.hm_profile_enable.restype = None
-    L.hm_profile_report.argtypes = [C.c_char_p, C.c_size_t]
-    L.hm_profile_report.restype = C.c_size_t
+    for f in ("hm_profile_report", "hm_profile_sequence"):
+        getattr(L, f).argtypes = [C.c_char_p, C.c_size_t]
+        getattr(L, f).restype = C.c_size_t
     _lib = L
     return L
 
@@ -124,6 +125,16 @@ def profile_report() -> dict:
     buf = C.create_string_buffer(int(n))
     L.hm_profile_report(buf, n)
     return {k: tuple(v) for k, v in json.loads(buf.value.decode()).items()}
+
+
+def profile_sequence() -> list:
+    """[(step, launches, ms, algorithmic flops, algorithmic bytes), ...] in launch order."""
+    import json
+    L = load()
+    n = L.hm_profile_sequence(None, 0)
+    buf = C.create_string_buffer(int(n))
+    L.hm_profile_sequence(buf, n)
+    return [tuple(r) for r in json.loads(buf.value.decode())]
 
 
 def header_functions() -> list[str]:

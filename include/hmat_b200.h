@@ -214,6 +214,10 @@ HM_API void hm_profile_enable(int on);
  * recorded since hm_profile_enable(1); synchronises.  Returns the length needed
  * (including the terminating NUL); writes at most len bytes. */
 HM_API size_t hm_profile_report(char* buf, size_t len);
+/* The same records in launch order, one per recorded step execution:
+ * JSON [["step", launches, ms, algorithmic flops, algorithmic bytes], ...] (lines up with
+ * a profiler's kernel list, step by step); same buffer convention. */
+HM_API size_t hm_profile_sequence(char* buf, size_t len);
 
 #ifdef __cplusplus
 }
