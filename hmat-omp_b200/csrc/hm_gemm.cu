@@ -400,7 +400,17 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         if (!any_scale) pipe_bn_ = nmax <= 32 ? 32 : nmax <= 64 ? 64 : nmax <= 96 ? 96 : 128;
     }
     if (pipe_bn_) {
-        const int BM = tile::bm_for(sizeof(T), pipe_bn_);
+        // 64-row tiles when the batch's problems are short enough that 128-row (or
+        // 256-row) tiles would pad more than a quarter of the rows
+        const int big = tile::bm_for(sizeof(T), pipe_bn_);
+        double rows = 0, pad_big = 0, pad_small = 0;
+        for (auto& d : h_) {
+            rows += d.m;
+            pad_big += (double)ceil_div(d.m, big) * big - d.m;
+            pad_small += (double)ceil_div(d.m, 64) * 64 - d.m;
+        }
+        pipe_small_ = big > 64 && pad_big > 0.25 * rows && pad_small < pad_big;
+        const int BM = tile::bm_for(sizeof(T), pipe_bn_, pipe_small_);
         std::vector<GemmDesc<T>> dv(h_);
         int tt = 0;
         for (auto& d : dv) {
@@ -541,7 +551,12 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) cons
             return;
         }
     }
-    if (pipe_bn_ == 32) tile::launch<T, 32>(pipe_tiles_, s, d_.p, tmap_.p);
+    if (pipe_small_) {
+        if (pipe_bn_ == 32) tile::launch<T, 32, true>(pipe_tiles_, s, d_.p, tmap_.p);
+        else if (pipe_bn_ == 64) tile::launch<T, 64, true>(pipe_tiles_, s, d_.p, tmap_.p);
+        else if (pipe_bn_ == 96) tile::launch<T, 96, true>(pipe_tiles_, s, d_.p, tmap_.p);
+        else tile::launch<T, 128, true>(pipe_tiles_, s, d_.p, tmap_.p);
+    } else if (pipe_bn_ == 32) tile::launch<T, 32>(pipe_tiles_, s, d_.p, tmap_.p);
     else if (pipe_bn_ == 64) tile::launch<T, 64>(pipe_tiles_, s, d_.p, tmap_.p);
     else if (pipe_bn_ == 96) tile::launch<T, 96>(pipe_tiles_, s, d_.p, tmap_.p);
     else if (pipe_bn_ == 128) tile::launch<T, 128>(pipe_tiles_, s, d_.p, tmap_.p);

@@ -38,7 +38,9 @@ struct Cfg {
 // Tile shape per element type and tile width (the widest problem of the batch picks
 // the width; ranks are usually <= 96).  Chosen by timing the factor's update shapes
 // (m = node rows, n = rank, k = rank; m = n = rank, k = node rows) on B200.
-template <typename T, int BN> struct For;
+// SMALL: 64-row tiles, for batches of short problems (the many-system workload's leaves
+// and nodes of <= 64 rows), where 128-row tiles would be half padding.
+template <typename T, int BN, bool SMALL = false> struct For;
 template <> struct For<float, 128> { using C = Cfg<float, 2, 4, 2, 2>; };
 template <> struct For<float, 96> { using C = Cfg<float, 4, 2, 1, 3>; };
 template <> struct For<float, 64> { using C = Cfg<float, 4, 2, 1, 2>; };
@@ -47,8 +49,17 @@ template <> struct For<double, 128> { using C = Cfg<double, 2, 4, 1, 2, 2>; };
 template <> struct For<double, 96> { using C = Cfg<double, 4, 3, 1, 2>; };
 template <> struct For<double, 64> { using C = Cfg<double, 4, 2, 1, 2, 2>; };
 template <> struct For<double, 32> { using C = Cfg<double, 4, 2, 1, 1>; };
+template <> struct For<float, 128, true> { using C = Cfg<float, 2, 4, 1, 2>; };
+template <> struct For<float, 96, true> { using C = Cfg<float, 2, 3, 1, 2, 2>; };
+template <> struct For<float, 64, true> { using C = Cfg<float, 2, 2, 1, 2, 4>; };
+template <> struct For<float, 32, true> { using C = Cfg<float, 2, 2, 1, 1, 4>; };
+template <> struct For<double, 128, true> { using C = Cfg<double, 2, 4, 1, 2, 2>; };
+template <> struct For<double, 96, true> { using C = Cfg<double, 2, 3, 1, 2, 1>; };
+template <> struct For<double, 64, true> { using C = Cfg<double, 2, 2, 1, 2, 3>; };
+template <> struct For<double, 32, true> { using C = Cfg<double, 2, 2, 1, 1, 4>; };
 
-inline int bm_for(size_t elem, int bn) {
+inline int bm_for(size_t elem, int bn, bool small = false) {
+    if (small) return 64;
     if (elem == 4) return bn == 32 ? 256 : 128;
     return bn == 128 ? 64 : 128;
 }
@@ -481,9 +492,9 @@ gemm_async_kernel(const GemmDesc<T>* __restrict__ descs, const int* __restrict__
     }
 }
 
-template <typename T, int BN>
+template <typename T, int BN, bool SMALL = false>
 void launch(int tiles, cudaStream_t s, const GemmDesc<T>* d, const int* tile_problem) {
-    using CF = typename For<T, BN>::C;
+    using CF = typename For<T, BN, SMALL>::C;
     static size_t cur = 0;
     ensure_dyn_smem(gemm_tile_kernel<T, CF>, CF::smem, cur);
     gemm_tile_kernel<T, CF><<<tiles, CF::NT, CF::smem, s>>>(d, tile_problem);
