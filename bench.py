@@ -78,7 +78,7 @@ def parse():
     ap.add_argument("--nrhs", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="one profiled step, no timing")
-    ap.add_argument("--workload", default="headline", choices=["headline", "batched"])
+    ap.add_argument("--workload", default="headline", choices=["headline", "batched", "hss", "adjoint"])
     ap.add_argument("--systems", type=int, default=512)
     ap.add_argument("--refine", type=int, default=1, help="FP64 refinement steps (batched workload)")
     return ap.parse_args()
@@ -517,12 +517,139 @@ def roofline(prof: dict):
                     "(24-48 flop/byte), so the FMA pipe, not HBM, bounds it: see achieved_tflops"}
 
 
+def run_hss(args):
+    """HSS, FP64, Gaussian A_ij = exp(-(x_i-x_j)^2/(2h^2)) + 1e-2 delta_ij, h = 0.05, x
+    sorted uniform on [0,1] (seed 2), N = 65536, leaf 128, tolerance 1e-10 with ranks
+    <= 64, built matrix-free; a step = factor + solve of 32 RHS ~ N(0,1), device-resident,
+    with one FP64 refinement step (x += A^{-1}(b - A x), same factors).  Prints one JSON
+    line (not the headline metric)."""
+    import torch
+    import hmat_b200 as H
+    N, s, leaf = 65536, 32, 128
+    x = np.sort(np.random.default_rng(2).random(N))
+    h = H.HSSMatrix(1e-10, rsvd_rank=64, max_rank=64, oversample=10, sketch=H.SKETCH_DEVICE_NORMAL, seed=0,
+                    refine_steps=1)
+    stream = torch.cuda.current_stream()
+    h.set_stream(stream.cuda_stream)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h.build_from_kernel(H.KERNEL_GAUSSIAN, x, [0.05, 1e-2], leaf)
+    t_build = time.perf_counter() - t0
+    b = torch.randn(s, N, generator=torch.Generator().manual_seed(5), dtype=torch.float64).cuda()
+    xs = torch.empty_like(b)
+
+    def step():
+        h.factor()
+        h.solve_device(b.data_ptr(), s, N, xs.data_ptr(), N)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    for _ in range(args.warmup):
+        step()
+    ms = timed(step)
+    ms_f = timed(h.factor)
+    y = torch.empty_like(b)
+    h.multiply_device(xs.data_ptr(), s, N, y.data_ptr(), N)
+    torch.cuda.synchronize()
+    resid = float(torch.linalg.norm(y - b) / torch.linalg.norm(b))
+    t = h.tree()
+    print(json.dumps({
+        "metric": "HSS factor+solve RHS/s (Gaussian 1-D, N=65536, 32 RHS, FP64)", "value": s / (ms / 1e3),
+        "unit": "RHS/s", "higher_is_better": True, "n_gpus": 1, "ms_per_step": ms, "ms_factor": ms_f,
+        "steps": args.steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic", "build_s": t_build,
+        "rel_residual": resid, "hss_ranks": {"max": int(t["rank12"].max()), "leaf_mean": float(
+            t["rank12"][t["is_leaf"] == 1].mean())},
+        "config": {"workload": "hss_gaussian_N65536_leaf128", "N": N, "leaf": leaf, "tol": 1e-10, "max_rank": 64,
+                   "nrhs": s, "h": 0.05, "shift": 1e-2, "points": "sorted U[0,1], seed 2", "build": "matrix-free",
+                   "refine_steps": 1},
+    }))
+
+
+def run_adjoint(args):
+    """HODLR, FP64, A(h) = Gaussian (h = 0.05) + 1e-2 I on sorted uniform points (seed 2),
+    N = 131072, leaf 128, ranks <= 64.  Loss L = ||A^{-1} b - t||^2 with b, t ~ N(0,1).
+    A step = factor + solve + adjoint solve + gradients (dL/dh through the kernel), host
+    vectors in and out.  dL/dh is compared with central finite differences of the whole
+    pipeline (rebuild, factor, solve at h +- eps; Richardson over eps and eps/2,
+    eps = 2e-3 h); all builds at tolerance 1e-15."""
+    import torch
+    import hmat_b200 as H
+    N, leaf, hh = 131072, 128, 0.05
+    x = np.sort(np.random.default_rng(2).random(N)).reshape(-1, 1)
+    rng = np.random.default_rng(6)
+    b, tgt = rng.standard_normal(N), rng.standard_normal(N)
+
+    def make(hv):
+        A = H.HODLRMatrix(1e-15, rsvd_rank=64, max_rank=64, oversample=10, power_iters=1,
+                          sketch=H.SKETCH_DEVICE_NORMAL, seed=1)
+        A.build_from_kernel(H.KERNEL_GAUSSIAN, x, [hv, 1e-2], leaf)
+        return A
+
+    def loss(A):
+        A.factor()
+        return float(np.sum((A.solve(b) - tgt) ** 2))
+
+    t0 = time.perf_counter()
+    A = make(hh)
+    t_build = time.perf_counter() - t0
+    rk = A.tree()["rank12"]
+    out = {}
+
+    def step():
+        A.factor()
+        xs = A.solve(b)
+        lam = A.solve_transpose(2.0 * (xs - tgt))
+        out.update(xs=xs, dp=A.gradients(xs, lam))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) / args.steps * 1e3
+    L0 = float(np.sum((out["xs"] - tgt) ** 2))
+    dLdh = float(out["dp"][0])
+    del A
+
+    def central(eps):
+        return (loss(make(hh + eps)) - loss(make(hh - eps))) / (2 * eps)
+
+    fd = {}
+    for rel in (2e-3, 1e-2):
+        e = rel * hh
+        fd[f"{rel:g}"] = (4.0 * central(e / 2) - central(e)) / 3.0
+    print(json.dumps({
+        "metric": "HODLR adjoint step (factor+solve+adjoint solve+gradients), Gaussian N=131072, FP64",
+        "value": 1e3 / ms, "unit": "steps/s", "higher_is_better": True, "n_gpus": 1, "ms_per_step": ms,
+        "steps": args.steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic", "build_s": t_build,
+        "timing": "host wall clock, host vectors in and out", "loss": L0, "dL_dh_adjoint": dLdh,
+        "dL_dh_central_fd": fd, "rel_diff_vs_fd": {k: abs(v - dLdh) / abs(v) for k, v in fd.items()},
+        "ranks": {"max": int(rk.max()), "mean": float(rk[rk > 0].mean()), "at_cap": int((rk == 64).sum())},
+        "config": {"workload": "adjoint_gaussian_N131072_leaf128", "N": N, "leaf": leaf, "tol": 1e-15,
+                   "max_rank": 64, "h": hh, "shift": 1e-2, "fd": "Richardson central, eps/h in {2e-3, 1e-2}"},
+    }))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "hss":
+        run_hss(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_ours(args)
 

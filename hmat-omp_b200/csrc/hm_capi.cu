@@ -144,20 +144,28 @@ int hm_hodlr_build_from_dense(hm_handle* h, const double* A, int N, int lda, int
     });
 }
 
+static void build_from_kernel(hm_handle* h, hm::Engine::Kind kind, int kernel, const double* points, int dim,
+                              int N, const double* params, int nparams, int leaf) {
+    HM_CHECK(points && N > 0 && dim >= 1, HM_ERR_ARG, "build_from_kernel: bad arguments");
+    HM_CHECK(nparams >= 2 && params, HM_ERR_ARG, "build_from_kernel: two parameters expected");
+    int gen = kernel == HM_KERNEL_CAUCHY ? hm::GEN_CAUCHY
+              : kernel == HM_KERNEL_GAUSSIAN ? hm::GEN_GAUSSIAN
+              : kernel == HM_KERNEL_COULOMB ? hm::GEN_COULOMB : -1;
+    HM_CHECK(gen > 0, HM_ERR_ARG, "build_from_kernel: unknown kernel");
+    HM_CHECK(kernel != HM_KERNEL_CAUCHY || dim == 1, HM_ERR_ARG, "Cauchy points are 1-D");
+    size_t npts = kernel == HM_KERNEL_CAUCHY ? 2 * (size_t)N : (size_t)N * dim;
+    engine(h, kind).build_kernel(gen, points, npts, dim, N, params[0], params[1], leaf);
+    HM_CUDA(cudaStreamSynchronize(h->stream));
+}
+
 int hm_hodlr_build_from_kernel(hm_handle* h, int kernel, const double* points, int dim, int N,
                                const double* params, int nparams, int leaf) {
-    return guard(h, [&] {
-        HM_CHECK(points && N > 0 && dim >= 1, HM_ERR_ARG, "build_from_kernel: bad arguments");
-        HM_CHECK(nparams >= 2 && params, HM_ERR_ARG, "build_from_kernel: two parameters expected");
-        int gen = kernel == HM_KERNEL_CAUCHY ? hm::GEN_CAUCHY
-                  : kernel == HM_KERNEL_GAUSSIAN ? hm::GEN_GAUSSIAN
-                  : kernel == HM_KERNEL_COULOMB ? hm::GEN_COULOMB : -1;
-        HM_CHECK(gen > 0, HM_ERR_ARG, "build_from_kernel: unknown kernel");
-        HM_CHECK(kernel != HM_KERNEL_CAUCHY || dim == 1, HM_ERR_ARG, "Cauchy points are 1-D");
-        size_t npts = kernel == HM_KERNEL_CAUCHY ? 2 * (size_t)N : (size_t)N * dim;
-        engine(h, hm::Engine::HODLR).build_kernel(gen, points, npts, dim, N, params[0], params[1], leaf);
-        HM_CUDA(cudaStreamSynchronize(h->stream));
-    });
+    return guard(h, [&] { build_from_kernel(h, hm::Engine::HODLR, kernel, points, dim, N, params, nparams, leaf); });
+}
+
+int hm_hss_build_from_kernel(hm_handle* h, int kernel, const double* points, int dim, int N,
+                             const double* params, int nparams, int leaf) {
+    return guard(h, [&] { build_from_kernel(h, hm::Engine::HSS, kernel, points, dim, N, params, nparams, leaf); });
 }
 
 int hm_hss_build_from_dense(hm_handle* h, const double* A, int N, int lda, int leaf) {

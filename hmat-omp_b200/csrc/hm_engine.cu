@@ -764,7 +764,8 @@ void Engine::build_hodlr(const Source& src) {
 // are identities (hss_routines.h:86-90), so a node's basis is the block diagonal of its
 // leaves' bases and B12 = UL^T A12 VR is the set of leaf-pair blocks U_l^T A_lm V_m.
 // Those come from the panels Pt_l = A[l, :]^T U_l (N x rank_U(l)): block (l, m) of B is
-// Pt_l[m rows]^T V_m.  The engine then factors/solves/multiplies this two-block form.
+// Pt_l[m rows]^T V_m.  reduce_hss_coupling then derives the operator that the factor,
+// solve and multiply run on.
 void Engine::build_hss(const Source& src) {
     const int N = N_;
     const int kguess = opts_.rsvd_rank + opts_.oversample;
@@ -927,12 +928,6 @@ void Engine::build_hss(const Source& src) {
         n.rankU = nodes_[n.left].rankU + nodes_[n.right].rankU;
         n.rankV = nodes_[n.left].rankV + nodes_[n.right].rankV;
     }
-    for (auto& n : nodes_) {
-        n.capU = n.rankU;
-        n.capV = n.rankV;
-    }
-    alloc_UV();
-    // dense bases: block diagonal of the leaf bases (reconstruct_U/V, hss_routines.h:23-45)
     std::vector<std::vector<int>> under(nodes_.size());  // leaves under each node, left to right
     for (int i = (int)nodes_.size() - 1; i >= 0; --i) {
         if (nodes_[i].is_leaf) under[i] = {i};
@@ -940,35 +935,6 @@ void Engine::build_hss(const Source& src) {
             under[i] = under[nodes_[i].left];
             under[i].insert(under[i].end(), under[nodes_[i].right].begin(), under[nodes_[i].right].end());
         }
-    }
-    {
-        Plan bp;
-        auto cp = std::make_unique<CopyStep>();
-        for (size_t c = 0; c < nodes_.size(); ++c) {
-            const Node& C = nodes_[c];
-            if (C.parent < 0) continue;
-            int cu = 0, cv = 0;
-            for (int l : under[c]) {
-                const Node& L = nodes_[l];
-                const size_t ro = (size_t)(L.start - C.start);
-                if (L.rankU)
-                    cp->t.h.push_back({dLeafB.p + leafU_[l].first, L.len(), dU.p + C.offU + ro + (size_t)cu * C.len(),
-                                       C.len(), L.len(), L.rankU, 0, 0, 0});
-                if (L.rankV)
-                    cp->t.h.push_back({dLeafB.p + leafV_[l].first, L.len(), dV.p + C.offV + ro + (size_t)cv * C.len(),
-                                       C.len(), L.len(), L.rankV, 0, 0, 0});
-                cu += L.rankU;
-                cv += L.rankV;
-                if (cp->t.h.size() >= 60000) {
-                    cp->t.upload(stream_);
-                    bp.add(std::move(cp));
-                    cp = std::make_unique<CopyStep>();
-                }
-            }
-        }
-        if (!cp->t.h.empty()) { cp->t.upload(stream_); bp.add(std::move(cp)); }
-        bp.run(stream_, dstatus.p);
-        HM_CUDA(cudaStreamSynchronize(stream_));
     }
     // coupling blocks
     size_t totB = 0;
@@ -1039,6 +1005,192 @@ void Engine::build_hss(const Source& src) {
         HM_CUDA(cudaStreamSynchronize(stream_));
     }
     check_status("hss build");
+    reduce_hss_coupling(under);
+}
+
+// The reference's transfers are identities (hss_routines.h:86-90): a node's basis is the
+// block diagonal of its leaves' bases, so its coupling blocks B12 (p1 x q2) and B21 are
+// as wide as the sums of its leaves' ranks (2.5K at the top for N = 65536, leaf 128)
+// while their numerical rank is that of the kernel block between the two children
+// (tens).  A Woodbury factorization over that wide form carries capacitance systems of
+// the same width, and its error grows with them (relative residual 2.6e-3 at
+// N = 65536 against 1e-8 for the HODLR of the same kernel).  So each coupling block is
+// recompressed once, B = F H^T with F orthonormal (p x r) and the singular values
+// above 1e-15 s_0 kept in H (q x r), and the operator that factor, solve and multiply
+// use is the two-block form U' = U F, V' = V H, B' = I -- equal to the HSS operator to
+// rounding.  F and H come from a randomized range finder with an adaptive width:
+// Y = B Omega (q x k Gaussian), Q = orth(Y), Z = B^T Q = W S R^T (Gram/Jacobi SVD),
+// F = Q R, H = Z R; a block whose rank comes within 8 of k (k < min(p, q)) is redone
+// with 2k.  The reference's leaf bases and B stay in hss_ and dLeafB for export.
+void Engine::reduce_hss_coupling(const std::vector<std::vector<int>>& under) {
+    const int nn = (int)nodes_.size();
+    hss_.rankU.assign(nn, 0);
+    hss_.rankV.assign(nn, 0);
+    hss_.offB12.assign(nn, 0);
+    hss_.offB21.assign(nn, 0);
+    for (int i = 0; i < nn; ++i) {
+        hss_.rankU[i] = nodes_[i].rankU;
+        hss_.rankV[i] = nodes_[i].rankV;
+        hss_.offB12[i] = nodes_[i].offB12;
+        hss_.offB21[i] = nodes_[i].offB21;
+    }
+    hss_.B = std::move(dB);
+    struct Cpl {
+        int node, side, rowc, colc, p, q;
+        int k = 0, r = 0;
+        const double* B = nullptr;
+        const double *F = nullptr, *H = nullptr;  // p x k, q x k (ld p, q)
+    };
+    std::vector<Cpl> cp;
+    for (const auto& lvl : levels_)
+        for (int id : lvl) {
+            const Node& n = nodes_[id];
+            for (int side = 0; side < 2; ++side) {
+                Cpl c;
+                c.node = id;
+                c.side = side;
+                c.rowc = side == 0 ? n.left : n.right;
+                c.colc = side == 0 ? n.right : n.left;
+                c.p = hss_.rankU[c.rowc];
+                c.q = hss_.rankV[c.colc];
+                c.B = hss_.B.p + (side == 0 ? hss_.offB12[id] : hss_.offB21[id]);
+                if (c.p > 0 && c.q > 0) cp.push_back(c);
+            }
+        }
+    std::vector<std::unique_ptr<Plan>> keep;   // owns the F/H scratch of every attempt
+    std::vector<int> want(cp.size(), 96);
+    std::vector<size_t> pending(cp.size());
+    for (size_t i = 0; i < cp.size(); ++i) pending[i] = i;
+    while (!pending.empty()) {
+        keep.push_back(std::make_unique<Plan>());
+        Plan& plan = *keep.back();
+        size_t omega_total = 0;
+        std::vector<size_t> om(pending.size());
+        for (size_t j = 0; j < pending.size(); ++j) {
+            Cpl& c = cp[pending[j]];
+            c.k = std::min(std::min(c.p, c.q), want[pending[j]]);
+            om[j] = omega_total;
+            omega_total += (size_t)c.q * c.k;
+        }
+        double* Om = plan.scratch(omega_total);
+        normal_fill_kernel<<<grid_for(omega_total), 256, 0, stream_>>>(Om, omega_total, opts_.seed,
+                                                                        0x4853530000000000ull + omega_total);
+        HM_CUDA(cudaGetLastError());
+        count_launch();
+        DBuf<int> dRank(pending.size());
+        auto gY = std::make_unique<GemmStep<double>>();
+        auto gZ = std::make_unique<GemmStep<double>>();
+        auto gF = std::make_unique<GemmStep<double>>();
+        std::vector<SvdProblem> s1, s2;
+        struct W { double *Y, *Q, *Z, *R, *F, *H; };
+        std::vector<W> w(pending.size());
+        for (size_t j = 0; j < pending.size(); ++j) {
+            Cpl& c = cp[pending[j]];
+            W& x = w[j];
+            x.Y = plan.scratch((size_t)c.p * c.k);
+            x.Q = plan.scratch((size_t)c.p * c.k);
+            x.Z = plan.scratch((size_t)c.q * c.k);
+            x.R = plan.scratch((size_t)c.k * c.k);
+            x.F = plan.scratch((size_t)c.p * c.k);
+            x.H = plan.scratch((size_t)c.q * c.k);
+            gY->batch.add(c.p, c.k, c.q, 1.0, c.B, c.p, OP_N, Om + om[j], c.q, OP_N, 0.0, x.Y, c.p);
+            SvdProblem a{};
+            a.X = x.Y; a.ldx = c.p; a.rows = c.p; a.k = c.k;
+            a.L = x.Q; a.ldl = c.p;
+            s1.push_back(a);
+            gZ->batch.add(c.q, c.k, c.p, 1.0, c.B, c.p, OP_T, x.Q, c.p, OP_N, 0.0, x.Z, c.q);
+            SvdProblem b{};
+            b.X = x.Z; b.ldx = c.q; b.rows = c.q; b.k = c.k;
+            b.R = x.R; b.ldr = c.k;
+            b.rank = dRank.p + j;
+            b.sort = true;
+            s2.push_back(b);
+            gF->batch.add(c.p, c.k, c.k, 1.0, x.Q, c.p, OP_N, x.R, c.k, OP_N, 0.0, x.F, c.p);
+            gF->batch.add(c.q, c.k, c.k, 1.0, x.Z, c.q, OP_N, x.R, c.k, OP_N, 0.0, x.H, c.q);
+        }
+        gY->batch.finalize(stream_);
+        plan.add(std::move(gY));
+        plan_gram_svd(plan, s1, 0.0, 0, stream_);
+        gZ->batch.finalize(stream_);
+        plan.add(std::move(gZ));
+        plan_gram_svd(plan, s2, 1e-15, 0, stream_);
+        gF->batch.finalize(stream_);
+        plan.add(std::move(gF));
+        plan.run(stream_, dstatus.p);
+        std::vector<int> rk(pending.size());
+        HM_CUDA(cudaMemcpyAsync(rk.data(), dRank.p, rk.size() * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        HM_CUDA(cudaStreamSynchronize(stream_));
+        check_status("hss coupling recompression");
+        std::vector<size_t> next;
+        for (size_t j = 0; j < pending.size(); ++j) {
+            Cpl& c = cp[pending[j]];
+            if (rk[j] > c.k - 8 && c.k < std::min(c.p, c.q)) {
+                want[pending[j]] = 2 * c.k;
+                next.push_back(pending[j]);
+            } else {
+                c.r = std::min(rk[j], c.k);
+                c.F = w[j].F;
+                c.H = w[j].H;
+            }
+        }
+        pending.swap(next);
+    }
+    // the two-block operator: ranks, bases U F / V H leaf by leaf, B' = I
+    for (auto& n : nodes_) n.rankU = n.rankV = 0;
+    for (const Cpl& c : cp) {
+        nodes_[c.rowc].rankU = c.r;
+        nodes_[c.colc].rankV = c.r;
+    }
+    for (auto& n : nodes_) {
+        n.capU = n.rankU;
+        n.capV = n.rankV;
+    }
+    alloc_UV();
+    size_t totB = 0;
+    for (auto& n : nodes_) {
+        if (n.is_leaf) continue;
+        n.offB12 = totB;
+        totB += (size_t)nodes_[n.left].rankU * nodes_[n.right].rankV;
+        n.offB21 = totB;
+        totB += (size_t)nodes_[n.right].rankU * nodes_[n.left].rankV;
+    }
+    dB.alloc(std::max<size_t>(totB, 1));
+    dB.zero(stream_);
+    Plan bp;
+    auto gb = std::make_unique<GemmStep<double>>();
+    auto id = std::make_unique<IdentStep>();
+    for (const Cpl& c : cp) {
+        if (c.r == 0) continue;
+        const Node& Rw = nodes_[c.rowc];
+        const Node& Cl = nodes_[c.colc];
+        int ro = 0;
+        for (int l : under[c.rowc]) {
+            const Node& L = nodes_[l];
+            const int rl = leafU_[l].second;
+            if (rl)
+                gb->batch.add(L.len(), c.r, rl, 1.0, dLeafB.p + leafU_[l].first, L.len(), OP_N, c.F + ro, c.p, OP_N,
+                              0.0, dU.p + Rw.offU + (L.start - Rw.start), Rw.len());
+            ro += rl;
+        }
+        int co = 0;
+        for (int m : under[c.colc]) {
+            const Node& M = nodes_[m];
+            const int rm = leafV_[m].second;
+            if (rm)
+                gb->batch.add(M.len(), c.r, rm, 1.0, dLeafB.p + leafV_[m].first, M.len(), OP_N, c.H + co, c.q, OP_N,
+                              0.0, dV.p + Cl.offV + (M.start - Cl.start), Cl.len());
+            co += rm;
+        }
+        const Node& n = nodes_[c.node];
+        id->t.h.push_back({dB.p + (c.side == 0 ? n.offB12 : n.offB21), c.r, c.r, c.r, 1.0});
+    }
+    gb->batch.finalize(stream_);
+    bp.add(std::move(gb));
+    id->t.upload(stream_);
+    bp.add(std::move(id));
+    bp.run(stream_, dstatus.p);
+    HM_CUDA(cudaStreamSynchronize(stream_));
+    check_status("hss two-block form");
 }
 
 // ---------------------------------------------------------------------------------
@@ -1770,8 +1922,8 @@ void Engine::export_tree(int* start, int* end, int* is_leaf, int* depth, int* r1
         if (depth) depth[i] = n.depth;
         int a = 0, b = 0;
         if (kind_ == HSS) {  // rank_U, rank_V (utils.h:41-42)
-            a = n.rankU;
-            b = n.rankV;
+            a = hss_.rankU[i];
+            b = hss_.rankV[i];
         } else if (!n.is_leaf) {  // B_12, B_21 sizes (hodlr_routines.h:140-141)
             a = nodes_[n.left].rankU;
             b = nodes_[n.right].rankU;
@@ -1791,11 +1943,11 @@ void Engine::get_factor(int node, int which, double* out, int* rows, int* cols) 
         std::vector<double> host;
         switch (which) {
             case 0: if (n.is_leaf) { src = dD.p + n.offD; r = c = ld = n.len(); } break;
-            case 1: if (n.is_leaf) { src = dLeafB.p + leafU_[node].first; r = ld = n.len(); c = n.rankU; } break;
-            case 2: if (n.is_leaf) { src = dLeafB.p + leafV_[node].first; r = ld = n.len(); c = n.rankV; } break;
+            case 1: if (n.is_leaf) { src = dLeafB.p + leafU_[node].first; r = ld = n.len(); c = leafU_[node].second; } break;
+            case 2: if (n.is_leaf) { src = dLeafB.p + leafV_[node].first; r = ld = n.len(); c = leafV_[node].second; } break;
             case 3:  // R = I (hss_routines.h:86-87)
             case 4: {  // W = I (hss_routines.h:89-90)
-                const int k = which == 3 ? n.rankU : n.rankV;
+                const int k = which == 3 ? hss_.rankU[node] : hss_.rankV[node];
                 if (n.is_leaf || k == 0) break;
                 r = c = k;
                 if (out)
@@ -1806,24 +1958,27 @@ void Engine::get_factor(int node, int which, double* out, int* rows, int* cols) 
                 return;
             }
             case 5: {  // B = [[0, B12], [B21, 0]] at (0, lc.rank_V) and (lc.rank_U, 0) (hss_routines.h:105-107)
-                if (n.is_leaf || n.rankU == 0 || n.rankV == 0) break;
-                const Node& L = nodes_[n.left];
-                const Node& R = nodes_[n.right];
-                r = n.rankU;
-                c = n.rankV;
+                const auto& hu = hss_.rankU;
+                const auto& hv = hss_.rankV;
+                if (n.is_leaf || hu[node] == 0 || hv[node] == 0) break;
+                const int lc = n.left, rc = n.right;
+                r = hu[node];
+                c = hv[node];
                 if (out) {
                     std::fill(out, out + (size_t)r * c, 0.0);
-                    std::vector<double> b12((size_t)L.rankU * R.rankV), b21((size_t)R.rankU * L.rankV);
+                    std::vector<double> b12((size_t)hu[lc] * hv[rc]), b21((size_t)hu[rc] * hv[lc]);
                     if (!b12.empty())
-                        HM_CUDA(cudaMemcpy(b12.data(), dB.p + n.offB12, b12.size() * 8, cudaMemcpyDeviceToHost));
+                        HM_CUDA(cudaMemcpy(b12.data(), hss_.B.p + hss_.offB12[node], b12.size() * 8,
+                                           cudaMemcpyDeviceToHost));
                     if (!b21.empty())
-                        HM_CUDA(cudaMemcpy(b21.data(), dB.p + n.offB21, b21.size() * 8, cudaMemcpyDeviceToHost));
-                    for (int j = 0; j < R.rankV; ++j)
-                        for (int i = 0; i < L.rankU; ++i)
-                            out[i + (size_t)(L.rankV + j) * r] = b12[i + (size_t)j * L.rankU];
-                    for (int j = 0; j < L.rankV; ++j)
-                        for (int i = 0; i < R.rankU; ++i)
-                            out[(L.rankU + i) + (size_t)j * r] = b21[i + (size_t)j * R.rankU];
+                        HM_CUDA(cudaMemcpy(b21.data(), hss_.B.p + hss_.offB21[node], b21.size() * 8,
+                                           cudaMemcpyDeviceToHost));
+                    for (int j = 0; j < hv[rc]; ++j)
+                        for (int i = 0; i < hu[lc]; ++i)
+                            out[i + (size_t)(hv[lc] + j) * r] = b12[i + (size_t)j * hu[lc]];
+                    for (int j = 0; j < hv[lc]; ++j)
+                        for (int i = 0; i < hu[rc]; ++i)
+                            out[(hu[lc] + i) + (size_t)j * r] = b21[i + (size_t)j * hu[rc]];
                 }
                 if (rows) *rows = r;
                 if (cols) *cols = c;

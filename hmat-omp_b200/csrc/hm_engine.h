@@ -130,6 +130,7 @@ class Engine {
     void begin_build(int N, int leaf);
     void build_hodlr(const Source& src);
     void build_hss(const Source& src);
+    void reduce_hss_coupling(const std::vector<std::vector<int>>& under);
     // Append steps materialising blocks (dense copy or generator fill).
     void add_block_fill(Plan& plan, const Source& src,
                         const std::vector<std::tuple<int, int, int, int, int, double*, int>>& blocks);
@@ -160,6 +161,15 @@ class Engine {
     // HSS: compressed leaf bases (offset into dLeafB, rank) per leaf node
     DBuf<double> dLeafB;
     std::vector<std::pair<size_t, int>> leafU_, leafV_;
+    // HSS: the reference's representation, kept for export: rank_U / rank_V of every
+    // node (sums over its leaves) and the coupling blocks at those widths.  The operator
+    // in nodes_/dU/dV/dB that factor, solve and multiply use is its recompressed
+    // two-block form (reduce_hss_coupling).
+    struct HssForm {
+        std::vector<int> rankU, rankV;
+        std::vector<size_t> offB12, offB21;
+        DBuf<double> B;
+    } hss_;
     bool built_ = false;
     // factorizations
     FactorStore<double> f64_;

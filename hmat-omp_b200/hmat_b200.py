@@ -74,8 +74,8 @@ def load() -> C.CDLL:
     L.hm_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     for f in ("hm_hodlr_build_from_dense", "hm_hss_build_from_dense"):
         getattr(L, f).argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, C.c_int]
-    L.hm_hodlr_build_from_kernel.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int,
-                                             C.c_int]
+    for f in ("hm_hodlr_build_from_kernel", "hm_hss_build_from_kernel"):
+        getattr(L, f).argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int]
     L.hm_hodlr_build_from_dense_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
     PP = C.POINTER(C.c_void_p)
     L.hm_hodlr_import.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip, PP, PP, PP, PP, PP]
@@ -314,6 +314,8 @@ class HODLRMatrix(_Handle):
         self.N = N
         self._check(self._L.hm_hodlr_build_from_dense_device(self._h, C.c_void_p(dA), N, lda, leaf_size))
 
+    _kernel_build = "hm_hodlr_build_from_kernel"
+
     def build_from_kernel(self, kernel: int, points: np.ndarray, params, leaf_size: int, N: int | None = None):
         """Matrix-free build.  Cauchy: points = concat(x, y) (1-D); Gaussian/Coulomb:
         points N x dim."""
@@ -326,8 +328,8 @@ class HODLRMatrix(_Handle):
             N, dim = pts2.shape
         pr = np.ascontiguousarray(params, dtype=np.float64)
         self.N = N
-        self._check(self._L.hm_hodlr_build_from_kernel(self._h, kernel, _d(pts), dim, N, _d(pr), pr.size,
-                                                       leaf_size))
+        self._check(getattr(self._L, self._kernel_build)(self._h, kernel, _d(pts), dim, N, _d(pr), pr.size,
+                                                         leaf_size))
 
     def import_factors(self, N: int, leaf_size: int, nodes) -> None:
         """Upload a tree of reference factors; ``nodes`` in pre-order with attributes
@@ -367,6 +369,9 @@ class HSSMatrix(_Handle):
         A = np.asfortranarray(A, dtype=np.float64)
         self.N = A.shape[0]
         self._check(self._L.hm_hss_build_from_dense(self._h, _d(A), self.N, self.N, leaf_size))
+
+    _kernel_build = "hm_hss_build_from_kernel"
+    build_from_kernel = HODLRMatrix.build_from_kernel
 
 
 class HODLRBatch(_Handle):

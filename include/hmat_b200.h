@@ -124,6 +124,13 @@ HM_API int hm_hodlr_build_from_kernel(hm_handle* h, int kernel, const double* po
 /* HSSMatrix::build_from_dense(A, leaf_size) (hss_routines.h:50-113): build_topo ids,
  * leaf row/column bases of the off-diagonal strips, identity transfers, dense B. */
 HM_API int hm_hss_build_from_dense(hm_handle* h, const double* A, int N, int lda, int leaf_size);
+/* Matrix-free counterpart of HSSMatrix::build_from_dense (hss_routines.h:50-113): the
+ * leaf strips and coupling blocks are evaluated from the kernel on the device (same
+ * points/params layout as hm_hodlr_build_from_kernel), so A is never stored.  Same
+ * tree, ranks and sketch stream as hm_hss_build_from_dense on the matrix the kernel
+ * defines. */
+HM_API int hm_hss_build_from_kernel(hm_handle* h, int kernel, const double* points, int dim, int N,
+                                    const double* params, int nparams, int leaf_size);
 
 /* Upload a HODLR tree built elsewhere (e.g. by HODLRMatrix::build_from_dense) so the
  * device path can multiply/solve with exactly those factors.  Nodes in pre-order

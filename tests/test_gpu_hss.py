@@ -85,3 +85,22 @@ def test_hss_factor_download_matches_oracle():
             ref_blk = o.reconstruct_U(n.left) @ n.B[:lu, lv:] @ o.reconstruct_V(n.right).T
             dev_blk = basis(n.left, H.HSSMatrix.U) @ B[:lu, lv:] @ basis(n.right, H.HSSMatrix.V).T
             assert O.rel_err(ref_blk, dev_blk) < 1e-10
+
+
+@pytest.mark.parametrize("name", HSS_CASES)
+def test_hss_kernel_build_matches_dense(name):
+    """hm_hss_build_from_kernel (entries generated on the device, A never stored) gives
+    the operator the dense build gives: same tree and ranks, multiply and solve equal to
+    rounding (same sketch stream)."""
+    c = CASES[name]
+    A = make_matrix(c)
+    x, b = make_vectors(c, A.shape[0])
+    from cases import points
+    hd = build(c, A)
+    hk = H.HSSMatrix(c["tol"], rsvd_rank=c["rsvd_rank"], seed=c["seed"])
+    hk.build_from_kernel(H.KERNEL_GAUSSIAN, points(c, A.shape[0]), [c["h"], c["shift"]], c["leaf"])
+    td, tk = hd.tree(), hk.tree()
+    for key in ("start", "end", "is_leaf", "rank12", "rank21"):
+        assert np.array_equal(td[key], tk[key]), key
+    assert O.rel_err(hd.multiply(x), hk.multiply(x)) < 1e-12
+    assert O.rel_err(hd.solve(b), hk.solve(b)) < 1e-10
