@@ -561,8 +561,12 @@ def run_hss(args):
     torch.cuda.synchronize()
     resid = float(torch.linalg.norm(y - b) / torch.linalg.norm(b))
     t = h.tree()
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = hss_reference_sample()
     print(json.dumps({
         "metric": "HSS factor+solve RHS/s (Gaussian 1-D, N=65536, 32 RHS, FP64)", "value": s / (ms / 1e3),
+        "cpu_baseline": cpu,
         "unit": "RHS/s", "higher_is_better": True, "n_gpus": 1, "ms_per_step": ms, "ms_factor": ms_f,
         "steps": args.steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic", "build_s": t_build,
         "rel_residual": resid, "hss_ranks": {"max": int(t["rank12"].max()), "leaf_mean": float(
@@ -571,6 +575,30 @@ def run_hss(args):
                    "nrhs": s, "h": 0.05, "shift": 1e-2, "points": "sorted U[0,1], seed 2", "build": "matrix-free",
                    "refine_steps": 1},
     }))
+
+
+def hss_reference_sample():
+    """The reference's HSSMatrixOMP::solve (hss_routines_omp.h:235-290) on the host cores
+    at N = 1024 (same kernel and tolerances, 1 RHS).  Its recursion re-solves every
+    child for the columns of the parent's basis, so its cost grows much faster than N
+    (measured: 4.4 s at N = 1024, 365 s at N = 2048 on 8 cores); N = 65536 is out of
+    reach and the sample is reported as measured, not extrapolated."""
+    import ref
+    if not ref.available():
+        return None
+    import hmat_oracle as O
+    Ns = 1024
+    xs = np.sort(np.random.default_rng(2).random(Ns))
+    A = O.gaussian_matrix(xs, 0.05, 1e-2)
+    R = ref.RefHSS(A, 128, 1e-10, 64, seed=0, omp=True)
+    b = np.random.default_rng(5).standard_normal((Ns, 1))
+    t0 = time.perf_counter()
+    R.solve(b)
+    per = time.perf_counter() - t0
+    R.close()
+    return {"value": 1.0 / per, "unit": "RHS/s", "cores": ref.lib().hmref_omp_max_threads(), "kind": "reference",
+            "sample": f"HSSMatrixOMP::solve, 1 RHS, N={Ns} leaf 128 tol 1e-10 ({per:.2f} s); the reference's "
+                      "solve cost grows super-linearly (365 s at N=2048 on 8 cores), N=65536 not reachable"}
 
 
 def run_adjoint(args):
