@@ -13,6 +13,7 @@
 #include "hm_dense.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 
 namespace hm {
@@ -83,8 +84,48 @@ std::string Profiler::sequence() {
     return out + "]";
 }
 
+bool graphs_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("HM_CUDA_GRAPHS");
+        return !(e && e[0] == '0' && e[1] == 0);
+    }();
+    return on;
+}
+
+void Plan::capture(cudaStream_t s, int* status) const {
+    graph_.reset();
+    cudaGraph_t g = nullptr;
+    HM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+        for (auto& st : steps_) st->run(s, status);
+    } catch (...) {
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    HM_CUDA(cudaStreamEndCapture(s, &g));
+    cudaGraphExec_t e = nullptr;
+    const cudaError_t rc = cudaGraphInstantiate(&e, g, 0);
+    cudaGraphDestroy(g);
+    HM_CUDA(rc);
+    graph_.reset(e, [](cudaGraphExec_t x) { cudaGraphExecDestroy(x); });
+    graph_status_ = status;
+}
+
 void Plan::run(cudaStream_t s, int* status) const {
     Profiler& P = Profiler::get();
+    if (runs_ >= 1 && !steps_.empty() && !P.enabled && s != nullptr && s != cudaStreamLegacy && graphs_enabled()) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        HM_CUDA(cudaStreamIsCapturing(s, &cs));
+        if (cs == cudaStreamCaptureStatusNone) {
+            if (!graph_ || graph_status_ != status) capture(s, status);
+            HM_CUDA(cudaGraphLaunch(graph_.get(), s));
+            for (auto& st : steps_) P.launches += st->nlaunch();
+            ++runs_;
+            return;
+        }
+    }
+    ++runs_;
     for (auto& st : steps_) {
         const int nl = st->nlaunch();
         if (P.enabled && nl > 0) {

@@ -137,13 +137,26 @@ class Plan {
         virtual double bytes() const { return 0; }
     };
     void add(std::unique_ptr<Step> st) { steps_.push_back(std::move(st)); }
+    // Runs the steps in order on s.  The first run launches them one by one; the second
+    // captures them into a CUDA graph (one per plan, i.e. per tree shape and column
+    // count) and every run from then on replays that graph.  Runs launch one by one
+    // instead while the profiler is on, on the legacy default stream, on a stream the
+    // caller is already capturing (the launches then join the caller's graph), or with
+    // HM_CUDA_GRAPHS=0.  A plan captured with one status word is re-captured if run
+    // with another.
     void run(cudaStream_t s, int* status) const;
     bool empty() const { return steps_.empty(); }
     // device scratch owned by the plan (bump-allocated from large chunks)
     double* scratch(size_t count) { return static_cast<double*>(bump(count * sizeof(double))); }
     float* scratch_f(size_t count) { return static_cast<float*>(bump(count * sizeof(float))); }
     int* scratch_i(size_t count) { return static_cast<int*>(bump(count * sizeof(int))); }
-    void clear() { steps_.clear(); chunks_.clear(); used_ = cap_ = 0; }
+    void clear() {
+        graph_.reset();
+        runs_ = 0;
+        steps_.clear();
+        chunks_.clear();
+        used_ = cap_ = 0;
+    }
     size_t scratch_bytes() const {
         size_t b = 0;
         for (auto& c : chunks_) b += c.n;
@@ -163,10 +176,15 @@ class Plan {
         used_ += bytes;
         return p;
     }
+    void capture(cudaStream_t s, int* status) const;
     std::vector<std::unique_ptr<Step>> steps_;
     std::vector<DBuf<unsigned char>> chunks_;
     size_t used_ = 0, cap_ = 0;
+    mutable std::shared_ptr<CUgraphExec_st> graph_;
+    mutable int* graph_status_ = nullptr;
+    mutable int runs_ = 0;
 };
+bool graphs_enabled();
 
 // Which labelled FP32 steps may run on the tensor cores.  By default the three bulk
 // updates of the factorization (leaf_apply, update_project, update_small).  The rest of
