@@ -317,4 +317,8 @@ size_t hm_profile_sequence(char* buf, size_t len) {
     return copy_out_text(r, buf, len);
 }
 
+int hm_tile_table_load(const char* path) { return hm::tile_table_load(path) ? HM_OK : HM_ERR_ARG; }
+
+int hm_tile_table_size(void) { return hm::tile_table_size(); }
+
 }  // extern "C"

@@ -71,14 +71,14 @@ std::string Profiler::report() {
 
 std::string Profiler::sequence() {
     std::string out = "[";
-    char buf[320];
+    char buf[512];
     for (size_t i = 0; i < recs.size(); ++i) {
         const Rec& r = recs[i];
         HM_CUDA(cudaEventSynchronize(r.b));
         float ms = 0;
         HM_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
-        snprintf(buf, sizeof buf, "%s[\"%s\", %d, %.6f, %.6e, %.6e]", i ? ", " : "", r.name.c_str(), r.launches, ms,
-                 r.flops, r.bytes);
+        snprintf(buf, sizeof buf, "%s[\"%s\", %d, %.6f, %.6e, %.6e, \"%s\"]", i ? ", " : "", r.name.c_str(),
+                 r.launches, ms, r.flops, r.bytes, r.sig.c_str());
         out += buf;
     }
     return out + "]";
@@ -129,7 +129,7 @@ void Plan::run(cudaStream_t s, int* status) const {
     for (auto& st : steps_) {
         const int nl = st->nlaunch();
         if (P.enabled && nl > 0) {
-            Profiler::Rec r{st->name(), P.event(), P.event(), st->flops(), st->bytes(), nl};
+            Profiler::Rec r{st->name(), P.event(), P.event(), st->flops(), st->bytes(), nl, st->sig()};
             HM_CUDA(cudaEventRecord(r.a, s));
             st->run(s, status);
             HM_CUDA(cudaEventRecord(r.b, s));

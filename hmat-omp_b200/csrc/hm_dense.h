@@ -110,6 +110,7 @@ struct Profiler {
         cudaEvent_t a, b;
         double flops, bytes;
         int launches;
+        std::string sig;   // tuning signature and tile choice of a GEMM step ("" otherwise)
     };
     bool enabled = false;
     long long launches = 0;
@@ -120,7 +121,8 @@ struct Profiler {
     void reset();
     // {"name": [launches, ms, flops, bytes], ...} (synchronises)
     std::string report();
-    // [["name", launches, ms, flops, bytes], ...] in record order (synchronises)
+    // [["name", launches, ms, flops, bytes, "signature#bn,small,tc"], ...] in record
+    // order (synchronises)
     std::string sequence();
 };
 inline void count_launch(int n = 1) { Profiler::get().launches += n; }
@@ -135,6 +137,7 @@ class Plan {
         virtual int nlaunch() const { return 1; }
         virtual double flops() const { return 0; }
         virtual double bytes() const { return 0; }
+        virtual std::string sig() const { return ""; }
     };
     void add(std::unique_ptr<Step> st) { steps_.push_back(std::move(st)); }
     // Runs the steps in order on s.  The first run launches them one by one; the second
@@ -212,6 +215,7 @@ struct GemmStep : Plan::Step {
     std::string label_tc;   // the same when the batch runs on the tensor cores
     explicit GemmStep(int cfg = CFG_64x64, int gen = GEN_DENSE) : batch(cfg, gen) {}
     GemmStep(const char* lbl) : batch(CFG_64x64, GEN_DENSE) {
+        batch.set_tag(lbl);
         label = std::string(sizeof(T) == 8 ? "gemm_f64:" : "gemm_f32:") + lbl;
         label_tc = std::string("tc_tf32x4:") + lbl;
         batch.allow_tensor_cores(tensor_cores_allowed(lbl));
@@ -226,6 +230,7 @@ struct GemmStep : Plan::Step {
     int nlaunch() const override { return batch.nlaunch(); }
     double flops() const override { return batch.flops(); }
     double bytes() const override { return batch.bytes(); }
+    std::string sig() const override { return batch.signature() + "#" + batch.choice(); }
 };
 
 struct GJStep : Plan::Step {

@@ -11,9 +11,17 @@
 
 #include "hm_gemm.h"
 
+#include <dlfcn.h>
+
 #include <algorithm>
+#include <cctype>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+#include <unordered_map>
 
 namespace hm {
 
@@ -375,6 +383,164 @@ void GemmBatch<T>::add(int m, int n, int k, T alpha, const T* A, int lda, int op
     h_.push_back(d);
 }
 
+// ---------------------------------------------------------------------------------
+// Tile-choice table (autotune.py writes it; finalize consults it)
+// ---------------------------------------------------------------------------------
+namespace {
+struct TileTable {
+    std::mutex mu;
+    bool loaded = false;
+    std::unordered_map<std::string, TileChoice> map;
+};
+TileTable& tile_table() {
+    static TileTable t;
+    return t;
+}
+
+bool valid_choice(const TileChoice& c) {
+    return (c.bn == 32 || c.bn == 64 || c.bn == 96 || c.bn == 128) && (c.small == 0 || c.small == 1) &&
+           (c.tc == 0 || c.tc == 1);
+}
+
+// {"signature": [bn, small, tc], ...}; nothing else is accepted
+bool parse_tile_table(const std::string& txt, std::unordered_map<std::string, TileChoice>& out) {
+    size_t i = 0;
+    auto peek = [&]() -> char { return i < txt.size() ? txt[i] : '\0'; };
+    auto skip = [&] { while (i < txt.size() && std::isspace((unsigned char)txt[i])) ++i; };
+    skip();
+    if (peek() != '{') return false;
+    ++i;
+    skip();
+    if (peek() == '}') return true;
+    for (;;) {
+        skip();
+        if (peek() != '"') return false;
+        const size_t j = txt.find('"', i + 1);
+        if (j == std::string::npos) return false;
+        const std::string key = txt.substr(i + 1, j - i - 1);
+        i = j + 1;
+        skip();
+        if (peek() != ':') return false;
+        ++i;
+        skip();
+        if (peek() != '[') return false;
+        ++i;
+        long v[3];
+        for (int q = 0; q < 3; ++q) {
+            skip();
+            const char* b = txt.c_str() + i;
+            char* e = nullptr;
+            v[q] = std::strtol(b, &e, 10);
+            if (e == b) return false;
+            i += (size_t)(e - b);
+            skip();
+            if (q < 2) {
+                if (peek() != ',') return false;
+                ++i;
+            }
+        }
+        if (peek() != ']') return false;
+        ++i;
+        TileChoice c;
+        c.bn = (int)v[0];
+        c.small = (int)v[1];
+        c.tc = (int)v[2];
+        if (!valid_choice(c)) return false;
+        out[key] = c;
+        skip();
+        if (peek() == ',') { ++i; continue; }
+        if (peek() == '}') return true;
+        return false;
+    }
+}
+
+bool read_tile_table(const std::string& path, std::unordered_map<std::string, TileChoice>& out) {
+    std::ifstream f(path);
+    if (!f) return false;
+    std::stringstream ss;
+    ss << f.rdbuf();
+    std::unordered_map<std::string, TileChoice> m;
+    if (!parse_tile_table(ss.str(), m)) return false;
+    out.swap(m);
+    return true;
+}
+
+std::string library_dir() {
+    Dl_info info{};
+    if (!dladdr(reinterpret_cast<void*>(&tile_table_size), &info) || !info.dli_fname) return "";
+    std::string p(info.dli_fname);
+    const size_t slash = p.rfind('/');
+    return slash == std::string::npos ? std::string(".") : p.substr(0, slash);
+}
+
+const TileChoice* forced_choice() {
+    static TileChoice c;
+    static const bool on = [] {
+        const char* e = std::getenv("HM_TILE_FORCE");
+        if (!e || !*e) return false;
+        int bn = 0, sm = 0, tc = 0;
+        HM_CHECK(std::sscanf(e, "%d,%d,%d", &bn, &sm, &tc) == 3, HM_ERR_ARG, "HM_TILE_FORCE: expected bn,small,tc");
+        c.bn = bn;
+        c.small = sm;
+        c.tc = tc;
+        HM_CHECK(valid_choice(c), HM_ERR_ARG, "HM_TILE_FORCE: bn in {32,64,96,128}, small and tc 0 or 1");
+        return true;
+    }();
+    return on ? &c : nullptr;
+}
+}  // namespace
+
+bool tile_choice(const std::string& sig, TileChoice& out) {
+    if (const TileChoice* f = forced_choice()) {
+        out = *f;
+        return true;
+    }
+    TileTable& t = tile_table();
+    std::lock_guard<std::mutex> g(t.mu);
+    if (!t.loaded) {
+        t.loaded = true;
+        const char* e = std::getenv("HM_TILE_TABLE");
+        if (e && *e) {
+            HM_CHECK(read_tile_table(e, t.map), HM_ERR_ARG, std::string("HM_TILE_TABLE: cannot read ") + e);
+        } else {
+            const std::string dir = library_dir();
+            if (!dir.empty()) read_tile_table(dir + "/tile_table.json", t.map);  // optional
+        }
+    }
+    auto it = t.map.find(sig);
+    if (it == t.map.end()) return false;
+    out = it->second;
+    return true;
+}
+
+bool tile_table_load(const char* path) {
+    TileTable& t = tile_table();
+    std::lock_guard<std::mutex> g(t.mu);
+    t.loaded = true;
+    if (!path || !*path) {
+        t.map.clear();
+        return true;
+    }
+    return read_tile_table(path, t.map);
+}
+
+int tile_table_size() {
+    TileTable& t = tile_table();
+    std::lock_guard<std::mutex> g(t.mu);
+    return (int)t.map.size();
+}
+
+static int pow2_ceil(long long v) {
+    int p = 1;
+    while (p < v && p < (1 << 30)) p <<= 1;
+    return p;
+}
+
+template <typename T>
+std::string GemmBatch<T>::choice() const {
+    return std::to_string(pipe_bn_) + "," + (pipe_small_ ? "1" : "0") + "," + (use_tc_ ? "1" : "0");
+}
+
 template <typename T>
 void GemmBatch<T>::finalize(cudaStream_t s) {
     int t = 0;
@@ -387,6 +553,24 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         bytes_ += sizeof(T) * (a + (double)d.k * d.n + (double)d.m * d.n * (d.beta != T(0) ? 2 : 1));
     }
     total_tiles_ = t;
+    {   // tuning signature
+        int mmax = 0, nmax = 0;
+        std::vector<int> ks;
+        ks.reserve(h_.size());
+        for (auto& d : h_) {
+            mmax = std::max(mmax, d.m);
+            nmax = std::max(nmax, d.n);
+            ks.push_back(d.k);
+        }
+        int kmed = 0;
+        if (!ks.empty()) {
+            std::nth_element(ks.begin(), ks.begin() + ks.size() / 2, ks.end());
+            kmed = ks[ks.size() / 2];
+        }
+        sig_ = tag_ + (sizeof(T) == 4 ? "|f32" : "|f64") + "|p" + std::to_string(pow2_ceil((long long)h_.size())) +
+               "|m" + std::to_string(pow2_ceil(mmax)) + "|n" + std::to_string(ceil_div(nmax, 32) * 32) + "|k" +
+               std::to_string(pow2_ceil(kmed));
+    }
     // dense batches run the warp-tiled kernel: tile counts for its shape in a device-side
     // copy of the table (BN fitted to the widest problem: ranks are usually <= 96)
     pipe_bn_ = 0;
@@ -399,6 +583,9 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         }
         if (!any_scale) pipe_bn_ = nmax <= 32 ? 32 : nmax <= 64 ? 64 : nmax <= 96 ? 96 : 128;
     }
+    TileChoice tuned;
+    const bool have_tuned = pipe_bn_ && tile_choice(sig_, tuned);
+    if (have_tuned) pipe_bn_ = tuned.bn;
     if (pipe_bn_) {
         // 64-row tiles when the batch's problems are short enough that 128-row (or
         // 256-row) tiles would pad more than a quarter of the rows
@@ -409,7 +596,7 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
             pad_big += (double)ceil_div(d.m, big) * big - d.m;
             pad_small += (double)ceil_div(d.m, 64) * 64 - d.m;
         }
-        pipe_small_ = big > 64 && pad_big > 0.25 * rows && pad_small < pad_big;
+        pipe_small_ = have_tuned ? tuned.small != 0 : big > 64 && pad_big > 0.25 * rows && pad_small < pad_big;
         const int BM = tile::bm_for(sizeof(T), pipe_bn_, pipe_small_);
         std::vector<GemmDesc<T>> dv(h_);
         int tt = 0;
@@ -438,7 +625,7 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
     }
     use_tc_ = false;
     if constexpr (std::is_same<T, float>::value) {
-        if (pipe_bn_ && tc_allowed_) finalize_tc(s);
+        if (pipe_bn_ && tc_allowed_ && (!have_tuned || tuned.tc)) finalize_tc(s);
     }
     if (!hz_.empty()) {
         dz_.alloc(hz_.size());

@@ -10,6 +10,8 @@
 // hold beta*C (the batch zeroes C first when beta == 0).
 #pragma once
 
+#include <string>
+
 #include "hm_common.h"
 
 namespace hm {
@@ -75,6 +77,23 @@ void gemm_launch_tables(const GemmDesc<double>* dtab, int ndesc, int total_tiles
 // Tile configurations.
 enum : int { CFG_64x64 = 0, CFG_N_SKINNY = 1 };
 
+// Autotuned tile choices for the dense batched GEMM.  A batch is identified by its
+// signature (step tag, element type and bucketed problem count / m / n / k, see
+// GemmBatch::signature); the choice is the warp-tiled kernel's tile width BN, its
+// 64-row tile shapes, and whether an eligible FP32 batch takes the tensor-core kernel.
+// Sources, first match wins: HM_TILE_FORCE="bn,small,tc" (every batch; the offline
+// sweep's switch), then the table in the JSON file HM_TILE_TABLE names, else
+// tile_table.json beside the loaded library ({"signature": [bn, small, tc], ...},
+// written by autotune.py).  Batches without an entry keep the built-in heuristics.
+struct TileChoice {
+    int bn = 0, small = 0, tc = 1;
+};
+bool tile_choice(const std::string& sig, TileChoice& out);
+// Replace the table with the one in `path` (an empty path clears it); false if the file
+// cannot be read or parsed.
+bool tile_table_load(const char* path);
+int tile_table_size();
+
 template <typename T>
 class GemmBatch {
   public:
@@ -85,6 +104,13 @@ class GemmBatch {
              int ga_r0 = 0, int ga_c0 = 0);
     bool empty() const { return h_.empty(); }
     size_t size() const { return h_.size(); }
+    // step name used in the tuning signature
+    void set_tag(const std::string& t) { tag_ = t; }
+    // "<tag>|<f32|f64>|p<count>|m<max m>|n<max n>|k<median k>" (counts and m/k rounded up
+    // to powers of two, n to multiples of 32); set by finalize
+    const std::string& signature() const { return sig_; }
+    // "bn,small,tc" as finalize chose it (bn 0: not the warp-tiled kernel)
+    std::string choice() const;
     // Upload the table (once); later launches reuse it (and may be graph-captured).
     void finalize(cudaStream_t s);
     void finalize_tc(cudaStream_t s);
@@ -117,6 +143,7 @@ class GemmBatch {
 
   private:
     int cfg_, gen_;
+    std::string tag_, sig_;
     std::vector<GemmDesc<T>> h_;
     DBuf<GemmDesc<T>> d_;
     // regions to zero before a split-K launch

@@ -104,6 +104,8 @@ def load() -> C.CDLL:
     for f in ("hm_profile_report", "hm_profile_sequence"):
         getattr(L, f).argtypes = [C.c_char_p, C.c_size_t]
         getattr(L, f).restype = C.c_size_t
+    L.hm_tile_table_load.argtypes = [C.c_char_p]
+    L.hm_tile_table_size.argtypes = []
     _lib = L
     return L
 
@@ -127,8 +129,20 @@ def profile_report() -> dict:
     return {k: tuple(v) for k, v in json.loads(buf.value.decode()).items()}
 
 
+def tile_table_load(path: str | None) -> None:
+    """Replace the batched-GEMM tile table (autotune.py's JSON); None or "" clears it."""
+    rc = load().hm_tile_table_load((path or "").encode())
+    if rc != HM_OK:
+        raise HmError(rc, f"cannot read tile table {path!r}")
+
+
+def tile_table_size() -> int:
+    return load().hm_tile_table_size()
+
+
 def profile_sequence() -> list:
-    """[(step, launches, ms, algorithmic flops, algorithmic bytes), ...] in launch order."""
+    """[(step, launches, ms, algorithmic flops, algorithmic bytes, tuning), ...] in launch
+    order; tuning = "signature#bn,small,tc" for batched-GEMM steps, else ""."""
     import json
     L = load()
     n = L.hm_profile_sequence(None, 0)

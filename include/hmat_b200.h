@@ -222,9 +222,24 @@ HM_API void hm_profile_enable(int on);
  * (including the terminating NUL); writes at most len bytes. */
 HM_API size_t hm_profile_report(char* buf, size_t len);
 /* The same records in launch order, one per recorded step execution:
- * JSON [["step", launches, ms, algorithmic flops, algorithmic bytes], ...] (lines up with
- * a profiler's kernel list, step by step); same buffer convention. */
+ * JSON [["step", launches, ms, algorithmic flops, algorithmic bytes, "tuning"], ...]
+ * (lines up with a profiler's kernel list, step by step); "tuning" is
+ * "<signature>#<bn>,<small>,<tc>" for batched-GEMM steps (see hm_tile_table_load), ""
+ * otherwise; same buffer convention. */
 HM_API size_t hm_profile_sequence(char* buf, size_t len);
+
+/* ---- tile autotuning (no counterpart in the reference) ----
+ * Batched-GEMM steps pick their tile shape (width BN of the warp-tiled kernel, its 64-row
+ * shapes, tensor cores or not for eligible FP32 batches) from a table keyed by the batch's
+ * signature (step, element type, bucketed problem count and m/n/k), written by
+ * hmat-omp_b200/autotune.py from timed sweeps: JSON {"signature": [bn, small, tc], ...}.
+ * The table is read from HM_TILE_TABLE if set, else from tile_table.json beside the
+ * library, at the first batch finalised; entries apply to operators planned afterwards.
+ * Batches without an entry keep the built-in heuristics.  hm_tile_table_load replaces
+ * the table (NULL or "" clears it); returns HM_OK or HM_ERR_ARG if the file cannot be
+ * read or parsed.  hm_tile_table_size: entries in the table. */
+HM_API int hm_tile_table_load(const char* path);
+HM_API int hm_tile_table_size(void);
 
 #ifdef __cplusplus
 }
