@@ -561,6 +561,14 @@ def run_hss(args):
     torch.cuda.synchronize()
     resid = float(torch.linalg.norm(y - b) / torch.linalg.norm(b))
     t = h.tree()
+    # the same right-hand sides solved against the exact kernel operator (the factors as
+    # preconditioner, residuals from generated entries of A)
+    bh = b.cpu().numpy().T
+    t0 = time.perf_counter()
+    _, est = h.solve_exact(bh, tol=1e-10, max_iter=10, stats=True)
+    t_exact = time.perf_counter() - t0
+    exact = {"tol": 1e-10, "seconds": t_exact, "sweeps": est.ir_iters, "rel_residual_vs_exact_A": est.rel_residual,
+             "flops_per_sweep": 2.0 * N * N * s}
     cpu = None
     if not args.no_cpu_baseline:
         cpu = hss_reference_sample()
@@ -569,7 +577,7 @@ def run_hss(args):
         "cpu_baseline": cpu,
         "unit": "RHS/s", "higher_is_better": True, "n_gpus": 1, "ms_per_step": ms, "ms_factor": ms_f,
         "steps": args.steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic", "build_s": t_build,
-        "rel_residual": resid, "hss_ranks": {"max": int(t["rank12"].max()), "leaf_mean": float(
+        "rel_residual": resid, "exact_operator_refinement": exact, "hss_ranks": {"max": int(t["rank12"].max()), "leaf_mean": float(
             t["rank12"][t["is_leaf"] == 1].mean())},
         "config": {"workload": "hss_gaussian_N65536_leaf128", "N": N, "leaf": leaf, "tol": 1e-10, "max_rank": 64,
                    "nrhs": s, "h": 0.05, "shift": 1e-2, "points": "sorted U[0,1], seed 2", "build": "matrix-free",

@@ -229,6 +229,19 @@ int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ld
     });
 }
 
+int hm_solve_exact_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx, double tol,
+                          int max_iter, hm_solve_stats* st) {
+    return guard(h, [&] { built(h).solve_exact_device(db, nrhs, ldb, dx, ldx, tol, max_iter, st); });
+}
+
+int hm_solve_exact(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ldx, double tol, int max_iter,
+                   hm_solve_stats* st) {
+    return guard(h, [&] {
+        built(h).solve_exact_device(b, nrhs, ldb, x, ldx, tol, max_iter, st);   // host pointers: unified addressing
+        HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
 int hm_batch_build_from_kernel(hm_handle* h, int kernel, const double* points, int dim, int nsys, const int* N,
                                const double* params, int leaf) {
     return guard(h, [&] {

@@ -122,7 +122,7 @@ __global__ void residual_kernel(const double* __restrict__ b, double* __restrict
         double bv = b[e];
         double rv = bv - r[e];
         r[e] = rv;
-        rf[e] = (float)rv;
+        if (rf) rf[e] = (float)rv;
         a2 += rv * rv;
         c2 += bv * bv;
     }
@@ -291,6 +291,9 @@ void Engine::begin_build(int N, int leaf) {
     solve64_plans_.clear();
     solve32_plans_.clear();
     solveT_plans_.clear();
+    exact_plans_.clear();
+    io_cols_ = 0;        // staging buffers are sized N x columns: a new N needs new ones
+    ex_cols_ = 0;
     grads_ready_ = false;
     gen_ = GEN_DENSE;
     gp_ = GenParams();
@@ -1730,6 +1733,82 @@ void Engine::solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, 
     if (!(worst <= opts_.ir_tol)) {
         char msg[128];
         snprintf(msg, sizeof msg, "iterative refinement stopped at relative residual %.3e after %d sweeps", worst, it);
+        throw Error(HM_ERR_IR, msg);
+    }
+}
+
+// Refinement against the exact kernel operator of a matrix-free build:
+//   x = A~^{-1} b;  repeat r = b - A x (A generated on the device, 2 N^2 s flops),
+//   stop when max_j ||r_j|| / ||b_j|| <= tol, else x += A~^{-1} r,
+// with A~^{-1} the compressed factorization in the handle's precision.  Each sweep
+// contracts the error by about ||A - A~|| ||A~^{-1}||.
+Plan& Engine::exact_plan(int s) {
+    auto it = exact_plans_.find(s);
+    if (it != exact_plans_.end()) return it->second;
+    Plan& pl = exact_plans_[s];
+    auto g = std::make_unique<GemmStep<double>>(s <= 16 ? CFG_N_SKINNY : CFG_64x64, gen_);
+    g->gp = gp_;
+    g->batch.add(N_, s, N_, 1.0, nullptr, 0, OP_N, exX_.p, N_, OP_N, 0.0, exR_.p, N_, nullptr, 0, 0, 0);
+    g->batch.finalize(stream_);
+    pl.add(std::move(g));
+    return pl;
+}
+
+void Engine::solve_exact_device(const double* db, int s, int ldb, double* dx, int ldx, double tol, int max_iter,
+                                hm_solve_stats* st) {
+    HM_CHECK(built_, HM_ERR_STATE, "solve_exact before build");
+    HM_CHECK(gen_ != GEN_DENSE && sys_N_.size() == 1, HM_ERR_STATE,
+             "solve_exact needs a single operator built from a kernel (hm_*_build_from_kernel)");
+    HM_CHECK(s >= 1 && ldb >= N_ && ldx >= N_ && db && dx && tol > 0 && max_iter >= 0, HM_ERR_ARG,
+             "solve_exact: bad arguments");
+    const size_t n = (size_t)N_ * s;
+    if (s > ex_cols_) {
+        exB_.alloc(n);
+        exX_.alloc(n);
+        exR_.alloc(n);
+        exD_.alloc(n);
+        exNorm_.alloc(2 * (size_t)s);
+        ex_cols_ = s;
+        exact_plans_.clear();
+    }
+    cudaStream_t q = stream_;
+    HM_CUDA(cudaMemcpy2DAsync(exB_.p, (size_t)N_ * sizeof(double), db, (size_t)ldb * sizeof(double),
+                              (size_t)N_ * sizeof(double), s, cudaMemcpyDefault, q));
+    solve_device(exB_.p, s, N_, exX_.p, N_, nullptr);
+    Plan& ap = exact_plan(s);
+    std::vector<double> hn(2 * (size_t)s);
+    double worst = 0.0;
+    int it = 0;
+    for (;; ++it) {
+        ap.run(q, dstatus.p);   // exR = A x
+        HM_CUDA(cudaMemsetAsync(exNorm_.p, 0, 2 * (size_t)s * sizeof(double), q));
+        residual_kernel<<<dim3(std::min(64, ceil_div(N_, 256)), s), 256, 0, q>>>(
+            exB_.p, exR_.p, nullptr, N_, s, exNorm_.p, exNorm_.p + s);   // exR = b - A x
+        count_launch();
+        HM_CUDA(cudaMemcpyAsync(hn.data(), exNorm_.p, 2 * s * sizeof(double), cudaMemcpyDeviceToHost, q));
+        HM_CUDA(cudaStreamSynchronize(q));
+        check_status("solve_exact");
+        worst = 0.0;
+        for (int j = 0; j < s; ++j) {
+            const double den = std::sqrt(hn[s + j]);
+            worst = std::max(worst, den > 0 ? std::sqrt(hn[j]) / den : std::sqrt(hn[j]));
+        }
+        if (!(worst == worst) || worst <= tol || it >= max_iter) break;
+        solve_device(exR_.p, s, N_, exD_.p, N_, nullptr);
+        axpby_kernel<<<grid_for(n), 256, 0, q>>>(exX_.p, exX_.p, 1.0, exD_.p, 1.0, n);
+        count_launch();
+    }
+    HM_CUDA(cudaMemcpy2DAsync(dx, (size_t)ldx * sizeof(double), exX_.p, (size_t)N_ * sizeof(double),
+                              (size_t)N_ * sizeof(double), s, cudaMemcpyDefault, q));
+    HM_CUDA(cudaStreamSynchronize(q));
+    if (st) {
+        st->ir_iters = it;
+        st->rel_residual = worst;
+    }
+    if (!(worst <= tol)) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "exact-operator refinement stopped at relative residual %.3e after %d sweeps",
+                 worst, it);
         throw Error(HM_ERR_IR, msg);
     }
 }

@@ -99,6 +99,9 @@ class Engine {
     void multiply_device(const double* dx, int s, int ldx, double* dy, int ldy);
     void factor();
     void solve_device(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st);
+    // refinement against the exact kernel operator (matrix-free builds)
+    void solve_exact_device(const double* db, int s, int ldb, double* dx, int ldx, double tol, int max_iter,
+                            hm_solve_stats* st);
     // adjoint solve and gradient accumulation
     void solve_transpose_device(const double* dg, int s, int ldg, double* dl, int ldl);
     void gradients(const double* dx, int ldx, const double* dl, int ldl, int s, double* dparams);
@@ -141,6 +144,7 @@ class Engine {
     Plan& matvec_plan(const std::vector<int>& sc);
     std::vector<int> uniform(int s) const { return std::vector<int>(sys_N_.size(), s); }
     Plan& solveT_plan(int s);
+    Plan& exact_plan(int s);
     void ensure_io(int s);
     std::vector<int> path_of(int n) const;   // n and its ancestors below the root
     void solve_fp64(const double* db, int s, int ldb, double* dx, int ldx);
@@ -183,6 +187,10 @@ class Engine {
     int io_cols_ = 0;
     std::map<std::vector<int>, Plan> mv_plans_, solve64_plans_, solve32_plans_;
     std::map<int, Plan> solveT_plans_;
+    // exact-operator refinement: b, x, r, correction (N x ex_cols_), norms, A x plans
+    DBuf<double> exB_, exX_, exR_, exD_, exNorm_;
+    int ex_cols_ = 0;
+    std::map<int, Plan> exact_plans_;
     // independent systems sharing the launches: size and first global row of each
     std::vector<int> sys_N_{0}, sys_off_{0};
     DBuf<int> dRowSys;

@@ -183,6 +183,22 @@ HM_API int hm_num_systems(const hm_handle* h);
 HM_API int hm_batch_solve(hm_handle* h, const double* b, const int* nrhs, double* x);
 HM_API int hm_batch_multiply(hm_handle* h, const double* x, const int* nrhs, double* y);
 
+/* ---- exact-operator refinement (no counterpart in the reference) ----
+ * For operators built by hm_*_build_from_kernel: solve A x = b with A the exact kernel
+ * matrix, the compressed factorization serving as the preconditioner of an iterative
+ * refinement x += A~^{-1}(b - A x) whose residual is computed with A's entries generated
+ * on the device (2 N^2 nrhs flops per sweep; A is never stored).  Stops when
+ * max_j ||b_j - A x_j|| / ||b_j|| <= tol (stats: sweeps, that residual) or returns
+ * HM_ERR_IR after max_iter sweeps (x then holds the last iterate).  Each sweep contracts
+ * the error by about ||A - A~|| ||A~^{-1}||: a few sweeps when the compression tolerance
+ * times cond(A) is well below one.  HM_ERR_STATE for dense builds and batches.  Host or
+ * device b/x; the _device form takes device pointers (it synchronises once per sweep to
+ * read the residual norms). */
+HM_API int hm_solve_exact(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ldx, double tol,
+                          int max_iter, hm_solve_stats* stats);
+HM_API int hm_solve_exact_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx,
+                                 double tol, int max_iter, hm_solve_stats* stats);
+
 /* ---- adjoint (no counterpart in the reference) ----
  * A^T lam = g with the FP64 factorization run transposed in reverse level order
  * (the transpose of the Woodbury recursion of hodlr_routines.h:112-175); factors in FP64
