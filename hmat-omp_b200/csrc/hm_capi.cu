@@ -185,6 +185,18 @@ int hm_hodlr_import(hm_handle* h, int N, int leaf, const int* r12, const int* r2
     return guard(h, [&] { engine(h, hm::Engine::HODLR).import_hodlr(N, leaf, r12, r21, D, U, V, B12, B21); });
 }
 
+int hm_save(hm_handle* h, const char* path) {
+    return guard(h, [&] { built(h).save(path); });
+}
+
+int hm_load(hm_handle* h, const char* path) {
+    return guard(h, [&] {
+        const auto kind = static_cast<hm::Engine::Kind>(hm::Engine::file_kind(path));
+        engine(h, kind).load(path);
+        HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
 int hm_num_nodes(const hm_handle* h) {
     if (!h || !h->eng) return 0;
     return (int)h->eng->nodes().size();

@@ -107,6 +107,11 @@ class Engine {
     void gradients(const double* dx, int ldx, const double* dl, int ldl, int s, double* dparams);
     void get_gradient(int node, int which, double* out, int* rows, int* cols) const;
 
+    // serialized operators (hm_io.cu): the built operator to / from one file
+    void save(const char* path) const;
+    void load(const char* path);
+    static int file_kind(const char* path);   // HODLR or HSS, after checking the header
+
     // introspection
     void export_tree(int* start, int* end, int* is_leaf, int* depth, int* r12, int* r21) const;
     void get_factor(int node, int which, double* out, int* rows, int* cols) const;

@@ -108,6 +108,8 @@ def load() -> C.CDLL:
     for f in ("hm_profile_report", "hm_profile_sequence"):
         getattr(L, f).argtypes = [C.c_char_p, C.c_size_t]
         getattr(L, f).restype = C.c_size_t
+    L.hm_save.argtypes = [C.c_void_p, C.c_char_p]
+    L.hm_load.argtypes = [C.c_void_p, C.c_char_p]
     L.hm_tile_table_load.argtypes = [C.c_char_p]
     L.hm_tile_table_size.argtypes = []
     _lib = L
@@ -309,6 +311,10 @@ class _Handle:
             self._check(self._L.hm_get_gradient(self._h, node, which, _d(out), C.byref(r), C.byref(c)))
         return out.reshape(c.value, r.value).T.copy()
 
+    def save(self, path: str) -> None:
+        """Write the built operator to `path` (hm_save)."""
+        self._check(self._L.hm_save(self._h, str(path).encode()))
+
     def num_nodes(self) -> int:
         return self._L.hm_num_nodes(self._h)
 
@@ -403,6 +409,21 @@ class HSSMatrix(_Handle):
 
     _kernel_build = "hm_hss_build_from_kernel"
     build_from_kernel = HODLRMatrix.build_from_kernel
+
+
+def load_operator(path: str, tol: float = 1e-10, **kw):
+    """Read an operator written by save() into a new HODLRMatrix or HSSMatrix (the kind
+    stored in the file); tol/kw are the handle's options (precision, refinement...)."""
+    import struct
+    with open(path, "rb") as f:
+        head = f.read(16)
+    if len(head) < 16 or head[:8] != b"HMATB200":
+        raise HmError(HM_ERR_ARG, f"{path}: not an hmat_b200 operator file")
+    kind = struct.unpack("<I", head[12:16])[0]
+    m = (HSSMatrix if kind == 1 else HODLRMatrix)(tol, **kw)
+    m._check(m._L.hm_load(m._h, str(path).encode()))
+    m.N = int(m.tree()["end"].max())
+    return m
 
 
 class HODLRBatch(_Handle):

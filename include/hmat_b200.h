@@ -132,6 +132,19 @@ HM_API int hm_hss_build_from_dense(hm_handle* h, const double* A, int N, int lda
 HM_API int hm_hss_build_from_kernel(hm_handle* h, int kernel, const double* points, int dim, int N,
                                     const double* params, int nparams, int leaf_size);
 
+/* ---- serialized operators (no counterpart in the reference, which has no format) ----
+ * hm_save writes the built operator (tree, leaf blocks, bases, coupling blocks; for HSS
+ * also the reference-form leaf bases and B that hm_get_factor exports; for kernel builds
+ * the kernel, its parameters and points) to one binary file; hm_load replaces the
+ * handle's operator with the file's (HODLR or HSS as saved), ready to multiply, factor and
+ * solve without recompressing.  Factorizations are not stored (the first solve factors).
+ * The handle's options (precision, refinement) apply to the loaded operator.  Errors:
+ * HM_ERR_STATE (save before build), HM_ERR_UNSUPPORTED (batches), HM_ERR_ARG (unreadable,
+ * truncated or inconsistent file; a load that fails after the header leaves the handle
+ * with no operator). */
+HM_API int hm_save(hm_handle* h, const char* path);
+HM_API int hm_load(hm_handle* h, const char* path);
+
 /* Upload a HODLR tree built elsewhere (e.g. by HODLRMatrix::build_from_dense) so the
  * device path can multiply/solve with exactly those factors.  Nodes in pre-order
  * (root, left subtree, right subtree); per node pointers to host column-major
