@@ -241,6 +241,13 @@ int hm_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ld
     });
 }
 
+int hm_factor_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ldx, hm_solve_stats* st) {
+    return guard(h, [&] {
+        built(h).factor_solve(b, nrhs, ldb, x, ldx, st);
+        HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
 int hm_solve_exact_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx, double tol,
                           int max_iter, hm_solve_stats* st) {
     return guard(h, [&] { built(h).solve_exact_device(db, nrhs, ldb, dx, ldx, tol, max_iter, st); });

@@ -1813,6 +1813,42 @@ void Engine::solve_exact_device(const double* db, int s, int ldb, double* dx, in
     }
 }
 
+// The reference's solve(b) (factor and solve in one call): a host b is staged to the
+// device on a copy stream while the factorization runs on the handle's stream.
+void Engine::factor_solve(const double* b, int s, int ldb, double* x, int ldx, hm_solve_stats* st) {
+    HM_CHECK(built_, HM_ERR_STATE, "solve before build");
+    HM_CHECK(s >= 1 && ldb >= N_ && ldx >= N_ && b && x, HM_ERR_ARG, "solve: bad arguments");
+    cudaPointerAttributes pa{};
+    HM_CUDA(cudaPointerGetAttributes(&pa, b));
+    const bool host = pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged;
+    if (!host) {
+        factor();
+        solve_device(b, s, ldb, x, ldx, st);
+        return;
+    }
+    const size_t n = (size_t)N_ * s;
+    if (fsB_.n < n) fsB_.alloc(n);
+    if (!copy_stream_) {
+        cudaStream_t cs = nullptr;
+        HM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        copy_stream_.reset(cs, [](cudaStream_t q) { cudaStreamDestroy(q); });
+        cudaEvent_t e = nullptr;
+        HM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        copy_done_.reset(e, [](cudaEvent_t v) { cudaEventDestroy(v); });
+    }
+    HM_CUDA(cudaMemcpy2DAsync(fsB_.p, (size_t)N_ * sizeof(double), b, (size_t)ldb * sizeof(double),
+                              (size_t)N_ * sizeof(double), s, cudaMemcpyHostToDevice, copy_stream_.get()));
+    HM_CUDA(cudaEventRecord(copy_done_.get(), copy_stream_.get()));
+    try {
+        factor();
+    } catch (...) {
+        cudaEventSynchronize(copy_done_.get());   // fsB_ stays in use until the copy lands
+        throw;
+    }
+    HM_CUDA(cudaStreamWaitEvent(stream_, copy_done_.get(), 0));
+    solve_device(fsB_.p, s, N_, x, ldx, st);
+}
+
 void Engine::solve_device(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st) {
     HM_CHECK(built_, HM_ERR_STATE, "solve before build");
     HM_CHECK(s >= 1 && ldb >= N_ && ldx >= N_ && db && dx, HM_ERR_ARG, "solve: bad arguments");

@@ -99,6 +99,8 @@ class Engine {
     void multiply_device(const double* dx, int s, int ldx, double* dy, int ldy);
     void factor();
     void solve_device(const double* db, int s, int ldb, double* dx, int ldx, hm_solve_stats* st);
+    // factor, then solve (host or device b/x); a host b is copied while the factor runs
+    void factor_solve(const double* b, int s, int ldb, double* x, int ldx, hm_solve_stats* st);
     // refinement against the exact kernel operator (matrix-free builds)
     void solve_exact_device(const double* db, int s, int ldb, double* dx, int ldx, double tol, int max_iter,
                             hm_solve_stats* st);
@@ -192,6 +194,10 @@ class Engine {
     int io_cols_ = 0;
     std::map<std::vector<int>, Plan> mv_plans_, solve64_plans_, solve32_plans_;
     std::map<int, Plan> solveT_plans_;
+    // factor_solve: device copy of a host b, and the stream/event that carry it
+    DBuf<double> fsB_;
+    std::shared_ptr<CUstream_st> copy_stream_;
+    std::shared_ptr<CUevent_st> copy_done_;
     // exact-operator refinement: b, x, r, correction (N x ex_cols_), norms, A x plans
     DBuf<double> exB_, exX_, exR_, exD_, exNorm_;
     int ex_cols_ = 0;

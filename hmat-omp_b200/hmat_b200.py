@@ -86,6 +86,7 @@ def load() -> C.CDLL:
     L.hm_multiply_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]
     L.hm_factor.argtypes = [C.c_void_p]
     L.hm_solve.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_int, C.POINTER(SolveStats)]
+    L.hm_factor_solve.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_int, C.POINTER(SolveStats)]
     L.hm_solve_exact.argtypes = [C.c_void_p, _dp, C.c_int, C.c_int, _dp, C.c_int, C.c_double, C.c_int,
                                  C.POINTER(SolveStats)]
     L.hm_solve_exact_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_double,
@@ -270,6 +271,17 @@ class _Handle:
         self._check(self._L.hm_solve_device(self._h, C.c_void_p(db), nrhs, ldb, C.c_void_p(dx), ldx,
                                             C.byref(st)))
         return st
+
+    def factor_solve(self, b: np.ndarray, stats: bool = False):
+        """Factor, then solve (the reference's solve(b)); b's copy overlaps the factor."""
+        b = np.asarray(b, dtype=np.float64)
+        vec = b.ndim == 1
+        B = np.asfortranarray(b.reshape(self.N, -1))
+        X = np.zeros_like(B, order="F")
+        st = SolveStats()
+        self._check(self._L.hm_factor_solve(self._h, _d(B), B.shape[1], self.N, _d(X), self.N, C.byref(st)))
+        out = X.ravel() if vec else X
+        return (out, st) if stats else out
 
     def solve_exact(self, b: np.ndarray, tol: float = 1e-12, max_iter: int = 10, stats: bool = False):
         """Solve with the exact kernel operator (matrix-free builds): refinement whose

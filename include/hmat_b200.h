@@ -196,6 +196,14 @@ HM_API int hm_num_systems(const hm_handle* h);
 HM_API int hm_batch_solve(hm_handle* h, const double* b, const int* nrhs, double* x);
 HM_API int hm_batch_multiply(hm_handle* h, const double* x, const int* nrhs, double* y);
 
+/* HODLRMatrix::solve(b) / HSSMatrix::solve(b) as the reference runs them: factor the
+ * current operator, then solve (hodlr_routines.h:108-110 recomputes everything per call).
+ * Here the factorization is recomputed and kept for later hm_solve calls; when b is in
+ * host memory its copy to the device overlaps the factorization (page-locked b makes the
+ * copy fully asynchronous).  Host or device b/x; synchronises before returning. */
+HM_API int hm_factor_solve(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ldx,
+                           hm_solve_stats* stats);
+
 /* ---- exact-operator refinement (no counterpart in the reference) ----
  * For operators built by hm_*_build_from_kernel: solve A x = b with A the exact kernel
  * matrix, the compressed factorization serving as the preconditioner of an iterative
