@@ -1701,13 +1701,26 @@ void Engine::solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, 
     count_launch();
     Plan& sp = solve_plan<float>(f32_, uniform(s));
     Plan& mp = matvec_plan(uniform(s));
+    // x into page-locked host memory: each sweep's x is copied out on the copy stream while
+    // the residual of that x is computed; the copy of the sweep that converges is the answer
+    cudaPointerAttributes pa{};
+    HM_CUDA(cudaPointerGetAttributes(&pa, dx));
+    const bool spec_out = pa.type == cudaMemoryTypeHost;
+    if (spec_out) ensure_copy_stream();
     std::vector<double> hn(2 * (size_t)s);
     double worst = 0.0;
     int it = 0;
     for (; it < std::max(1, opts_.ir_max_iter); ++it) {
         sp.run(q, dstatus.p);                                   // ioYf = A32^{-1} r
+        if (spec_out && it > 0) HM_CUDA(cudaStreamWaitEvent(q, copy_done_.get(), 0));   // previous copy read x
         accumulate_kernel<<<grid_for((size_t)N_ * s), 256, 0, q>>>(ioX.p, ioYf.p, (size_t)N_ * s, it == 0);
         count_launch();
+        if (spec_out) {
+            HM_CUDA(cudaEventRecord(x_ready_.get(), q));
+            HM_CUDA(cudaStreamWaitEvent(copy_stream_.get(), x_ready_.get(), 0));
+            copy_out(dx, ldx, ioX.p, N_, s, copy_stream_.get());
+            HM_CUDA(cudaEventRecord(copy_done_.get(), copy_stream_.get()));
+        }
         mp.run(q, dstatus.p);                                   // ioY = A64 x
         HM_CUDA(cudaMemsetAsync(ioNorm.p, 0, 2 * (size_t)s * sizeof(double), q));
         residual_kernel<<<dim3(std::min(64, ceil_div(N_, 256)), s), 256, 0, q>>>(
@@ -1724,7 +1737,8 @@ void Engine::solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, 
         if (!(worst == worst)) break;  // NaN
         if (worst <= opts_.ir_tol) { ++it; break; }
     }
-    copy_out(dx, ldx, ioX.p, N_, s, q);
+    if (spec_out) HM_CUDA(cudaStreamSynchronize(copy_stream_.get()));
+    else copy_out(dx, ldx, ioX.p, N_, s, q);
     HM_CUDA(cudaStreamSynchronize(q));
     if (st) {
         st->ir_iters = it;
@@ -1813,6 +1827,18 @@ void Engine::solve_exact_device(const double* db, int s, int ldb, double* dx, in
     }
 }
 
+void Engine::ensure_copy_stream() {
+    if (copy_stream_) return;
+    cudaStream_t cs = nullptr;
+    HM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    copy_stream_.reset(cs, [](cudaStream_t q) { cudaStreamDestroy(q); });
+    cudaEvent_t e = nullptr, r = nullptr;
+    HM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    copy_done_.reset(e, [](cudaEvent_t v) { cudaEventDestroy(v); });
+    HM_CUDA(cudaEventCreateWithFlags(&r, cudaEventDisableTiming));
+    x_ready_.reset(r, [](cudaEvent_t v) { cudaEventDestroy(v); });
+}
+
 // The reference's solve(b) (factor and solve in one call): a host b is staged to the
 // device on a copy stream while the factorization runs on the handle's stream.
 void Engine::factor_solve(const double* b, int s, int ldb, double* x, int ldx, hm_solve_stats* st) {
@@ -1828,14 +1854,7 @@ void Engine::factor_solve(const double* b, int s, int ldb, double* x, int ldx, h
     }
     const size_t n = (size_t)N_ * s;
     if (fsB_.n < n) fsB_.alloc(n);
-    if (!copy_stream_) {
-        cudaStream_t cs = nullptr;
-        HM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-        copy_stream_.reset(cs, [](cudaStream_t q) { cudaStreamDestroy(q); });
-        cudaEvent_t e = nullptr;
-        HM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        copy_done_.reset(e, [](cudaEvent_t v) { cudaEventDestroy(v); });
-    }
+    ensure_copy_stream();
     HM_CUDA(cudaMemcpy2DAsync(fsB_.p, (size_t)N_ * sizeof(double), b, (size_t)ldb * sizeof(double),
                               (size_t)N_ * sizeof(double), s, cudaMemcpyHostToDevice, copy_stream_.get()));
     HM_CUDA(cudaEventRecord(copy_done_.get(), copy_stream_.get()));

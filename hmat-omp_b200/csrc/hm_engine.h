@@ -197,7 +197,8 @@ class Engine {
     // factor_solve: device copy of a host b, and the stream/event that carry it
     DBuf<double> fsB_;
     std::shared_ptr<CUstream_st> copy_stream_;
-    std::shared_ptr<CUevent_st> copy_done_;
+    std::shared_ptr<CUevent_st> copy_done_, x_ready_;
+    void ensure_copy_stream();
     // exact-operator refinement: b, x, r, correction (N x ex_cols_), norms, A x plans
     DBuf<double> exB_, exX_, exR_, exD_, exNorm_;
     int ex_cols_ = 0;
