@@ -583,6 +583,24 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         }
         if (!any_scale) pipe_bn_ = nmax <= 32 ? 32 : nmax <= 64 ? 64 : nmax <= 96 ? 96 : 128;
     }
+    // generated-operand batches (matrix-free sketches: n = sketch width, ~100): 128-wide
+    // tiles so each generated entry of A feeds the whole width once
+    gen_wide_ = false;
+    if (gen_ != GEN_DENSE && cfg_ == CFG_64x64 && !h_.empty()) {
+        int nmax = 0;
+        for (auto& d : h_) nmax = std::max(nmax, d.n);
+        if (nmax > 64) {
+            gen_wide_ = true;
+            int tt = 0;
+            for (auto& d : h_) {
+                d.tiles_m = ceil_div(d.m, 64);
+                d.tiles_n = ceil_div(d.n, 128);
+                d.tile0 = tt;
+                tt += d.tiles_m * d.tiles_n * d.ksplit;
+            }
+            total_tiles_ = tt;
+        }
+    }
     TileChoice tuned;
     const bool have_tuned = pipe_bn_ && tile_choice(sig_, tuned);
     if (have_tuned) pipe_bn_ = tuned.bn;
@@ -747,6 +765,8 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) cons
     else if (pipe_bn_ == 64) tile::launch<T, 64>(pipe_tiles_, s, d_.p, tmap_.p);
     else if (pipe_bn_ == 96) tile::launch<T, 96>(pipe_tiles_, s, d_.p, tmap_.p);
     else if (pipe_bn_ == 128) tile::launch<T, 128>(pipe_tiles_, s, d_.p, tmap_.p);
+    else if (gen_wide_)
+        launch_gen<T, 64, 128, 8, 4, 8>(gen_, total_tiles_, s, d_.p, (int)h_.size(), gp);
     else if (cfg_ == CFG_N_SKINNY)
         launch_gen<T, 128, 16, 16, 4, 2>(gen_, total_tiles_, s, d_.p, (int)h_.size(), gp);
     else

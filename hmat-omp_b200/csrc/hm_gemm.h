@@ -154,6 +154,7 @@ class GemmBatch {
     double flops_ = 0, bytes_ = 0;
     int pipe_bn_ = 0, pipe_tiles_ = 0;   // warp-tiled dense kernel: tile width and tile count
     bool pipe_small_ = false;            // its 64-row tile shapes
+    bool gen_wide_ = false;              // generated-A batch on 64 x 128 tiles
     DBuf<int> tmap_;                     // its tile -> problem table
     // FP32 batches with long k on the tensor cores: tile count, tables, tensor maps
     bool use_tc_ = false, tc_allowed_ = true;
