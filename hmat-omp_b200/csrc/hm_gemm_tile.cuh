@@ -298,200 +298,6 @@ gemm_tile_kernel(const GemmDesc<T>* __restrict__ descs, const int* __restrict__ 
     }
 }
 
-// ---------------------------------------------------------------------------------
-// The same warp tiling fed by an ST-stage cp.async pipeline instead of register staging:
-// 16-byte copies along the contiguous rows of an operand (MN-contiguous), element copies
-// into the transposed positions of a k-contiguous one, zero fill past the edges; ST - 1
-// k-tiles in flight while one is multiplied, no staging registers.
-// ---------------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void cpa16(T* s, const T* g) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(s)), "l"(g)
-                 : "memory");
-}
-template <typename T>
-__device__ __forceinline__ void cpa_el(T* s, const T* g, bool valid) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
-    if constexpr (sizeof(T) == 4)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(g), "r"(valid ? 4 : 0) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(g), "r"(valid ? 8 : 0) : "memory");
-}
-__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// k-tile [k0, k0 + BK) of BMN rows of op(X) into s ([k][row], row pitch P)
-template <typename T, int BMN, int BK, int NT>
-__device__ __forceinline__ void issue_tile(T* s, int P, const T* __restrict__ X, int ld, bool mn_contig, bool vec_ok,
-                                           int r0, int rmax, int k0, int ke, int tid) {
-    constexpr int VW = 16 / (int)sizeof(T);
-    if (mn_contig) {
-        constexpr int NVEC = BMN * BK / VW;
-#pragma unroll
-        for (int q = 0; q < (NVEC + NT - 1) / NT; ++q) {
-            const int e = tid + NT * q;
-            if (NVEC % NT != 0 && e >= NVEC) continue;
-            const int r = (e % (BMN / VW)) * VW, kk = e / (BMN / VW);
-            const int gr = r0 + r, gk = k0 + kk;
-            T* d = s + kk * P + r;
-            const bool kin = gk < ke;
-            if (vec_ok && kin && gr + VW <= rmax) {
-                cpa16(d, X + gr + (size_t)gk * ld);
-            } else {
-#pragma unroll
-                for (int u = 0; u < VW; ++u) {
-                    const bool v = kin && gr + u < rmax;
-                    cpa_el(d + u, v ? X + gr + u + (size_t)gk * ld : X, v);
-                }
-            }
-        }
-    } else {
-        constexpr int NEL = BMN * BK;
-#pragma unroll
-        for (int q = 0; q < (NEL + NT - 1) / NT; ++q) {
-            const int e = tid + NT * q;
-            if (NEL % NT != 0 && e >= NEL) continue;
-            const int kk = e % BK, r = e / BK;
-            const int gr = r0 + r, gk = k0 + kk;
-            const bool v = gr < rmax && gk < ke;
-            cpa_el(s + kk * P + r, v ? X + gk + (size_t)gr * ld : X, v);
-        }
-    }
-}
-
-template <typename T, class CF, int BKA, int ST>
-struct AsyncShape {
-    static constexpr size_t smem = (size_t)ST * BKA * (CF::PA + CF::PB) * sizeof(T);
-};
-
-template <typename T, class CF, int BK, int ST>
-__global__ void __launch_bounds__(CF::NT, CF::MINB)
-gemm_async_kernel(const GemmDesc<T>* __restrict__ descs, const int* __restrict__ tile_problem) {
-    constexpr int BM = CF::BM, BN = CF::BN, NT = CF::NT;
-    constexpr int PA = CF::PA, PB = CF::PB, UM = CF::UM, UN = CF::UN;
-    constexpr int VW = 16 / (int)sizeof(T);
-    constexpr int NG = 4 / VW;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    T* As = reinterpret_cast<T*>(smraw);   // [ST][BK][PA]
-    T* Bs = As + ST * BK * PA;             // [ST][BK][PB]
-
-    const int tile = blockIdx.x;
-    const GemmDesc<T>& D = descs[tile_problem[tile]];
-    const int m = D.m, n = D.n, k = D.k, lda = D.lda, ldb = D.ldb;
-    const T* __restrict__ A = D.A;
-    const T* __restrict__ B = D.B;
-    int t = tile - D.tile0;
-    const int tm = t % D.tiles_m;
-    t /= D.tiles_m;
-    const int tn = t % D.tiles_n;
-    const int kslice = t / D.tiles_n;
-    const int m0 = tm * BM, n0 = tn * BN;
-    int kper = (k + D.ksplit - 1) / D.ksplit;
-    kper = (kper + BK - 1) / BK * BK;
-    const int kb = kslice * kper;
-    const int ke = min(k, kb + kper);
-    const int nk = ke > kb ? (ke - kb + BK - 1) / BK : 0;
-
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int am = (w % CF::WGM) * 32 * UM + (lane & 7) * VW;
-    const int bn = (w / CF::WGM) * 16 * UN + (lane >> 3) * VW;
-    const bool a_mn = D.opA == OP_N, b_mn = D.opB == OP_T;
-    const bool a_vec = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (lda % VW == 0);
-    const bool b_vec = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (ldb % VW == 0);
-
-    T acc[4 * UM][4 * UN];
-#pragma unroll
-    for (int i = 0; i < 4 * UM; ++i)
-#pragma unroll
-        for (int j = 0; j < 4 * UN; ++j) acc[i][j] = T(0);
-
-#pragma unroll
-    for (int sidx = 0; sidx < ST - 1; ++sidx) {
-        if (sidx < nk) {
-            issue_tile<T, BM, BK, NT>(As + sidx * BK * PA, PA, A, lda, a_mn, a_vec, m0, m, kb + sidx * BK, ke, tid);
-            issue_tile<T, BN, BK, NT>(Bs + sidx * BK * PB, PB, B, ldb, b_mn, b_vec, n0, n, kb + sidx * BK, ke, tid);
-        }
-        cpa_commit();
-    }
-    for (int it = 0; it < nk; ++it) {
-        cpa_wait<ST - 2>();
-        __syncthreads();
-        const int nxt = it + ST - 1;
-        if (nxt < nk) {
-            const int bsl = nxt % ST;
-            issue_tile<T, BM, BK, NT>(As + bsl * BK * PA, PA, A, lda, a_mn, a_vec, m0, m, kb + nxt * BK, ke, tid);
-            issue_tile<T, BN, BK, NT>(Bs + bsl * BK * PB, PB, B, ldb, b_mn, b_vec, n0, n, kb + nxt * BK, ke, tid);
-        }
-        cpa_commit();
-        const int buf = it % ST;
-        const T* as = As + buf * BK * PA + am;
-        const T* bs = Bs + buf * BK * PB + bn;
-#pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            T a[4 * UM], b[4 * UN];
-#pragma unroll
-            for (int u = 0; u < UM; ++u)
-#pragma unroll
-                for (int g = 0; g < NG; ++g) ld16(as + kk * PA + 32 * u + g * 8 * VW, a + 4 * u + g * VW);
-#pragma unroll
-            for (int v = 0; v < UN; ++v)
-#pragma unroll
-                for (int g = 0; g < NG; ++g) ld16(bs + kk * PB + 16 * v + g * 4 * VW, b + 4 * v + g * VW);
-#pragma unroll
-            for (int i = 0; i < 4 * UM; ++i)
-#pragma unroll
-                for (int j = 0; j < 4 * UN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-    }
-    cpa_wait<0>();
-
-    T* __restrict__ C = D.C;
-    const int ldc = D.ldc;
-    const T alpha = D.alpha, beta = D.beta;
-    const bool split = D.ksplit > 1;
-    const bool c_vec = ((reinterpret_cast<uintptr_t>(C) & 15) == 0) && (ldc % VW == 0);
-#pragma unroll
-    for (int u = 0; u < UM; ++u) {
-#pragma unroll
-        for (int gu = 0; gu < NG; ++gu) {
-            const int gi = m0 + am + 32 * u + gu * 8 * VW;
-            if (gi >= m) continue;
-#pragma unroll
-            for (int v = 0; v < UN; ++v) {
-#pragma unroll
-                for (int jj = 0; jj < 4; ++jj) {
-                    const int gj = n0 + bn + 16 * v + (jj / VW) * 4 * VW + (jj % VW);
-                    if (gj >= n) continue;
-                    T* c = C + gi + (size_t)gj * ldc;
-                    T val[VW];
-#pragma unroll
-                    for (int r = 0; r < VW; ++r) val[r] = alpha * acc[4 * u + gu * VW + r][4 * v + jj];
-                    if (split) {
-#pragma unroll
-                        for (int r = 0; r < VW; ++r)
-                            if (gi + r < m) atomicAdd(c + r, val[r]);
-                    } else if (c_vec && gi + VW <= m) {
-                        if (beta != T(0)) {
-                            T old[VW];
-                            ld16(c, old);
-#pragma unroll
-                            for (int r = 0; r < VW; ++r) val[r] = fma(beta, old[r], val[r]);
-                        }
-                        st16(c, val);
-                    } else {
-#pragma unroll
-                        for (int r = 0; r < VW; ++r) {
-                            if (gi + r >= m) continue;
-                            c[r] = (beta == T(0)) ? val[r] : fma(beta, c[r], val[r]);
-                        }
-                    }
-                }
-            }
-        }
-    }
-}
-
 template <typename T, int BN, bool SMALL = false>
 void launch(int tiles, cudaStream_t s, const GemmDesc<T>* d, const int* tile_problem) {
     using CF = typename For<T, BN, SMALL>::C;
