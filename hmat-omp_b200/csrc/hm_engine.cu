@@ -1511,17 +1511,14 @@ static void add_matvec(Plan& pl, const std::vector<Node>& nodes, const std::vect
                        const std::vector<std::vector<int>>& levels, const double* dD, const double* dU,
                        const double* dV, const double* dB, const double* X, double* Y, int N,
                        const std::vector<int>& sc, cudaStream_t st) {
-    auto gLeaf = std::make_unique<GemmStep<double>>("matvec.leaf");
-    for (int l : leaves) {
-        const Node& n = nodes[l];
-        const int s = sc[n.sys];
-        gLeaf->batch.add(n.len(), s, n.len(), 1.0, dD + n.offD, n.len(), OP_N, X + n.start, N, OP_N,
-                         0.0, Y + n.start, N);
-    }
+    // Projections and couplings of every level first (independent of y):
+    //   t = [V1^T x1; V2^T x2],  delta = [B12 t2; B21 t1]  per internal node;
+    // then one launch per leaf row block accumulates y = D x + sum over the leaf's path of
+    // U_c delta_c in registers (a chain of GEMM problems) and writes y once.
     auto gT = std::make_unique<GemmStep<double>>("matvec.project");
     auto gD = std::make_unique<GemmStep<double>>("matvec.couple");
-    std::vector<std::unique_ptr<GemmStep<double>>> gE(levels.size());
-    for (size_t d = 0; d < levels.size(); ++d) gE[d] = std::make_unique<GemmStep<double>>("matvec.expand");
+    std::vector<const double*> delta(nodes.size(), nullptr);   // delta_c of child c
+    std::vector<int> ldd(nodes.size(), 0);
     for (size_t d = 0; d < levels.size(); ++d) {
         for (int id : levels[d]) {
             const Node& n = nodes[id];
@@ -1539,23 +1536,31 @@ static void add_matvec(Plan& pl, const std::vector<Node>& nodes, const std::vect
             // delta1 = B12 T2, delta2 = B21 T1
             gD->batch.add(p1, s, q2, 1.0, dB + n.offB12, p1, OP_N, T + q1, q1 + q2, OP_N, 0.0, Dl, p1 + p2);
             gD->batch.add(p2, s, q1, 1.0, dB + n.offB21, p2, OP_N, T, q1 + q2, OP_N, 0.0, Dl + p1, p1 + p2);
-            // y1 += U1 delta1, y2 += U2 delta2
-            gE[d]->batch.add(L.len(), s, p1, 1.0, dU + L.offU, L.len(), OP_N, Dl, p1 + p2, OP_N, 1.0,
-                             Y + L.start, N);
-            gE[d]->batch.add(R.len(), s, p2, 1.0, dU + R.offU, R.len(), OP_N, Dl + p1, p1 + p2, OP_N, 1.0,
-                             Y + R.start, N);
+            delta[n.left] = Dl;
+            delta[n.right] = Dl + p1;
+            ldd[n.left] = ldd[n.right] = p1 + p2;
         }
     }
-    gLeaf->batch.finalize(st);
-    pl.add(std::move(gLeaf));
+    auto gY = std::make_unique<GemmStep<double>>("matvec.leaf_expand");
+    for (int l : leaves) {
+        const Node& n = nodes[l];
+        const int s = sc[n.sys];
+        if (s == 0) continue;
+        gY->batch.add(n.len(), s, n.len(), 1.0, dD + n.offD, n.len(), OP_N, X + n.start, N, OP_N, 0.0, Y + n.start,
+                      N, nullptr, 1);
+        for (int c = l; nodes[c].parent >= 0; c = nodes[c].parent) {
+            const Node& C = nodes[c];
+            if (C.rankU == 0 || !delta[c]) continue;
+            gY->batch.add_chained(n.len(), s, C.rankU, 1.0, dU + C.offU + (n.start - C.start), C.len(), OP_N,
+                                  delta[c], ldd[c], OP_N);
+        }
+    }
     gT->batch.finalize(st);
     pl.add(std::move(gT));
     gD->batch.finalize(st);
     pl.add(std::move(gD));
-    for (auto& g : gE) {
-        g->batch.finalize(st);
-        pl.add(std::move(g));
-    }
+    gY->batch.finalize(st);
+    pl.add(std::move(gY));
 }
 
 Plan& Engine::matvec_plan(const std::vector<int>& sc) {

@@ -365,6 +365,8 @@ void GemmBatch<T>::add(int m, int n, int k, T alpha, const T* A, int lda, int op
     d.tiles_m = ceil_div(m, cs.BM);
     d.tiles_n = ceil_div(n, cs.BN);
     d.ga_r0 = ga_r0; d.ga_c0 = ga_c0;
+    d.next = -1;
+    d.is_link = 0;
     if (ksplit <= 0) {
         int tiles = d.tiles_m * d.tiles_n;
         ksplit = 1;
@@ -381,6 +383,27 @@ void GemmBatch<T>::add(int m, int n, int k, T alpha, const T* A, int lda, int op
         d.ksplit = 1;
     }
     h_.push_back(d);
+    chain_head_ = chain_tail_ = (int)h_.size() - 1;
+}
+
+template <typename T>
+void GemmBatch<T>::add_chained(int m, int n, int k, T alpha, const T* A, int lda, int opA, const T* B, int ldb,
+                               int opB) {
+    HM_CHECK(!finalized_, HM_ERR_STATE, "GemmBatch::add_chained after finalize");
+    HM_CHECK(chain_head_ >= 0 && gen_ == GEN_DENSE, HM_ERR_STATE, "add_chained: no dense head problem");
+    const GemmDesc<T>& hd = h_[chain_head_];
+    HM_CHECK(hd.m == m && hd.n == n && hd.alpha == alpha && hd.ksplit == 1 && hd.kscale == nullptr, HM_ERR_ARG,
+             "add_chained: the link must match its head (m, n, alpha; head ksplit 1, no kscale)");
+    if (k <= 0) return;
+    GemmDesc<T> d = hd;
+    d.A = A; d.B = B; d.lda = lda; d.ldb = ldb; d.opA = opA; d.opB = opB; d.k = k;
+    d.tiles_m = d.tiles_n = 0;
+    d.next = -1;
+    d.is_link = 1;
+    h_.push_back(d);
+    h_[chain_tail_].next = (int)h_.size() - 1;
+    chain_tail_ = (int)h_.size() - 1;
+    has_chains_ = true;
 }
 
 // ---------------------------------------------------------------------------------
@@ -619,8 +642,8 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         std::vector<GemmDesc<T>> dv(h_);
         int tt = 0;
         for (auto& d : dv) {
-            d.tiles_m = ceil_div(d.m, BM);
-            d.tiles_n = ceil_div(d.n, pipe_bn_);
+            d.tiles_m = d.is_link ? 0 : ceil_div(d.m, BM);
+            d.tiles_n = d.is_link ? 0 : ceil_div(d.n, pipe_bn_);
             d.tile0 = tt;
             tt += d.tiles_m * d.tiles_n * d.ksplit;
         }
@@ -637,13 +660,14 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
             HM_CUDA(cudaMemcpyAsync(tmap_.p, tp.data(), tp.size() * sizeof(int), cudaMemcpyHostToDevice, s));
         HM_CUDA(cudaStreamSynchronize(s));  // dv and tp are local vectors
     } else if (!h_.empty()) {
+        HM_CHECK(!has_chains_, HM_ERR_STATE, "chained GEMM problems need the warp-tiled kernel");
         d_.alloc(h_.size());
         HM_CUDA(cudaMemcpyAsync(d_.p, h_.data(), h_.size() * sizeof(GemmDesc<T>),
                                 cudaMemcpyHostToDevice, s));
     }
     use_tc_ = false;
     if constexpr (std::is_same<T, float>::value) {
-        if (pipe_bn_ && tc_allowed_ && (!have_tuned || tuned.tc)) finalize_tc(s);
+        if (pipe_bn_ && tc_allowed_ && !has_chains_ && (!have_tuned || tuned.tc)) finalize_tc(s);
     }
     if (!hz_.empty()) {
         dz_.alloc(hz_.size());
@@ -755,6 +779,22 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) cons
             HM_CUDA(cudaGetLastError());
             return;
         }
+    }
+    if (has_chains_) {   // chained batches (the FP64 matvec's leaf + expansion)
+        if constexpr (std::is_same<T, double>::value) {
+            if (pipe_small_) {
+                if (pipe_bn_ == 32) tile::launch<T, 32, true, true>(pipe_tiles_, s, d_.p, tmap_.p);
+                else if (pipe_bn_ == 64) tile::launch<T, 64, true, true>(pipe_tiles_, s, d_.p, tmap_.p);
+                else if (pipe_bn_ == 96) tile::launch<T, 96, true, true>(pipe_tiles_, s, d_.p, tmap_.p);
+                else tile::launch<T, 128, true, true>(pipe_tiles_, s, d_.p, tmap_.p);
+            } else if (pipe_bn_ == 32) tile::launch<T, 32, false, true>(pipe_tiles_, s, d_.p, tmap_.p);
+            else if (pipe_bn_ == 64) tile::launch<T, 64, false, true>(pipe_tiles_, s, d_.p, tmap_.p);
+            else if (pipe_bn_ == 96) tile::launch<T, 96, false, true>(pipe_tiles_, s, d_.p, tmap_.p);
+            else tile::launch<T, 128, false, true>(pipe_tiles_, s, d_.p, tmap_.p);
+            HM_CUDA(cudaGetLastError());
+            return;
+        }
+        throw Error(HM_ERR_UNSUPPORTED, "chained GEMM problems are FP64 only");
     }
     if (pipe_small_) {
         if (pipe_bn_ == 32) tile::launch<T, 32, true>(pipe_tiles_, s, d_.p, tmap_.p);

@@ -53,6 +53,11 @@ struct GemmDesc {
     int tiles_m, tiles_n;
     int tile0;         // first global tile index of this problem
     int ga_r0, ga_c0;  // generated A: origin of the block in the global operator
+    // Chains (warp-tiled dense kernel only): a problem with next >= 0 is followed, in the
+    // same CTA and register accumulators, by problem `next` (same m and n; its product is
+    // added before the head's epilogue writes C).  Linked problems own no tiles.
+    int next;
+    int is_link;
 };
 
 // Materialise a block of a generated operator: dst(i,j) = trans ? G(r0+j, c0+i) : G(r0+i, c0+j)
@@ -102,6 +107,9 @@ class GemmBatch {
     void add(int m, int n, int k, T alpha, const T* A, int lda, int opA, const T* B, int ldb,
              int opB, T beta, T* C, int ldc, const T* kscale = nullptr, int ksplit = 0,
              int ga_r0 = 0, int ga_c0 = 0);
+    // Add op(A) op(B) (m x n, same alpha) to the C tile of the last problem added with
+    // add() (ksplit 1): the whole chain is accumulated in registers and C is written once.
+    void add_chained(int m, int n, int k, T alpha, const T* A, int lda, int opA, const T* B, int ldb, int opB);
     bool empty() const { return h_.empty(); }
     size_t size() const { return h_.size(); }
     // step name used in the tuning signature
@@ -145,6 +153,8 @@ class GemmBatch {
     int cfg_, gen_;
     std::string tag_, sig_;
     std::vector<GemmDesc<T>> h_;
+    int chain_head_ = -1, chain_tail_ = -1;
+    bool has_chains_ = false;
     DBuf<GemmDesc<T>> d_;
     // regions to zero before a split-K launch
     std::vector<ZeroRegion<T>> hz_;

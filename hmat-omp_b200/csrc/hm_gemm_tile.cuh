@@ -144,8 +144,69 @@ struct Stage {
     }
 };
 
+// The main loop of gemm_tile_kernel for one chained problem (whole k), accumulating
+// into the caller's registers: only the chain instantiation uses it.
 template <typename T, class CF>
-__global__ void __launch_bounds__(CF::NT, CF::MINB)
+__device__ __forceinline__ void chain_mainloop(const GemmDesc<T>& P, int m, int n, int m0, int n0, int am, int bn,
+                                               T* As, T* Bs, T (&acc)[4 * CF::UM][4 * CF::UN]) {
+    constexpr int BK = CF::BK, NT = CF::NT, PA = CF::PA, PB = CF::PB, UM = CF::UM, UN = CF::UN;
+    constexpr int VW = 16 / (int)sizeof(T);
+    constexpr int NG = 4 / VW;
+    const int tid = threadIdx.x;
+    const int k = P.k, lda = P.lda, ldb = P.ldb;
+    const T* __restrict__ A = P.A;
+    const T* __restrict__ B = P.B;
+    const bool a_mn = P.opA == OP_N, b_mn = P.opB == OP_T;
+    const bool a_vec = ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && (lda % VW == 0);
+    const bool b_vec = ((reinterpret_cast<uintptr_t>(B) & 15) == 0) && (ldb % VW == 0);
+    const int nk = (k + BK - 1) / BK;
+    if (nk <= 0) return;
+    Stage<T, CF::BM, BK, NT> sa;
+    Stage<T, CF::BN, BK, NT> sb;
+    sa.load(A, lda, a_mn, a_vec, m0, m, 0, k, tid);
+    sb.load(B, ldb, b_mn, b_vec, n0, n, 0, k, tid);
+    sa.store(As, PA, a_mn, tid);
+    sb.store(Bs, PB, b_mn, tid);
+    __syncthreads();
+    for (int it = 0; it < nk; ++it) {
+        const int buf = it & 1;
+        const bool more = it + 1 < nk;
+        if (more) {
+            const int k1 = (it + 1) * BK;
+            sa.load(A, lda, a_mn, a_vec, m0, m, k1, k, tid);
+            sb.load(B, ldb, b_mn, b_vec, n0, n, k1, k, tid);
+        }
+        const T* as = As + buf * BK * PA + am;
+        const T* bs = Bs + buf * BK * PB + bn;
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            T a[4 * UM], b[4 * UN];
+#pragma unroll
+            for (int u = 0; u < UM; ++u)
+#pragma unroll
+                for (int g = 0; g < NG; ++g) ld16(as + kk * PA + 32 * u + g * 8 * VW, a + 4 * u + g * VW);
+#pragma unroll
+            for (int v = 0; v < UN; ++v)
+#pragma unroll
+                for (int g = 0; g < NG; ++g) ld16(bs + kk * PB + 16 * v + g * 4 * VW, b + 4 * v + g * VW);
+#pragma unroll
+            for (int i = 0; i < 4 * UM; ++i)
+#pragma unroll
+                for (int j = 0; j < 4 * UN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        if (more) {
+            sa.store(As + (buf ^ 1) * BK * PA, PA, a_mn, tid);
+            sb.store(Bs + (buf ^ 1) * BK * PB, PB, b_mn, tid);
+        }
+        __syncthreads();
+    }
+}
+
+// CHAIN: after the head problem, follow GemmDesc::next (problems accumulated into the
+// head's tile; one CTA per SM of register budget, so the chain's extra state does not
+// spill); the plain instantiation is the single-problem kernel.
+template <typename T, class CF, bool CHAIN = false>
+__global__ void __launch_bounds__(CF::NT, CHAIN ? 1 : CF::MINB)
 gemm_tile_kernel(const GemmDesc<T>* __restrict__ descs, const int* __restrict__ tile_problem) {
     constexpr int BM = CF::BM, BN = CF::BN, BK = CF::BK, NT = CF::NT;
     constexpr int PA = CF::PA, PB = CF::PB, UM = CF::UM, UN = CF::UN;
@@ -252,6 +313,11 @@ gemm_tile_kernel(const GemmDesc<T>* __restrict__ descs, const int* __restrict__ 
         }
     }
 
+    if constexpr (CHAIN) {
+        for (int nx = D.next; nx >= 0; nx = descs[nx].next)
+            chain_mainloop<T, CF>(descs[nx], m, n, m0, n0, am, bn, As, Bs, acc);
+    }
+
     T* __restrict__ C = D.C;
     const int ldc = D.ldc;
     const T alpha = D.alpha, beta = D.beta;
@@ -298,12 +364,12 @@ gemm_tile_kernel(const GemmDesc<T>* __restrict__ descs, const int* __restrict__ 
     }
 }
 
-template <typename T, int BN, bool SMALL = false>
+template <typename T, int BN, bool SMALL = false, bool CHAIN = false>
 void launch(int tiles, cudaStream_t s, const GemmDesc<T>* d, const int* tile_problem) {
     using CF = typename For<T, BN, SMALL>::C;
     static size_t cur = 0;
-    ensure_dyn_smem(gemm_tile_kernel<T, CF>, CF::smem, cur);
-    gemm_tile_kernel<T, CF><<<tiles, CF::NT, CF::smem, s>>>(d, tile_problem);
+    ensure_dyn_smem(gemm_tile_kernel<T, CF, CHAIN>, CF::smem, cur);
+    gemm_tile_kernel<T, CF, CHAIN><<<tiles, CF::NT, CF::smem, s>>>(d, tile_problem);
 }
 
 }  // namespace tile
