@@ -25,6 +25,25 @@ inline void check(int rc, hm_handle* h) {
     if (rc != HM_OK) throw std::runtime_error(std::string("hmat_b200: ") + hm_last_error(h));
 }
 
+// Download factor `which` of node `node` into M (left untouched when absent).
+inline void get_factor(hm_handle* h, size_t node, int which, Matrix& M, bool present) {
+    if (!present) return;
+    int r = 0, c = 0;
+    check(hm_get_factor(h, (int)node, which, nullptr, &r, &c), h);
+    M = Matrix(r, c);
+    if (r * c) check(hm_get_factor(h, (int)node, which, M.data(), &r, &c), h);
+}
+
+// A fresh handle with the caller's options (tolerance and RSVD rank from the members).
+inline hm_handle* new_handle(hm_opts& opts, double tol, int rsvd_rank, hm_handle* old) {
+    opts.tol = tol;
+    opts.rsvd_rank = rsvd_rank;
+    if (old) hm_destroy(old);
+    hm_handle* h = nullptr;
+    if (hm_create(&opts, &h) != HM_OK) throw std::runtime_error("hmat_b200: hm_create failed (no GPU?)");
+    return h;
+}
+
 }  // namespace hmat_b200_detail
 
 class HODLRMatrixCUDA {
@@ -85,21 +104,9 @@ public:
 private:
     hm_handle* h_;
 
-    void ensure_handle() {
-        opts.tol = tolerance;
-        opts.rsvd_rank = rsvd_rank;
-        if (h_) hm_destroy(h_);
-        h_ = nullptr;
-        if (hm_create(&opts, &h_) != HM_OK) throw std::runtime_error("hmat_b200: hm_create failed (no GPU?)");
-    }
+    void ensure_handle() { h_ = hmat_b200_detail::new_handle(opts, tolerance, rsvd_rank, h_); }
 
-    void get(size_t node, int which, Matrix& M, bool present) {
-        if (!present) return;
-        int r = 0, c = 0;
-        hmat_b200_detail::check(hm_get_factor(h_, (int)node, which, nullptr, &r, &c), h_);
-        M = Matrix(r, c);
-        if (r * c) hmat_b200_detail::check(hm_get_factor(h_, (int)node, which, M.data(), &r, &c), h_);
-    }
+    void get(size_t node, int which, Matrix& M, bool present) { hmat_b200_detail::get_factor(h_, node, which, M, present); }
 
     void clear_tree() {
         for (auto* n : nodes) delete n;
@@ -131,6 +138,106 @@ private:
         const int r = link(i + 1);
         nodes[i]->right = nodes[r];
         return link(r);
+    }
+};
+
+class HSSMatrixCUDA {
+public:
+    HSSNode* root;
+    std::vector<HSSNode*> nodes;   // build_topo id order (hss_routines.h:293-306)
+    int N;
+    double tolerance;
+    int rsvd_rank;
+    hm_opts opts;                  // extension options (sketch, seed, refinement, ...)
+
+    explicit HSSMatrixCUDA(double tol = 1e-9) : root(nullptr), N(0), tolerance(tol), rsvd_rank(64), h_(nullptr) {
+        hm_opts_default(&opts);
+    }
+    ~HSSMatrixCUDA() {
+        clear_tree();
+        if (h_) hm_destroy(h_);
+    }
+    HSSMatrixCUDA(const HSSMatrixCUDA&) = delete;
+    HSSMatrixCUDA& operator=(const HSSMatrixCUDA&) = delete;
+
+    // hss_routines.h:50
+    void build_from_dense(const Matrix& A, int leaf_size) {
+        h_ = hmat_b200_detail::new_handle(opts, tolerance, rsvd_rank, h_);
+        N = A.rows();
+        hmat_b200_detail::check(hm_hss_build_from_dense(h_, A.data(), N, N, leaf_size), h_);
+        fill_tree();
+    }
+
+    // hss_routines.h:118 (all columns of x)
+    Matrix multiply(const Matrix& x) {
+        Matrix y(N, x.cols());
+        hmat_b200_detail::check(hm_multiply(h_, x.data(), x.cols(), N, y.data(), N), h_);
+        return y;
+    }
+
+    // hss_routines.h:197 (factors once, then solves every column together)
+    Matrix solve(const Matrix& b) {
+        Matrix x(N, b.cols());
+        hmat_b200_detail::check(hm_solve(h_, b.data(), b.cols(), N, x.data(), N, nullptr), h_);
+        return x;
+    }
+
+    // Copy D, U, V (leaves), R, W, B (internal) into the nodes, as HSSMatrix holds them.
+    void download_factors() {
+        for (size_t i = 0; i < nodes.size(); ++i) {
+            HSSNode* n = nodes[i];
+            hmat_b200_detail::get_factor(h_, i, 0, n->D, n->is_leaf);
+            hmat_b200_detail::get_factor(h_, i, 1, n->U, n->is_leaf);
+            hmat_b200_detail::get_factor(h_, i, 2, n->V, n->is_leaf);
+            hmat_b200_detail::get_factor(h_, i, 3, n->R, !n->is_leaf);
+            hmat_b200_detail::get_factor(h_, i, 4, n->W, !n->is_leaf);
+            hmat_b200_detail::get_factor(h_, i, 5, n->B, !n->is_leaf);
+        }
+    }
+
+    hm_handle* handle() { return h_; }
+
+private:
+    hm_handle* h_;
+
+    void clear_tree() {
+        for (auto* n : nodes) delete n;
+        nodes.clear();
+        root = nullptr;
+    }
+
+    void fill_tree() {
+        clear_tree();
+        const int n = hm_num_nodes(h_);
+        std::vector<int> s(n), e(n), leaf(n), depth(n), ru(n), rv(n);
+        hmat_b200_detail::check(
+            hm_export_tree(h_, s.data(), e.data(), leaf.data(), depth.data(), ru.data(), rv.data()), h_);
+        nodes.resize(n);
+        for (int i = 0; i < n; ++i) {
+            nodes[i] = new HSSNode();
+            nodes[i]->id = i;
+            nodes[i]->idx_start = s[i];
+            nodes[i]->idx_end = e[i];
+            nodes[i]->is_leaf = leaf[i] != 0;
+            nodes[i]->rank_U = ru[i];
+            nodes[i]->rank_V = rv[i];
+        }
+        // build_topo numbers both children of a node before descending into the left one
+        int next = 1;
+        if (n) link(0, next);
+        root = n ? nodes[0] : nullptr;
+    }
+
+    void link(int i, int& next) {
+        if (nodes[i]->is_leaf) return;
+        HSSNode* l = nodes[next];
+        HSSNode* r = nodes[next + 1];
+        next += 2;
+        nodes[i]->left = l;
+        nodes[i]->right = r;
+        l->parent = r->parent = nodes[i];
+        link(l->id, next);
+        link(r->id, next);
     }
 };
 

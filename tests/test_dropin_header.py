@@ -13,7 +13,8 @@ def test_dropin_header_compiles(tmp_path):
         pytest.skip("reference headers not present")
     src = tmp_path / "t.cpp"
     src.write_text('#include "hodlr_routines_cuda.h"\n'
-                   'int main(){ HODLRMatrixCUDA m(1e-8); m.rsvd_rank = 16; return m.N; }\n')
+                   'int main(){ HODLRMatrixCUDA m(1e-8); m.rsvd_rank = 16;\n'
+                   '            HSSMatrixCUDA h(1e-9); h.rsvd_rank = 32; return m.N + h.N; }\n')
     r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", REF_INC, "-I", os.path.join(ROOT, "include"),
                         str(src)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

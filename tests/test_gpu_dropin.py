@@ -1,6 +1,6 @@
 """The C++ drop-in (include/hodlr_routines_cuda.h) inside a driver shaped like the
-reference's src/main_hodlr.cpp: HODLRMatrix and HODLRMatrixCUDA on the same operator,
-same sketch seed (oracle/dropin_driver.cpp, built into oracle/_ref by oracle/Makefile)."""
+reference's src/main_hodlr.cpp and src/main_hss.cpp: HODLRMatrix / HSSMatrix and
+HODLRMatrixCUDA / HSSMatrixCUDA on the same operators, same sketch seed (oracle/dropin_driver.cpp, built into oracle/_ref by oracle/Makefile)."""
 import json
 import os
 import subprocess
@@ -23,3 +23,8 @@ def test_dropin_matches_reference_class():
     assert r["root_children_linked"] == 1
     assert r["multiply_rel"] < 1e-10
     assert r["solve_rel"] < 1e-10
+    # HSSMatrix against HSSMatrixCUDA (build_topo ids, ranks, parents, factor shapes)
+    assert r["hss_nodes_ref"] == r["hss_nodes_gpu"]
+    assert r["hss_tree_mismatches"] == 0
+    assert r["hss_multiply_rel"] < 1e-10
+    assert r["hss_solve_rel"] < 1e-10
