@@ -1,7 +1,8 @@
 // Small batched dense kernels for sm_100a: one CTA per problem.
 //
 //  * gj_inverse_kernel  — Gauss-Jordan inversion with partial pivoting, the matrix held
-//                          in registers (n <= GJ_MAX).  Larger inverses are built by
+//                          in registers (n <= GJ_MAX; used up to the threshold of
+//                          plan_inverse).  Larger inverses are built by
 //                          2x2 block elimination over these plus batched GEMMs.
 //  * jacobi_kernel      — cyclic two-sided Jacobi for symmetric positive semi-definite
 //                          Gram matrices, parallel (round-robin) pair ordering, rotation
@@ -607,11 +608,25 @@ void launch_ident(const DevTable<IdentDesc>& t, cudaStream_t s) {
 // ---------------------------------------------------------------------------------
 // Plans
 // ---------------------------------------------------------------------------------
+// Largest order inverted by one Gauss-Jordan kernel; larger ones are split into 2 x 2
+// blocks recursively, moving the work into batched GEMMs.  64 by default (leaf blocks of
+// 256 at N = 2^18: Gauss-Jordan time 3.2 ms at 128, 1.7 ms at 64 per factorization);
+// HM_GJ_MAX (32, 64, 96 or 128) overrides it.
+static int gj_max() {
+    static const int v = [] {
+        const char* e = std::getenv("HM_GJ_MAX");
+        const int x = e ? std::atoi(e) : 64;
+        return (x == 32 || x == 64 || x == 96 || x == 128) ? x : 64;
+    }();
+    return v;
+}
+
 void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t s) {
     std::vector<InvProblem> small, large;
+    const int gmax = gj_max();
     for (auto& p : probs) {
         if (p.n <= 0) continue;
-        (p.n <= GJ_MAX ? small : large).push_back(p);
+        (p.n <= gmax ? small : large).push_back(p);
     }
     if (!small.empty()) {
         auto st = std::make_unique<GJStep>();

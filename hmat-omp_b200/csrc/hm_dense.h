@@ -310,7 +310,8 @@ struct IdentStep : Plan::Step {
 };
 
 // X_i = inv(A_i) for a batch of square FP64 matrices of any size (X may not alias A
-// when n > GJ_MAX).  Appends the launches to `plan`.
+// when n is above the Gauss-Jordan threshold, 64 unless HM_GJ_MAX says otherwise).
+// Appends the launches to `plan`.
 struct InvProblem {
     const double* A;
     int lda;
