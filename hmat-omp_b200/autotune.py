@@ -102,6 +102,27 @@ def run_child(workload: str, choice, reps: int) -> dict:
     return json.loads(out.stdout.strip().splitlines()[-1])
 
 
+def select(base: dict, runs: list, margin: float, table: dict) -> dict:
+    """Fold child results into `table` (updated in place) and return a per-signature report.
+    base: {sig: [choice, ms]} of the heuristic run; runs: the forced runs' results.  A
+    signature gets an entry only when its fastest effective choice differs from the
+    heuristic's and beats it by more than `margin`; otherwise any old entry is dropped."""
+    cands = {sig: {} for sig in base}
+    for res in runs:
+        for sig, (eff, ms) in res.items():
+            if sig in cands:
+                cands[sig][eff] = min(ms, cands[sig].get(eff, float("inf")))
+    report = {}
+    for sig, (eff0, ms0) in base.items():
+        eff, ms = min(cands[sig].items(), key=lambda kv: kv[1]) if cands[sig] else (eff0, ms0)
+        report[sig] = {"heuristic": [eff0, round(ms0, 4)], "best": [eff, round(ms, 4)]}
+        if ms < (1.0 - margin) * ms0 and eff != eff0:
+            table[sig] = [int(v) for v in eff.split(",")]
+        else:
+            table.pop(sig, None)
+    return report
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", nargs="+", default=["headline"], choices=sorted(WORKLOADS))
@@ -120,18 +141,8 @@ def main():
     report = {}
     for wl in args.workload:
         base = run_child(wl, None, args.reps)
-        cands = {sig: {} for sig in base}
-        for ch in CHOICES:
-            for sig, (eff, ms) in run_child(wl, ch, args.reps).items():
-                if sig in cands:
-                    cands[sig][eff] = min(ms, cands[sig].get(eff, float("inf")))
-        for sig, (eff0, ms0) in base.items():
-            eff, ms = min(cands[sig].items(), key=lambda kv: kv[1]) if cands[sig] else (eff0, ms0)
-            report[sig] = {"heuristic": [eff0, round(ms0, 4)], "best": [eff, round(ms, 4)]}
-            if ms < (1.0 - args.margin) * ms0 and eff != eff0:
-                table[sig] = [int(v) for v in eff.split(",")]
-            else:
-                table.pop(sig, None)
+        runs = [run_child(wl, ch, args.reps) for ch in CHOICES]
+        report.update(select(base, runs, args.margin, table))
     with open(args.out, "w") as f:
         json.dump(dict(sorted(table.items())), f, indent=1)
         f.write("\n")
