@@ -199,6 +199,7 @@ gemm_batched_kernel(const GemmDesc<T>* __restrict__ descs, int ndesc, GenParams 
 }
 
 #include "hm_gemm_tile.cuh"
+#include "hm_gemm_dmma.cuh"
 #include "hm_gemm_tc.cuh"
 
 template <typename T>
@@ -561,7 +562,17 @@ static int pow2_ceil(long long v) {
 
 template <typename T>
 std::string GemmBatch<T>::choice() const {
-    return std::to_string(pipe_bn_) + "," + (pipe_small_ ? "1" : "0") + "," + (use_tc_ ? "1" : "0");
+    return std::to_string(pipe_bn_) + "," + (pipe_small_ ? "1" : "0") + "," + (use_tc_ || use_dmma_ ? "1" : "0");
+}
+
+// HM_FP64_DMMA=1 puts every FP64 batch the warp-tiled kernel would run on the FP64 MMA
+// kernel (tile-table entries choose it per batch through their tc flag otherwise).
+static bool fp64_dmma_forced() {
+    static const bool on = [] {
+        const char* e = std::getenv("HM_FP64_DMMA");
+        return e && e[0] == '1' && e[1] == 0;
+    }();
+    return on;
 }
 
 template <typename T>
@@ -627,6 +638,8 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
     TileChoice tuned;
     const bool have_tuned = pipe_bn_ && tile_choice(sig_, tuned);
     if (have_tuned) pipe_bn_ = tuned.bn;
+    // FP64 batches: the FP64 MMA kernel when the table's tc flag or HM_FP64_DMMA asks
+    use_dmma_ = std::is_same<T, double>::value && pipe_bn_ && (fp64_dmma_forced() || (have_tuned && tuned.tc));
     if (pipe_bn_) {
         // 64-row tiles when the batch's problems are short enough that 128-row (or
         // 256-row) tiles would pad more than a quarter of the rows
@@ -638,7 +651,8 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
             pad_small += (double)ceil_div(d.m, 64) * 64 - d.m;
         }
         pipe_small_ = have_tuned ? tuned.small != 0 : big > 64 && pad_big > 0.25 * rows && pad_small < pad_big;
-        const int BM = tile::bm_for(sizeof(T), pipe_bn_, pipe_small_);
+        if (use_dmma_) pipe_small_ = false;
+        const int BM = use_dmma_ ? dmma::bm_for(pipe_bn_) : tile::bm_for(sizeof(T), pipe_bn_, pipe_small_);
         std::vector<GemmDesc<T>> dv(h_);
         int tt = 0;
         for (auto& d : dv) {
@@ -776,6 +790,23 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) cons
             else if (pipe_bn_ == 64) tc::launch<64>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
             else if (pipe_bn_ == 96) tc::launch<96>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
             else tc::launch<128>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
+            HM_CUDA(cudaGetLastError());
+            return;
+        }
+    }
+    if constexpr (std::is_same<T, double>::value) {
+        if (use_dmma_) {
+            if (has_chains_) {
+                if (pipe_bn_ == 32) dmma::launch<32, true>(pipe_tiles_, s, d_.p, tmap_.p);
+                else if (pipe_bn_ == 64) dmma::launch<64, true>(pipe_tiles_, s, d_.p, tmap_.p);
+                else if (pipe_bn_ == 96) dmma::launch<96, true>(pipe_tiles_, s, d_.p, tmap_.p);
+                else dmma::launch<128, true>(pipe_tiles_, s, d_.p, tmap_.p);
+            } else {
+                if (pipe_bn_ == 32) dmma::launch<32, false>(pipe_tiles_, s, d_.p, tmap_.p);
+                else if (pipe_bn_ == 64) dmma::launch<64, false>(pipe_tiles_, s, d_.p, tmap_.p);
+                else if (pipe_bn_ == 96) dmma::launch<96, false>(pipe_tiles_, s, d_.p, tmap_.p);
+                else dmma::launch<128, false>(pipe_tiles_, s, d_.p, tmap_.p);
+            }
             HM_CUDA(cudaGetLastError());
             return;
         }

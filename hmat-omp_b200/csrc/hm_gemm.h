@@ -165,6 +165,7 @@ class GemmBatch {
     int pipe_bn_ = 0, pipe_tiles_ = 0;   // warp-tiled dense kernel: tile width and tile count
     bool pipe_small_ = false;            // its 64-row tile shapes
     bool gen_wide_ = false;              // generated-A batch on 64 x 128 tiles
+    bool use_dmma_ = false;              // FP64 batch on the FP64 MMA kernel (same tables)
     DBuf<int> tmap_;                     // its tile -> problem table
     // FP32 batches with long k on the tensor cores: tile count, tables, tensor maps
     bool use_tc_ = false, tc_allowed_ = true;

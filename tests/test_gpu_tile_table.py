@@ -2,6 +2,7 @@
 an operator planned under a table that forces 32-wide, 64-row tiles (and no tensor
 cores) on every step reports that choice in the profile and solves to the same answer."""
 import json
+import os
 
 import numpy as np
 import pytest
@@ -30,6 +31,8 @@ def _profiled(m, b):
     return x, {r[5].split("#")[0]: r[5].split("#")[1] for r in seq if "#" in r[5]}
 
 
+@pytest.mark.skipif(bool(os.environ.get("HM_TILE_FORCE") or os.environ.get("HM_FP64_DMMA")),
+                    reason="a forced tile choice overrides the table")
 def test_table_entries_apply_and_keep_results(tmp_path):
     b = np.random.default_rng(4).standard_normal((8192, 3))
     H.tile_table_load("")
