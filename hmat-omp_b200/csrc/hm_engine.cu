@@ -292,6 +292,7 @@ void Engine::begin_build(int N, int leaf) {
     solve32_plans_.clear();
     solveT_plans_.clear();
     exact_plans_.clear();
+    grad_plans_.clear();
     io_cols_ = 0;        // staging buffers are sized N x columns: a new N needs new ones
     ex_cols_ = 0;
     grads_ready_ = false;
@@ -1499,6 +1500,7 @@ void Engine::ensure_io(int s) {
     ioYf.alloc(n);
     ioNorm.alloc(2 * (size_t)s);
     io_cols_ = s;
+    grad_plans_.clear();
     mv_plans_.clear();
     solve64_plans_.clear();
     solve32_plans_.clear();
@@ -1953,12 +1955,43 @@ void Engine::gradients(const double* dx, int ldx, const double* dl, int ldl, int
     // stage x in ioX and lam in ioY (ld N)
     copy_in(ioX.p, dx, N, s, ldx, stream_);
     copy_in(ioY.p, dl, N, s, ldl, stream_);
-    gD_.alloc(std::max<size_t>(dD.n, 1));
-    gU_.alloc(std::max<size_t>(dU.n, 1));
-    gV_.alloc(std::max<size_t>(dV.n, 1));
-    gB_.alloc(std::max<size_t>(dB.n, 1));
+    // gradient storage like the factors' (kept across calls); the launch plan per column
+    // count is recorded once per operator
+    bool fresh = false;
+    for (auto pr : {std::make_pair(&gD_, dD.n), std::make_pair(&gU_, dU.n), std::make_pair(&gV_, dV.n),
+                    std::make_pair(&gB_, dB.n)}) {
+        if (pr.first->n != std::max<size_t>(pr.second, 1)) {
+            pr.first->alloc(std::max<size_t>(pr.second, 1));
+            fresh = true;
+        }
+    }
+    if (fresh) grad_plans_.clear();
+    if (!gAcc_.p) gAcc_.alloc(2);
     gU_.zero(stream_);
     gV_.zero(stream_);
+    auto found = grad_plans_.find(s);
+    if (found == grad_plans_.end()) found = grad_plans_.emplace(s, grad_plan(s)).first;
+    found->second.run(stream_, dstatus.p);
+    if (dparams) {
+        dparams[0] = dparams[1] = std::nan("");
+        if (gen_ != GEN_DENSE) {
+            gAcc_.zero(stream_);
+            launch_param_grad(gen_, gp_, ioX.p, ioY.p, N, s, gAcc_.p, stream_);
+            count_launch();
+            double h[2];
+            HM_CUDA(cudaMemcpyAsync(h, gAcc_.p, sizeof h, cudaMemcpyDeviceToHost, stream_));
+            HM_CUDA(cudaStreamSynchronize(stream_));
+            dparams[0] = h[0];
+            dparams[1] = h[1];
+        }
+    }
+    HM_CUDA(cudaStreamSynchronize(stream_));
+    grads_ready_ = true;
+}
+
+// dL/d(factors) for s columns staged in ioX (x) and ioY (lam), into gD_/gU_/gV_/gB_.
+Plan Engine::grad_plan(int s) {
+    const int N = N_;
     Plan pl;
     const double *X = ioX.p, *Lm = ioY.p;
     auto gLeaf = std::make_unique<GemmStep<double>>();
@@ -2008,23 +2041,7 @@ void Engine::gradients(const double* dx, int ldx, const double* dl, int ldl, int
     pl.add(std::move(gProj));
     pl.add(std::move(gMid));
     pl.add(std::move(gOut));
-    pl.run(stream_, dstatus.p);
-    if (dparams) {
-        dparams[0] = dparams[1] = std::nan("");
-        if (gen_ != GEN_DENSE) {
-            DBuf<double> acc(2);
-            acc.zero(stream_);
-            launch_param_grad(gen_, gp_, X, Lm, N, s, acc.p, stream_);
-            count_launch();
-            double h[2];
-            HM_CUDA(cudaMemcpyAsync(h, acc.p, sizeof h, cudaMemcpyDeviceToHost, stream_));
-            HM_CUDA(cudaStreamSynchronize(stream_));
-            dparams[0] = h[0];
-            dparams[1] = h[1];
-        }
-    }
-    HM_CUDA(cudaStreamSynchronize(stream_));
-    grads_ready_ = true;
+    return pl;
 }
 
 void Engine::get_gradient(int node, int which, double* out, int* rows, int* cols) const {

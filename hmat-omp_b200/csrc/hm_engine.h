@@ -152,6 +152,7 @@ class Engine {
     std::vector<int> uniform(int s) const { return std::vector<int>(sys_N_.size(), s); }
     Plan& solveT_plan(int s);
     Plan& exact_plan(int s);
+    Plan grad_plan(int s);
     void ensure_io(int s);
     std::vector<int> path_of(int n) const;   // n and its ancestors below the root
     void solve_fp64(const double* db, int s, int ldb, double* dx, int ldx);
@@ -210,7 +211,8 @@ class Engine {
     // the build's operator source (kernel generator and its parameters) and gradients
     int gen_ = GEN_DENSE;
     GenParams gp_;
-    DBuf<double> gD_, gU_, gV_, gB_;
+    DBuf<double> gD_, gU_, gV_, gB_, gAcc_;
+    std::map<int, Plan> grad_plans_;   // per column count, recorded once per operator
     bool grads_ready_ = false;
 };
 

@@ -249,55 +249,76 @@ void launch_gen_fill(const GenFillDesc* d_descs, int count, int max_elems, int g
 // ---------------------------------------------------------------------------------
 constexpr int PG_ROWS = 128, PG_COLS = 1024, PG_TILE = 128;
 
+// dA_ij/dp0 with the parameter-only factors precomputed (c1, c2: Gaussian 1/(2h^2), 1/h^3;
+// Coulomb: the softening p0, unused): no division per pair for the Gaussian.
 template <int GEN>
-__device__ __forceinline__ double gen_dparam(const GenParams& g, int r, int c) {
+__device__ __forceinline__ double gen_dparam(const GenParams& g, int r, int c, double c1, double c2) {
     if constexpr (GEN == GEN_GAUSSIAN) {
         double d2 = 0.0;
         for (int t = 0; t < g.dim; ++t) {
             const double d = g.pts[(size_t)r * g.dim + t] - g.pts[(size_t)c * g.dim + t];
             d2 += d * d;
         }
-        const double h = g.p0;
-        return exp(-d2 / (2.0 * h * h)) * d2 / (h * h * h);
+        return exp(-d2 * c1) * d2 * c2;
     } else if constexpr (GEN == GEN_COULOMB) {
         double d2 = 0.0;
         for (int t = 0; t < g.dim; ++t) {
             const double d = g.pts[(size_t)r * g.dim + t] - g.pts[(size_t)c * g.dim + t];
             d2 += d * d;
         }
-        const double den = sqrt(d2) + g.p0;
+        const double den = sqrt(d2) + c1;
         return -1.0 / (den * den);
     } else {
         return r == c ? 1.0 : 0.0;  // Cauchy: p0 is the diagonal shift
     }
 }
 
-template <int GEN>
+// SYM (kernels symmetric in i, j: Gaussian, Coulomb): only pairs j >= i are visited and an
+// off-diagonal pair adds g_ij (Lam_ij + Lam_ji), Lam = lam x^T summed over the columns;
+// CTAs whose whole column range lies below their rows return at once.
+template <int GEN, bool SYM>
 __global__ void __launch_bounds__(PG_ROWS) param_grad_kernel(GenParams gp, const double* __restrict__ X,
                                                              const double* __restrict__ L, int N, int s,
                                                              double* acc) {
     extern __shared__ double sm[];
-    double* Ls = sm;                  // [s][PG_ROWS]
-    double* Xs = sm + (size_t)s * PG_ROWS;  // [s][PG_TILE]
+    double* Lr = sm;                                     // [s][PG_ROWS]  lam of this CTA's rows
+    double* Xr = Lr + (size_t)s * PG_ROWS;               // [s][PG_ROWS]  x of the rows (SYM)
+    double* Xc = Xr + (SYM ? (size_t)s * PG_ROWS : 0);   // [s][PG_TILE]  x of the column tile
+    double* Lc = Xc + (size_t)s * PG_TILE;               // [s][PG_TILE]  lam of the column tile (SYM)
     const int i0 = blockIdx.x * PG_ROWS, j0 = blockIdx.y * PG_COLS;
+    if (SYM && j0 + PG_COLS <= i0) return;
     const int t = threadIdx.x, i = i0 + t;
-    for (int k = 0; k < s; ++k) Ls[k * PG_ROWS + t] = i < N ? L[i + (size_t)k * N] : 0.0;
+    for (int k = 0; k < s; ++k) {
+        Lr[k * PG_ROWS + t] = i < N ? L[i + (size_t)k * N] : 0.0;
+        if (SYM) Xr[k * PG_ROWS + t] = i < N ? X[i + (size_t)k * N] : 0.0;
+    }
+    double c1 = gp.p0, c2 = 0.0;
+    if (GEN == GEN_GAUSSIAN) {
+        const double h = gp.p0;
+        c1 = 1.0 / (2.0 * h * h);
+        c2 = 1.0 / (h * h * h);
+    }
     double a0 = 0.0, a1 = 0.0;
     for (int jt = j0; jt < min(N, j0 + PG_COLS); jt += PG_TILE) {
         __syncthreads();
         for (int k = 0; k < s; ++k) {
             const int j = jt + t;
-            Xs[k * PG_TILE + t] = j < N ? X[j + (size_t)k * N] : 0.0;
+            Xc[k * PG_TILE + t] = j < N ? X[j + (size_t)k * N] : 0.0;
+            if (SYM) Lc[k * PG_TILE + t] = j < N ? L[j + (size_t)k * N] : 0.0;
         }
         __syncthreads();
         if (i >= N) continue;
+        if (SYM && jt + PG_TILE <= i) continue;   // this tile lies below row i
         const int jn = min(PG_TILE, N - jt);
         for (int jj = 0; jj < jn; ++jj) {
             const int j = jt + jj;
+            if (SYM && j < i) continue;
             double dot = 0.0;
-            for (int k = 0; k < s; ++k) dot = fma(Ls[k * PG_ROWS + t], Xs[k * PG_TILE + jj], dot);
-            a0 = fma(gen_dparam<GEN>(gp, i, j), dot, a0);
+            for (int k = 0; k < s; ++k) dot = fma(Lr[k * PG_ROWS + t], Xc[k * PG_TILE + jj], dot);
             if (i == j) a1 += dot;
+            if (SYM && j > i)
+                for (int k = 0; k < s; ++k) dot = fma(Lc[k * PG_TILE + jj], Xr[k * PG_ROWS + t], dot);
+            a0 = fma(gen_dparam<GEN>(gp, i, j, c1, c2), dot, a0);
         }
     }
     for (int off = 16; off > 0; off >>= 1) {
@@ -310,30 +331,31 @@ __global__ void __launch_bounds__(PG_ROWS) param_grad_kernel(GenParams gp, const
     }
 }
 
+template <int GEN, bool SYM>
+static void launch_pg(dim3 grid, size_t smem, const GenParams& gp, const double* X, const double* L, int N, int s,
+                      double* acc, cudaStream_t st) {
+    static size_t cur = 0;
+    ensure_dyn_smem(param_grad_kernel<GEN, SYM>, smem, cur);
+    param_grad_kernel<GEN, SYM><<<grid, PG_ROWS, smem, st>>>(gp, X, L, N, s, acc);
+}
+
 void launch_param_grad(int gen, const GenParams& gp, const double* X, const double* L, int N, int s,
                        double* acc, cudaStream_t st) {
     HM_CHECK(s >= 1 && s <= 96, HM_ERR_UNSUPPORTED, "kernel-parameter gradient supports 1..96 columns");
-    const size_t smem = (size_t)s * (PG_ROWS + PG_TILE) * sizeof(double);
+    // the symmetric pass stages twice the operands: up to 48 columns within shared memory
+    const bool sym = (gen == GEN_GAUSSIAN || gen == GEN_COULOMB) && s <= 48;
+    const size_t smem = (size_t)s * (PG_ROWS + PG_TILE) * sizeof(double) * (sym ? 2 : 1);
     dim3 grid((unsigned)ceil_div(N, PG_ROWS), (unsigned)ceil_div(N, PG_COLS));
     switch (gen) {
-        case GEN_GAUSSIAN: {
-            static size_t cur = 0;
-            ensure_dyn_smem(param_grad_kernel<GEN_GAUSSIAN>, smem, cur);
-            param_grad_kernel<GEN_GAUSSIAN><<<grid, PG_ROWS, smem, st>>>(gp, X, L, N, s, acc);
+        case GEN_GAUSSIAN:
+            if (sym) launch_pg<GEN_GAUSSIAN, true>(grid, smem, gp, X, L, N, s, acc, st);
+            else launch_pg<GEN_GAUSSIAN, false>(grid, smem, gp, X, L, N, s, acc, st);
             break;
-        }
-        case GEN_COULOMB: {
-            static size_t cur = 0;
-            ensure_dyn_smem(param_grad_kernel<GEN_COULOMB>, smem, cur);
-            param_grad_kernel<GEN_COULOMB><<<grid, PG_ROWS, smem, st>>>(gp, X, L, N, s, acc);
+        case GEN_COULOMB:
+            if (sym) launch_pg<GEN_COULOMB, true>(grid, smem, gp, X, L, N, s, acc, st);
+            else launch_pg<GEN_COULOMB, false>(grid, smem, gp, X, L, N, s, acc, st);
             break;
-        }
-        case GEN_CAUCHY: {
-            static size_t cur = 0;
-            ensure_dyn_smem(param_grad_kernel<GEN_CAUCHY>, smem, cur);
-            param_grad_kernel<GEN_CAUCHY><<<grid, PG_ROWS, smem, st>>>(gp, X, L, N, s, acc);
-            break;
-        }
+        case GEN_CAUCHY: launch_pg<GEN_CAUCHY, false>(grid, smem, gp, X, L, N, s, acc, st); break;
         default: throw Error(HM_ERR_ARG, "parameter gradient needs a kernel-generated operator");
     }
     HM_CUDA(cudaGetLastError());
