@@ -154,7 +154,7 @@ void Engine::load(const char* path) {
     for (size_t i = 0; i < nodes.size(); ++i) {
         const Node &a = nodes[i], &b = nodes_[i];
         HM_CHECK(a.start == b.start && a.end == b.end && a.is_leaf == b.is_leaf && a.left == b.left &&
-                     a.right == b.right && a.parent == b.parent && a.depth == b.depth,
+                     a.right == b.right && a.parent == b.parent && a.depth == b.depth && a.sys == 0,
                  HM_ERR_ARG, "operator file: tree does not match (N, leaf)");
     }
     DBuf<double> D, U, V, B;
