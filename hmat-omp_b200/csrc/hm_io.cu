@@ -25,6 +25,9 @@
 namespace hm {
 
 namespace {
+// [off, off + count) inside an array of n elements, without wrapping
+inline bool fits(size_t off, size_t count, size_t n) { return off <= n && count <= n - off; }
+
 constexpr char MAGIC[8] = {'H', 'M', 'A', 'T', 'B', '2', '0', '0'};
 constexpr uint32_t VERSION = 1;
 static_assert(std::is_trivially_copyable<Node>::value, "Node is written as raw bytes");
@@ -164,16 +167,18 @@ void Engine::load(const char* path) {
     get_array(F, B, stream_);
     // every block the operator addresses must lie inside the arrays just read
     for (const Node& n : nodes) {
-        HM_CHECK(n.rankU >= 0 && n.rankV >= 0, HM_ERR_ARG, "operator file: bad rank");
-        if (n.is_leaf) HM_CHECK(n.offD + (size_t)n.len() * n.len() <= D.n, HM_ERR_ARG, "operator file: D range");
+        HM_CHECK(n.rankU >= 0 && n.rankV >= 0 && n.rankU <= n.len() && n.rankV <= n.len(), HM_ERR_ARG,
+                 "operator file: bad rank");
+        const size_t len = (size_t)n.len();
+        if (n.is_leaf) HM_CHECK(fits(n.offD, len * len, D.n), HM_ERR_ARG, "operator file: D range");
         if (n.parent >= 0) {
-            HM_CHECK(n.offU + (size_t)n.len() * n.rankU <= U.n && n.offV + (size_t)n.len() * n.rankV <= V.n,
-                     HM_ERR_ARG, "operator file: U/V range");
+            HM_CHECK(fits(n.offU, len * n.rankU, U.n) && fits(n.offV, len * n.rankV, V.n), HM_ERR_ARG,
+                     "operator file: U/V range");
         }
         if (!n.is_leaf) {
             const Node& L = nodes[n.left];
             const Node& R = nodes[n.right];
-            HM_CHECK(n.offB12 + (size_t)L.rankU * R.rankV <= B.n && n.offB21 + (size_t)R.rankU * L.rankV <= B.n,
+            HM_CHECK(fits(n.offB12, (size_t)L.rankU * R.rankV, B.n) && fits(n.offB21, (size_t)R.rankU * L.rankV, B.n),
                      HM_ERR_ARG, "operator file: B range");
         }
     }
@@ -198,8 +203,8 @@ void Engine::load(const char* path) {
             lv[i].first = (size_t)F.get_v<int64_t>();
             lv[i].second = F.get_v<int32_t>();
             const size_t len = (size_t)nodes[i].len();
-            HM_CHECK(lu[i].second >= 0 && lv[i].second >= 0 && lu[i].first + len * lu[i].second <= LB.n &&
-                         lv[i].first + len * lv[i].second <= LB.n,
+            HM_CHECK(lu[i].second >= 0 && lv[i].second >= 0 && fits(lu[i].first, len * lu[i].second, LB.n) &&
+                         fits(lv[i].first, len * lv[i].second, LB.n),
                      HM_ERR_ARG, "operator file: leaf basis range");
         }
         HssForm h;
@@ -217,8 +222,10 @@ void Engine::load(const char* path) {
         for (size_t i = 0; i < nodes.size(); ++i) {
             const Node& n = nodes[i];
             if (n.is_leaf) continue;
-            HM_CHECK(h.offB12[i] + (size_t)h.rankU[n.left] * h.rankV[n.right] <= HB.n &&
-                         h.offB21[i] + (size_t)h.rankU[n.right] * h.rankV[n.left] <= HB.n,
+            HM_CHECK(h.rankU[i] >= 0 && h.rankV[i] >= 0 && h.rankU[n.left] >= 0 && h.rankV[n.left] >= 0 &&
+                         h.rankU[n.right] >= 0 && h.rankV[n.right] >= 0 &&
+                         fits(h.offB12[i], (size_t)h.rankU[n.left] * h.rankV[n.right], HB.n) &&
+                         fits(h.offB21[i], (size_t)h.rankU[n.right] * h.rankV[n.left], HB.n),
                      HM_ERR_ARG, "operator file: HSS B range");
         }
         h.B = std::move(HB);
