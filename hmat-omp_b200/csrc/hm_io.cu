@@ -221,9 +221,15 @@ void Engine::load(const char* path) {
         get_array(F, HB, stream_);
         for (size_t i = 0; i < nodes.size(); ++i) {
             const Node& n = nodes[i];
-            if (n.is_leaf) continue;
-            HM_CHECK(h.rankU[i] >= 0 && h.rankV[i] >= 0 && h.rankU[n.left] >= 0 && h.rankV[n.left] >= 0 &&
-                         h.rankU[n.right] >= 0 && h.rankV[n.right] >= 0 &&
+            if (n.is_leaf) {
+                HM_CHECK(h.rankU[i] == lu[i].second && h.rankV[i] == lv[i].second, HM_ERR_ARG,
+                         "operator file: HSS leaf ranks");
+                continue;
+            }
+            // a node's rank is the sum of its children's (the reference form's B layout)
+            HM_CHECK(h.rankU[n.left] >= 0 && h.rankV[n.left] >= 0 && h.rankU[n.right] >= 0 &&
+                         h.rankV[n.right] >= 0 && h.rankU[i] == h.rankU[n.left] + h.rankU[n.right] &&
+                         h.rankV[i] == h.rankV[n.left] + h.rankV[n.right] &&
                          fits(h.offB12[i], (size_t)h.rankU[n.left] * h.rankV[n.right], HB.n) &&
                          fits(h.offB21[i], (size_t)h.rankU[n.right] * h.rankV[n.left], HB.n),
                      HM_ERR_ARG, "operator file: HSS B range");
