@@ -444,7 +444,7 @@ TileTable& tile_table() {
 }
 
 bool valid_choice(const TileChoice& c) {
-    return (c.bn == 32 || c.bn == 64 || c.bn == 96 || c.bn == 128) && (c.small == 0 || c.small == 1) &&
+    return (c.bn == 32 || c.bn == 64 || c.bn == 96 || c.bn == 128) && (c.small >= 0 && c.small <= 2) &&
            (c.tc == 0 || c.tc == 1);
 }
 
@@ -529,7 +529,7 @@ const TileChoice* forced_choice() {
         c.bn = bn;
         c.small = sm;
         c.tc = tc;
-        HM_CHECK(valid_choice(c), HM_ERR_ARG, "HM_TILE_FORCE: bn in {32,64,96,128}, small and tc 0 or 1");
+        HM_CHECK(valid_choice(c), HM_ERR_ARG, "HM_TILE_FORCE: bn in {32,64,96,128}, shape 0-2, tc 0 or 1");
         return true;
     }();
     return on ? &c : nullptr;
@@ -584,7 +584,17 @@ static int pow2_ceil(long long v) {
 
 template <typename T>
 std::string GemmBatch<T>::choice() const {
-    return std::to_string(pipe_bn_) + "," + (pipe_small_ ? "1" : "0") + "," + (use_tc_ || use_dmma_ ? "1" : "0");
+    return std::to_string(pipe_bn_) + "," + std::to_string(pipe_shape_) + "," + (use_tc_ || use_dmma_ ? "1" : "0");
+}
+
+// HM_FP64_BIG=1 gives FP64 batches without a table entry that would take the default
+// warp-tiled shape the 8 x 8-per-lane shape instead (a measurement switch).
+static bool fp64_big_forced() {
+    static const bool on = [] {
+        const char* e = std::getenv("HM_FP64_BIG");
+        return e && e[0] == '1' && e[1] == 0;
+    }();
+    return on;
 }
 
 // HM_FP64_DMMA=1 puts every FP64 batch the warp-tiled kernel would run on the FP64 MMA
@@ -672,9 +682,11 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
             pad_big += (double)ceil_div(d.m, big) * big - d.m;
             pad_small += (double)ceil_div(d.m, 64) * 64 - d.m;
         }
-        pipe_small_ = have_tuned ? tuned.small != 0 : big > 64 && pad_big > 0.25 * rows && pad_small < pad_big;
-        if (use_dmma_) pipe_small_ = false;
-        const int BM = use_dmma_ ? dmma::bm_for(pipe_bn_) : tile::bm_for(sizeof(T), pipe_bn_, pipe_small_);
+        pipe_shape_ = have_tuned ? tuned.small : (big > 64 && pad_big > 0.25 * rows && pad_small < pad_big ? 1 : 0);
+        if (!have_tuned && pipe_shape_ == 0 && fp64_big_forced()) pipe_shape_ = 2;
+        pipe_shape_ = tile::shape_for(sizeof(T), pipe_shape_);
+        if (use_dmma_) pipe_shape_ = 0;
+        const int BM = use_dmma_ ? dmma::bm_for(pipe_bn_) : tile::bm_for(sizeof(T), pipe_bn_, pipe_shape_);
         std::vector<GemmDesc<T>> dv(h_);
         int tt = 0;
         for (auto& d : dv) {
@@ -797,6 +809,19 @@ static void launch_gen(int gen, int grid, cudaStream_t s, const GemmDesc<T>* d, 
     }
 }
 
+// warp-tiled kernel for tile width bn and shape SHAPE (SHAPE 2 exists for FP64 only)
+template <typename T, int SHAPE, bool CHAIN>
+static void launch_tile(int bn, int tiles, cudaStream_t s, const GemmDesc<T>* d, const int* tp) {
+    if constexpr (SHAPE == 2 && !std::is_same<T, double>::value) {
+        throw Error(HM_ERR_STATE, "FP64-only tile shape on an FP32 batch");
+    } else {
+        if (bn == 32) tile::launch<T, 32, SHAPE, CHAIN>(tiles, s, d, tp);
+        else if (bn == 64) tile::launch<T, 64, SHAPE, CHAIN>(tiles, s, d, tp);
+        else if (bn == 96) tile::launch<T, 96, SHAPE, CHAIN>(tiles, s, d, tp);
+        else tile::launch<T, 128, SHAPE, CHAIN>(tiles, s, d, tp);
+    }
+}
+
 template <typename T>
 void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) const {
     if (h_.empty()) return;
@@ -835,29 +860,19 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) cons
     }
     if (has_chains_) {   // chained batches (the FP64 matvec's leaf + expansion)
         if constexpr (std::is_same<T, double>::value) {
-            if (pipe_small_) {
-                if (pipe_bn_ == 32) tile::launch<T, 32, true, true>(pipe_tiles_, s, d_.p, tmap_.p);
-                else if (pipe_bn_ == 64) tile::launch<T, 64, true, true>(pipe_tiles_, s, d_.p, tmap_.p);
-                else if (pipe_bn_ == 96) tile::launch<T, 96, true, true>(pipe_tiles_, s, d_.p, tmap_.p);
-                else tile::launch<T, 128, true, true>(pipe_tiles_, s, d_.p, tmap_.p);
-            } else if (pipe_bn_ == 32) tile::launch<T, 32, false, true>(pipe_tiles_, s, d_.p, tmap_.p);
-            else if (pipe_bn_ == 64) tile::launch<T, 64, false, true>(pipe_tiles_, s, d_.p, tmap_.p);
-            else if (pipe_bn_ == 96) tile::launch<T, 96, false, true>(pipe_tiles_, s, d_.p, tmap_.p);
-            else tile::launch<T, 128, false, true>(pipe_tiles_, s, d_.p, tmap_.p);
+            if (pipe_shape_ == 2) launch_tile<T, 2, true>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
+            else if (pipe_shape_ == 1) launch_tile<T, 1, true>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
+            else launch_tile<T, 0, true>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
             HM_CUDA(cudaGetLastError());
             return;
         }
         throw Error(HM_ERR_UNSUPPORTED, "chained GEMM problems are FP64 only");
     }
-    if (pipe_small_) {
-        if (pipe_bn_ == 32) tile::launch<T, 32, true>(pipe_tiles_, s, d_.p, tmap_.p);
-        else if (pipe_bn_ == 64) tile::launch<T, 64, true>(pipe_tiles_, s, d_.p, tmap_.p);
-        else if (pipe_bn_ == 96) tile::launch<T, 96, true>(pipe_tiles_, s, d_.p, tmap_.p);
-        else tile::launch<T, 128, true>(pipe_tiles_, s, d_.p, tmap_.p);
-    } else if (pipe_bn_ == 32) tile::launch<T, 32>(pipe_tiles_, s, d_.p, tmap_.p);
-    else if (pipe_bn_ == 64) tile::launch<T, 64>(pipe_tiles_, s, d_.p, tmap_.p);
-    else if (pipe_bn_ == 96) tile::launch<T, 96>(pipe_tiles_, s, d_.p, tmap_.p);
-    else if (pipe_bn_ == 128) tile::launch<T, 128>(pipe_tiles_, s, d_.p, tmap_.p);
+    if (pipe_bn_) {
+        if (pipe_shape_ == 2) launch_tile<T, 2, false>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
+        else if (pipe_shape_ == 1) launch_tile<T, 1, false>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
+        else launch_tile<T, 0, false>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
+    }
     else if (gen_wide_)
         launch_gen<T, 64, 128, 8, 4, 8>(gen_, total_tiles_, s, d_.p, (int)h_.size(), gp);
     else if (cfg_ == CFG_N_SKINNY)

@@ -84,14 +84,15 @@ enum : int { CFG_64x64 = 0, CFG_N_SKINNY = 1 };
 
 // Autotuned tile choices for the dense batched GEMM.  A batch is identified by its
 // signature (step tag, element type and bucketed problem count / m / n / k, see
-// GemmBatch::signature); the choice is the warp-tiled kernel's tile width BN, its
-// 64-row tile shapes, and whether an eligible FP32 batch takes the tensor-core kernel.
+// GemmBatch::signature); the choice is the warp-tiled kernel's tile width BN, its shape
+// (0 default, 1 64-row tiles, 2 8 x 8 outputs per lane, FP64 only), and tc: an eligible
+// FP32 batch on the tcgen05 kernel, an FP64 batch on the FP64 MMA kernel.
 // Sources, first match wins: HM_TILE_FORCE="bn,small,tc" (every batch; the offline
 // sweep's switch), then the table in the JSON file HM_TILE_TABLE names, else
 // tile_table.json beside the loaded library ({"signature": [bn, small, tc], ...},
 // written by autotune.py).  Batches without an entry keep the built-in heuristics.
 struct TileChoice {
-    int bn = 0, small = 0, tc = 1;
+    int bn = 0, small = 0, tc = 1;   // small: the shape (0, 1, 2)
 };
 bool tile_choice(const std::string& sig, TileChoice& out);
 // Replace the table with the one in `path` (an empty path clears it); false if the file
@@ -163,7 +164,7 @@ class GemmBatch {
     bool finalized_ = false;
     double flops_ = 0, bytes_ = 0;
     int pipe_bn_ = 0, pipe_tiles_ = 0;   // warp-tiled dense kernel: tile width and tile count
-    bool pipe_small_ = false;            // its 64-row tile shapes
+    int pipe_shape_ = 0;                 // its shape: 0 default, 1 64-row tiles, 2 8 x 8 per lane (FP64)
     bool gen_wide_ = false;              // generated-A batch on 64 x 128 tiles
     bool use_dmma_ = false;              // FP64 batch on the FP64 MMA kernel (same tables)
     DBuf<int> tmap_;                     // its tile -> problem table

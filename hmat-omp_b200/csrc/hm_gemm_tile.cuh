@@ -23,7 +23,9 @@ template <typename T, int WGM_, int WGN_, int UM_, int UN_, int MINB_ = 0>
 struct Cfg {
     static constexpr int WGM = WGM_, WGN = WGN_, UM = UM_, UN = UN_;
     static constexpr int NT = 32 * WGM * WGN;
-    static constexpr int BM = 32 * UM * WGM, BN = 16 * UN * WGN, BK = 16;
+    // 8-deep k-tiles for the FP64 8 x 8-per-lane shape: its accumulators take half the
+    // registers, so the next tile's staging registers must shrink
+    static constexpr int BM = 32 * UM * WGM, BN = 16 * UN * WGN, BK = (sizeof(T) == 8 && UM * UN >= 4) ? 8 : 16;
     // padded k-rows: 16 bytes past a multiple of 128 (FP32 +4, FP64 +2 elements), which
     // spreads the transposed stores of k-contiguous operands over the banks and keeps
     // every row 16-byte aligned
@@ -38,9 +40,11 @@ struct Cfg {
 // Tile shape per element type and tile width (the widest problem of the batch picks
 // the width; ranks are usually <= 96).  Chosen by timing the factor's update shapes
 // (m = node rows, n = rank, k = rank; m = n = rank, k = node rows) on B200.
-// SMALL: 64-row tiles, for batches of short problems (the many-system workload's leaves
+// SHAPE 1: 64-row tiles, for batches of short problems (the many-system workload's leaves
 // and nodes of <= 64 rows), where 128-row tiles would be half padding.
-template <typename T, int BN, bool SMALL = false> struct For;
+// SHAPE 2 (FP64): lanes own 8 x 8 outputs (UM = UN = 2), half the shared-memory reads per
+// FMA of the 4 x 8 default at the cost of one CTA per SM.
+template <typename T, int BN, int SHAPE = 0> struct For;
 template <> struct For<float, 128> { using C = Cfg<float, 2, 4, 2, 2>; };
 template <> struct For<float, 96> { using C = Cfg<float, 4, 2, 1, 3>; };
 template <> struct For<float, 64> { using C = Cfg<float, 4, 2, 1, 2>; };
@@ -49,17 +53,26 @@ template <> struct For<double, 128> { using C = Cfg<double, 2, 4, 1, 2, 2>; };
 template <> struct For<double, 96> { using C = Cfg<double, 4, 3, 1, 2>; };
 template <> struct For<double, 64> { using C = Cfg<double, 4, 2, 1, 2, 2>; };
 template <> struct For<double, 32> { using C = Cfg<double, 4, 2, 1, 1>; };
-template <> struct For<float, 128, true> { using C = Cfg<float, 2, 4, 1, 2>; };
-template <> struct For<float, 96, true> { using C = Cfg<float, 2, 3, 1, 2, 2>; };
-template <> struct For<float, 64, true> { using C = Cfg<float, 2, 2, 1, 2, 4>; };
-template <> struct For<float, 32, true> { using C = Cfg<float, 2, 2, 1, 1, 4>; };
-template <> struct For<double, 128, true> { using C = Cfg<double, 2, 4, 1, 2, 2>; };
-template <> struct For<double, 96, true> { using C = Cfg<double, 2, 3, 1, 2, 1>; };
-template <> struct For<double, 64, true> { using C = Cfg<double, 2, 2, 1, 2, 3>; };
-template <> struct For<double, 32, true> { using C = Cfg<double, 2, 2, 1, 1, 4>; };
+template <> struct For<float, 128, 1> { using C = Cfg<float, 2, 4, 1, 2>; };
+template <> struct For<float, 96, 1> { using C = Cfg<float, 2, 3, 1, 2, 2>; };
+template <> struct For<float, 64, 1> { using C = Cfg<float, 2, 2, 1, 2, 4>; };
+template <> struct For<float, 32, 1> { using C = Cfg<float, 2, 2, 1, 1, 4>; };
+template <> struct For<double, 128, 1> { using C = Cfg<double, 2, 4, 1, 2, 2>; };
+template <> struct For<double, 96, 1> { using C = Cfg<double, 2, 3, 1, 2, 1>; };
+template <> struct For<double, 64, 1> { using C = Cfg<double, 2, 2, 1, 2, 3>; };
+template <> struct For<double, 32, 1> { using C = Cfg<double, 2, 2, 1, 1, 4>; };
+template <> struct For<double, 128, 2> { using C = Cfg<double, 2, 4, 2, 2, 1>; };
+template <> struct For<double, 96, 2> { using C = Cfg<double, 2, 3, 2, 2, 1>; };
+template <> struct For<double, 64, 2> { using C = Cfg<double, 2, 2, 2, 2, 1>; };
+template <> struct For<double, 32, 2> { using C = Cfg<double, 4, 1, 2, 2, 1>; };
 
-inline int bm_for(size_t elem, int bn, bool small = false) {
-    if (small) return 64;
+// SHAPE 2 exists for FP64 only (FP32 batches fall back to SHAPE 0)
+inline int shape_for(size_t elem, int shape) { return (shape == 2 && elem == 4) ? 0 : shape; }
+
+inline int bm_for(size_t elem, int bn, int shape = 0) {
+    shape = shape_for(elem, shape);
+    if (shape == 1) return 64;
+    if (shape == 2) return bn == 32 ? 256 : 128;
     if (elem == 4) return bn == 32 ? 256 : 128;
     return bn == 128 ? 64 : 128;
 }
@@ -364,9 +377,9 @@ gemm_tile_kernel(const GemmDesc<T>* __restrict__ descs, const int* __restrict__ 
     }
 }
 
-template <typename T, int BN, bool SMALL = false, bool CHAIN = false>
+template <typename T, int BN, int SHAPE = 0, bool CHAIN = false>
 void launch(int tiles, cudaStream_t s, const GemmDesc<T>* d, const int* tile_problem) {
-    using CF = typename For<T, BN, SMALL>::C;
+    using CF = typename For<T, BN, SHAPE>::C;
     static size_t cur = 0;
     ensure_dyn_smem(gemm_tile_kernel<T, CF, CHAIN>, CF::smem, cur);
     gemm_tile_kernel<T, CF, CHAIN><<<tiles, CF::NT, CF::smem, s>>>(d, tile_problem);
