@@ -682,10 +682,10 @@ def main():
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)
-    elif args.workload == "hss":
-        run_hss(args)
-    elif args.workload == "adjoint":
-        run_adjoint(args)
+    elif args.workload in ("hss", "adjoint"):
+        # single-system workloads: rank 0 runs and prints; other ranks have nothing to do
+        if int(os.environ.get("RANK", "0")) == 0:
+            (run_hss if args.workload == "hss" else run_adjoint)(args)
     else:
         run_ours(args)
 

@@ -2,6 +2,7 @@
 accepted, anything else is refused with HM_ERR_ARG and leaves the table as it was.
 Host-only: no GPU needed."""
 import json
+import os
 
 import pytest
 
@@ -51,3 +52,11 @@ def test_missing_file_and_clear(tmp_path, lib):
     assert lib.hm_tile_table_size() == 0
     with pytest.raises(H.HmError):
         H.tile_table_load(str(tmp_path / "none.json"))
+
+
+def test_committed_table_is_valid(lib):
+    path = os.path.join(os.path.dirname(H.__file__), "tile_table.json")
+    with open(path) as f:
+        entries = json.load(f)
+    assert lib.hm_tile_table_load(path.encode()) == H.HM_OK
+    assert lib.hm_tile_table_size() == len(entries) > 0
