@@ -266,10 +266,12 @@ HM_API size_t hm_profile_report(char* buf, size_t len);
 HM_API size_t hm_profile_sequence(char* buf, size_t len);
 
 /* ---- tile autotuning (no counterpart in the reference) ----
- * Batched-GEMM steps pick their tile shape (width BN of the warp-tiled kernel, its 64-row
- * shapes, tensor cores or not for eligible FP32 batches) from a table keyed by the batch's
- * signature (step, element type, bucketed problem count and m/n/k), written by
- * hmat-omp_b200/autotune.py from timed sweeps: JSON {"signature": [bn, small, tc], ...}.
+ * Batched-GEMM steps pick their kernel and tile shape (width BN of the warp-tiled kernel;
+ * shape 0 default, 1 64-row tiles, 2 8 x 8 outputs per lane for FP64; tc: the tcgen05
+ * kernel for eligible FP32 batches, the FP64 MMA kernel for FP64 batches) from a table
+ * keyed by the batch's signature (step, element type, bucketed problem count and m/n/k),
+ * written by hmat-omp_b200/autotune.py from timed sweeps:
+ * JSON {"signature": [bn, shape, tc], ...}.
  * The table is read from HM_TILE_TABLE if set, else from tile_table.json beside the
  * library, at the first batch finalised; entries apply to operators planned afterwards.
  * Batches without an entry keep the built-in heuristics.  hm_tile_table_load replaces
