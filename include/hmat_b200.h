@@ -122,7 +122,11 @@ HM_API int hm_hodlr_build_from_kernel(hm_handle* h, int kernel, const double* po
                                       const double* params, int nparams, int leaf_size);
 
 /* HSSMatrix::build_from_dense(A, leaf_size) (hss_routines.h:50-113): build_topo ids,
- * leaf row/column bases of the off-diagonal strips, identity transfers, dense B. */
+ * leaf row/column bases of the off-diagonal strips, identity transfers, dense B — the
+ * factors hm_export_tree / hm_get_factor return.  Multiply, factor and solve run on the
+ * same operator with each coupling block recompressed to its numerical rank (singular
+ * values above 1e-15 of the largest), which keeps the Woodbury capacitance systems small
+ * and the solve accurate. */
 HM_API int hm_hss_build_from_dense(hm_handle* h, const double* A, int N, int lda, int leaf_size);
 /* Matrix-free counterpart of HSSMatrix::build_from_dense (hss_routines.h:50-113): the
  * leaf strips and coupling blocks are evaluated from the kernel on the device (same
