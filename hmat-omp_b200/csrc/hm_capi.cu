@@ -61,6 +61,49 @@ void validate(const hm_opts& o) {
     HM_CHECK(o.precision == HM_FP64 || o.precision == HM_MIXED, HM_ERR_ARG, "bad precision");
 }
 
+template <typename T>
+void gemm_batched(hm_handle* h, int count, const int* m, const int* n, const int* k, T alpha, const T* const* A,
+                  const int* lda, int opA, const T* const* B, const int* ldb, int opB, T beta, T* const* C,
+                  const int* ldc, int ksplit, int flags) {
+    HM_CHECK(count >= 0 && (count == 0 || (m && n && k && A && lda && B && ldb && C && ldc)), HM_ERR_ARG,
+             "gemm_batched: null array");
+    HM_CHECK((opA == hm::OP_N || opA == hm::OP_T) && (opB == hm::OP_N || opB == hm::OP_T), HM_ERR_ARG,
+             "gemm_batched: op must be 0 or 1");
+    const int mode = flags & 3;
+    const bool stall = (flags & HM_GEMM_TEST_STALL) != 0;
+    HM_CHECK(mode <= 2 && (flags & ~(3 | HM_GEMM_TEST_STALL)) == 0, HM_ERR_ARG, "gemm_batched: bad flags");
+    HM_CHECK(!stall || (mode == HM_GEMM_TENSOR_CORES && sizeof(T) == 4), HM_ERR_ARG,
+             "gemm_batched: HM_GEMM_TEST_STALL needs HM_GEMM_TENSOR_CORES on FP32");
+    HM_CHECK(ksplit >= 0, HM_ERR_ARG, "gemm_batched: ksplit must be >= 0");
+    if (count == 0) return;
+    cudaStream_t s = h->stream;
+    hm::GemmBatch<T> batch;
+    batch.set_tag("gemm_batched");
+    batch.set_kernel(mode);
+    batch.set_test_stall(stall);
+    for (int i = 0; i < count; ++i) {
+        HM_CHECK(m[i] >= 0 && n[i] >= 0 && k[i] >= 0, HM_ERR_ARG, "gemm_batched: negative size");
+        const int ar = opA == hm::OP_N ? m[i] : k[i], br = opB == hm::OP_N ? k[i] : n[i];
+        HM_CHECK(lda[i] >= std::max(1, ar) && ldb[i] >= std::max(1, br) && ldc[i] >= std::max(1, m[i]), HM_ERR_ARG,
+                 "gemm_batched: leading dimension below the row count");
+        if (m[i] == 0 || n[i] == 0) continue;
+        HM_CHECK(C[i] && (k[i] == 0 || (A[i] && B[i])), HM_ERR_ARG, "gemm_batched: null matrix");
+        int ks = ksplit;
+        if (ks == 0 && beta != T(0) && beta != T(1)) ks = 1;
+        batch.add(m[i], n[i], k[i], alpha, A[i], lda[i], opA, B[i], ldb[i], opB, beta, C[i], ldc[i], nullptr, ks);
+    }
+    if (batch.empty()) return;
+    batch.finalize(s);
+    hm::DBuf<int> status(1);
+    status.zero(s);
+    batch.launch(s, hm::GenParams(), status.p);
+    hm::count_launch(batch.nlaunch());
+    int st = 0;
+    HM_CUDA(cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    HM_CUDA(cudaStreamSynchronize(s));
+    if (st & hm::ST_TIMEOUT) throw hm::Error(HM_ERR_TIMEOUT, "gemm_batched: tensor-core pipeline wait timed out");
+}
+
 }  // namespace
 
 extern "C" {
@@ -352,5 +395,50 @@ size_t hm_profile_sequence(char* buf, size_t len) {
 int hm_tile_table_load(const char* path) { return hm::tile_table_load(path) ? HM_OK : HM_ERR_ARG; }
 
 int hm_tile_table_size(void) { return hm::tile_table_size(); }
+
+}  // extern "C"
+
+extern "C" {
+
+int hm_gemm_batched_f32_device(hm_handle* h, int count, const int* m, const int* n, const int* k, float alpha,
+                               const float* const* A, const int* lda, int opA, const float* const* B, const int* ldb,
+                               int opB, float beta, float* const* C, const int* ldc, int ksplit, int flags) {
+    return guard(h, [&] { gemm_batched<float>(h, count, m, n, k, alpha, A, lda, opA, B, ldb, opB, beta, C, ldc, ksplit,
+                                              flags); });
+}
+
+int hm_gemm_batched_f64_device(hm_handle* h, int count, const int* m, const int* n, const int* k, double alpha,
+                               const double* const* A, const int* lda, int opA, const double* const* B,
+                               const int* ldb, int opB, double beta, double* const* C, const int* ldc, int ksplit,
+                               int flags) {
+    return guard(h, [&] { gemm_batched<double>(h, count, m, n, k, alpha, A, lda, opA, B, ldb, opB, beta, C, ldc,
+                                               ksplit, flags); });
+}
+
+int hm_inverse_batched_device(hm_handle* h, int count, const int* n, const double* const* A, const int* lda,
+                              double* const* X, const int* ldx) {
+    return guard(h, [&] {
+        HM_CHECK(count >= 0 && (count == 0 || (n && A && lda && X && ldx)), HM_ERR_ARG, "inverse_batched: null array");
+        std::vector<hm::InvProblem> probs;
+        for (int i = 0; i < count; ++i) {
+            HM_CHECK(n[i] >= 0 && lda[i] >= std::max(1, n[i]) && ldx[i] >= std::max(1, n[i]), HM_ERR_ARG,
+                     "inverse_batched: bad order or leading dimension");
+            if (n[i] == 0) continue;
+            HM_CHECK(A[i] && X[i], HM_ERR_ARG, "inverse_batched: null matrix");
+            probs.push_back({A[i], lda[i], X[i], ldx[i], n[i]});
+        }
+        if (probs.empty()) return;
+        cudaStream_t s = h->stream;
+        hm::Plan plan;
+        hm::plan_inverse(plan, probs, s);
+        hm::DBuf<int> status(1);
+        status.zero(s);
+        plan.run(s, status.p);
+        int st = 0;
+        HM_CUDA(cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HM_CUDA(cudaStreamSynchronize(s));
+        if (st & hm::ST_SINGULAR) throw hm::Error(HM_ERR_SINGULAR, "inverse_batched: zero or non-finite pivot");
+    });
+}
 
 }  // extern "C"

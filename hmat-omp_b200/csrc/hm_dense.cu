@@ -2,8 +2,9 @@
 //
 //  * gj_inverse_kernel  — Gauss-Jordan inversion with partial pivoting, the matrix held
 //                          in registers (n <= GJ_MAX; used up to the threshold of
-//                          plan_inverse).  Larger inverses are built by
-//                          2x2 block elimination over these plus batched GEMMs.
+//                          plan_inverse).  Larger inverses are built by block
+//                          Gauss-Jordan with panel pivoting over these plus batched
+//                          GEMMs (panel_pivot_kernel, unscramble_kernel).
 //  * jacobi_kernel      — cyclic two-sided Jacobi for symmetric positive semi-definite
 //                          Gram matrices, parallel (round-robin) pair ordering, rotation
 //                          test relative to the diagonal so graded matrices keep small
@@ -608,9 +609,8 @@ void launch_ident(const DevTable<IdentDesc>& t, cudaStream_t s) {
 // ---------------------------------------------------------------------------------
 // Plans
 // ---------------------------------------------------------------------------------
-// Largest order inverted by one Gauss-Jordan kernel; larger ones are split into 2 x 2
-// blocks recursively, moving the work into batched GEMMs.  64 by default (leaf blocks of
-// 256 at N = 2^18: Gauss-Jordan time 3.2 ms at 128, 1.7 ms at 64 per factorization);
+// Largest order inverted by one Gauss-Jordan kernel; larger ones go through the block
+// Gauss-Jordan sweep below, whose bulk runs as batched GEMMs.  64 by default;
 // HM_GJ_MAX (32, 64, 96 or 128) overrides it.
 static int gj_max() {
     static const int v = [] {
@@ -620,6 +620,168 @@ static int gj_max() {
     }();
     return v;
 }
+
+// ---------------------------------------------------------------------------------
+// Block Gauss-Jordan with partial pivoting by panels (inverses above the Gauss-Jordan
+// threshold).  On a work copy W of A, for each panel of w columns K = [k0, k0 + kw):
+//   1. panel_pivot_kernel: Gaussian elimination with partial pivoting on the panel
+//      W[k0:, K] (in shared memory) chooses kw pivot rows, which are swapped into rows K
+//      across all n columns of W; the swaps are recorded in ipiv.
+//   2. Dinv = inv(W[K, K]) (Gauss-Jordan kernel);
+//   3. T = Dinv W[K, R], Z = -W[O, K] Dinv   (O, R: the rows / columns outside K);
+//   4. W[O, R] += Z W[K, R];
+//   5. W[K, K] = Dinv, W[K, R] = T, W[O, K] = Z.
+// This is the in-place (compact) Gauss-Jordan sweep a column block at a time, so
+// column c of W ends as column where[c] of inv(A), where[] being the row swaps applied
+// in order to the identity permutation (unscramble_kernel).  The pivot rows are those of
+// LU with partial pivoting of each panel, so the inverted pivot blocks W[K, K] are as
+// well conditioned as LU's diagonal blocks: a leaf whose leading block is singular while
+// the leaf is not (which getrf handles, matrix.h:120-131) inverts like any other.
+// ---------------------------------------------------------------------------------
+struct PanelDesc {
+    double* W;
+    int ld, n, k0, kw;
+    int* ipiv;    // n entries: row position i was swapped with row ipiv[i]
+};
+
+struct ScatterDesc {
+    const double* W;
+    int ldw;
+    double* X;
+    int ldx, n;
+    const int* ipiv;
+};
+
+// Panel width for order n: the (n - k0) x w panel fits in 128 KB of shared memory.
+static int bgj_width(int n) {
+    int w = 64;
+    while (w > 1 && (size_t)n * w * sizeof(double) > (size_t)128 * 1024) w /= 2;
+    return w;
+}
+
+__global__ void __launch_bounds__(256) panel_pivot_kernel(const PanelDesc* __restrict__ descs, int* status) {
+    extern __shared__ double pan[];   // m x kw, column-major, ld m
+    __shared__ double red_v[8];
+    __shared__ int red_i[8];
+    __shared__ int piv[64];
+    __shared__ int s_bad;
+    const PanelDesc d = descs[blockIdx.x];
+    const int m = d.n - d.k0, kw = d.kw, tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_bad = 0;
+    for (int e = tid; e < m * kw; e += nt) {
+        const int i = e % m, j = e / m;
+        pan[e] = d.W[(d.k0 + i) + (size_t)(d.k0 + j) * d.ld];
+    }
+    __syncthreads();
+    for (int j = 0; j < kw; ++j) {
+        // pivot: largest |pan[i, j]| over i >= j (ties to the lowest row)
+        double bv = -1.0;
+        int bi = j;
+        for (int i = j + tid; i < m; i += nt) {
+            const double v = fabs(pan[i + (size_t)j * m]);
+            if (v > bv) { bv = v; bi = i; }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, bv, off);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+        }
+        if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
+        __syncthreads();
+        if (tid == 0) {
+            double v = red_v[0];
+            int p = red_i[0];
+            for (int w = 1; w < (nt >> 5); ++w)
+                if (red_v[w] > v || (red_v[w] == v && red_i[w] < p)) { v = red_v[w]; p = red_i[w]; }
+            if (!(v > 0.0) || !isfinite(v)) { s_bad = 1; p = j; }
+            piv[j] = p;
+        }
+        __syncthreads();
+        const int p = piv[j];
+        if (p != j)
+            for (int c = tid; c < kw; c += nt) {
+                const double t = pan[j + (size_t)c * m];
+                pan[j + (size_t)c * m] = pan[p + (size_t)c * m];
+                pan[p + (size_t)c * m] = t;
+            }
+        __syncthreads();
+        const double pj = pan[j + (size_t)j * m];
+        if (pj != 0.0)
+            for (int i = j + 1 + tid; i < m; i += nt) {
+                const double l = pan[i + (size_t)j * m] / pj;
+                for (int c = j + 1; c < kw; ++c) pan[i + (size_t)c * m] -= l * pan[j + (size_t)c * m];
+            }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        if (s_bad) atomicOr(status, ST_SINGULAR);
+        for (int j = 0; j < kw; ++j) d.ipiv[d.k0 + j] = d.k0 + piv[j];
+    }
+    // the same swaps on the whole rows of W, in order (each thread owns its columns)
+    for (int c = tid; c < d.n; c += nt) {
+        double* col = d.W + (size_t)c * d.ld;
+        for (int j = 0; j < kw; ++j) {
+            const int a = d.k0 + j, b = d.k0 + piv[j];
+            if (a != b) { const double t = col[a]; col[a] = col[b]; col[b] = t; }
+        }
+    }
+}
+
+// X[:, where[c]] = W[:, c], where[] = the swaps of ipiv applied in order to the identity.
+__global__ void __launch_bounds__(256) unscramble_kernel(const ScatterDesc* __restrict__ descs) {
+    extern __shared__ int where[];
+    const ScatterDesc d = descs[blockIdx.x];
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < d.n; ++i) where[i] = i;
+        for (int i = 0; i < d.n; ++i) {
+            const int p = d.ipiv[i];
+            const int t = where[i]; where[i] = where[p]; where[p] = t;
+        }
+    }
+    __syncthreads();
+    const size_t total = (size_t)d.n * d.n;
+    for (size_t e = threadIdx.x; e < total; e += blockDim.x) {
+        const int i = (int)(e % d.n), c = (int)(e / d.n);
+        d.X[i + (size_t)where[c] * d.ldx] = d.W[i + (size_t)c * d.ldw];
+    }
+}
+
+namespace {
+struct PanelStep : Plan::Step {
+    DevTable<PanelDesc> t;
+    void run(cudaStream_t s, int* st) const override {
+        if (t.h.empty()) return;
+        size_t mx = 0;
+        for (auto& d : t.h) mx = std::max(mx, (size_t)(d.n - d.k0) * d.kw * sizeof(double));
+        static size_t cur = 0;
+        ensure_dyn_smem(panel_pivot_kernel, mx, cur);
+        panel_pivot_kernel<<<t.size(), 256, mx, s>>>(t.d.p, st);
+        HM_CUDA(cudaGetLastError());
+    }
+    const char* name() const override { return "panel_pivot"; }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
+};
+struct ScatterStep : Plan::Step {
+    DevTable<ScatterDesc> t;
+    void run(cudaStream_t s, int*) const override {
+        if (t.h.empty()) return;
+        int mx = 0;
+        for (auto& d : t.h) mx = std::max(mx, d.n);
+        static size_t cur = 0;
+        ensure_dyn_smem(unscramble_kernel, (size_t)mx * sizeof(int), cur);
+        unscramble_kernel<<<t.size(), 256, (size_t)mx * sizeof(int), s>>>(t.d.p);
+        HM_CUDA(cudaGetLastError());
+    }
+    const char* name() const override { return "unscramble_columns"; }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
+    double bytes() const override {
+        double b = 0;
+        for (auto& d : t.h) b += 16.0 * d.n * d.n;
+        return b;
+    }
+};
+}  // namespace
 
 void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t s) {
     std::vector<InvProblem> small, large;
@@ -636,50 +798,79 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
         plan.add(std::move(st));
     }
     if (large.empty()) return;
-    // 2x2 block elimination: X11 = inv(A11), T = X11 A12, W = A21 X11,
-    // S = A22 - A21 T, X22 = inv(S), X12 = -T X22, X21 = -X22 W, X11 -= X12 W.
-    std::vector<InvProblem> sub11, sub22;
-    auto copyS = std::make_unique<CopyStep>();
-    auto g1 = std::make_unique<GemmStep<double>>();
-    auto g2 = std::make_unique<GemmStep<double>>();
-    auto g3 = std::make_unique<GemmStep<double>>();
-    auto g4 = std::make_unique<GemmStep<double>>();
+    struct Work { const InvProblem* p; double *W, *Dinv, *T, *Z; int* ipiv; int w; };
+    std::vector<Work> ws;
+    int nmax = 0, steps = 0;
+    auto cp = std::make_unique<CopyStep>();
     for (auto& p : large) {
-        HM_CHECK(p.A != p.X, HM_ERR_ARG, "block inverse cannot run in place");
-        const int a = p.n / 2, b = p.n - a;
-        const double* A11 = p.A;
-        const double* A12 = p.A + (size_t)a * p.lda;
-        const double* A21 = p.A + a;
-        const double* A22 = p.A + a + (size_t)a * p.lda;
-        double* X11 = p.X;
-        double* X12 = p.X + (size_t)a * p.ldx;
-        double* X21 = p.X + a;
-        double* X22 = p.X + a + (size_t)a * p.ldx;
-        double* T = plan.scratch((size_t)a * b);
-        double* W = plan.scratch((size_t)b * a);
-        double* S = plan.scratch((size_t)b * b);
-        sub11.push_back({A11, p.lda, X11, p.ldx, a});
-        copyS->t.h.push_back({A22, p.lda, S, b, b, b, 0, 0, 0});
-        g1->batch.add(a, b, a, 1.0, X11, p.ldx, OP_N, A12, p.lda, OP_N, 0.0, T, a);
-        g1->batch.add(b, a, a, 1.0, A21, p.lda, OP_N, X11, p.ldx, OP_N, 0.0, W, b);
-        g2->batch.add(b, b, a, -1.0, A21, p.lda, OP_N, T, a, OP_N, 1.0, S, b);
-        sub22.push_back({S, b, X22, p.ldx, b});
-        g3->batch.add(a, b, b, -1.0, T, a, OP_N, X22, p.ldx, OP_N, 0.0, X12, p.ldx);
-        g3->batch.add(b, a, b, -1.0, X22, p.ldx, OP_N, W, b, OP_N, 0.0, X21, p.ldx);
-        g4->batch.add(a, a, b, -1.0, X12, p.ldx, OP_N, W, b, OP_N, 1.0, X11, p.ldx);
+        HM_CHECK(p.n <= 16384, HM_ERR_UNSUPPORTED, "inverse: order above 16384");
+        Work x{&p, nullptr, nullptr, nullptr, nullptr, nullptr, bgj_width(p.n)};
+        x.W = plan.scratch((size_t)p.n * p.n);
+        x.Dinv = plan.scratch((size_t)x.w * x.w);
+        x.T = plan.scratch((size_t)x.w * p.n);
+        x.Z = plan.scratch((size_t)p.n * x.w);
+        x.ipiv = plan.scratch_i(p.n);
+        cp->t.h.push_back({p.A, p.lda, x.W, p.n, p.n, p.n, 0, 0, 0});
+        ws.push_back(x);
+        nmax = std::max(nmax, p.n);
+        steps = std::max(steps, ceil_div(p.n, x.w));
     }
-    copyS->t.upload(s);
-    plan.add(std::move(copyS));
-    plan_inverse(plan, sub11, s);
-    g1->batch.finalize(s);
-    plan.add(std::move(g1));
-    g2->batch.finalize(s);
-    plan.add(std::move(g2));
-    plan_inverse(plan, sub22, s);
-    g3->batch.finalize(s);
-    plan.add(std::move(g3));
-    g4->batch.finalize(s);
-    plan.add(std::move(g4));
+    cp->t.upload(s);
+    plan.add(std::move(cp));
+    for (int b = 0; b < steps; ++b) {
+        auto pan = std::make_unique<PanelStep>();
+        auto gj = std::make_unique<GJStep>();
+        auto gTZ = std::make_unique<GemmStep<double>>("inverse.panel");
+        auto gUp = std::make_unique<GemmStep<double>>("inverse.update");
+        auto put = std::make_unique<CopyStep>();
+        for (auto& x : ws) {
+            const int n = x.p->n, k0 = b * x.w;
+            if (k0 >= n) continue;
+            const int kw = std::min(x.w, n - k0), e0 = k0 + kw, ld = n;
+            double* W = x.W;
+            pan->t.h.push_back({W, ld, n, k0, kw, x.ipiv});
+            gj->t[kw <= 32 ? 0 : 1].h.push_back({W + k0 + (size_t)k0 * ld, ld, x.Dinv, kw, kw});
+            // column ranges R1 = [0, k0), R2 = [e0, n); row ranges O1, O2 the same
+            const int r0[2] = {0, e0}, rl[2] = {k0, n - e0};
+            for (int q = 0; q < 2; ++q) {
+                if (rl[q] <= 0) continue;
+                // T[:, Rq] = Dinv W[K, Rq]
+                gTZ->batch.add(kw, rl[q], kw, 1.0, x.Dinv, kw, OP_N, W + k0 + (size_t)r0[q] * ld, ld, OP_N, 0.0,
+                               x.T + (size_t)r0[q] * kw, kw);
+                // Z[Oq, :] = -W[Oq, K] Dinv
+                gTZ->batch.add(rl[q], kw, kw, -1.0, W + r0[q] + (size_t)k0 * ld, ld, OP_N, x.Dinv, kw, OP_N, 0.0,
+                               x.Z + r0[q], n);
+            }
+            for (int qi = 0; qi < 2; ++qi)
+                for (int qj = 0; qj < 2; ++qj) {
+                    if (rl[qi] <= 0 || rl[qj] <= 0) continue;
+                    // W[Oqi, Rqj] += Z[Oqi, :] W[K, Rqj]
+                    gUp->batch.add(rl[qi], rl[qj], kw, 1.0, x.Z + r0[qi], n, OP_N, W + k0 + (size_t)r0[qj] * ld, ld,
+                                   OP_N, 1.0, W + r0[qi] + (size_t)r0[qj] * ld, ld);
+                }
+            put->t.h.push_back({x.Dinv, kw, W + k0 + (size_t)k0 * ld, ld, kw, kw, 0, 0, 0});
+            for (int q = 0; q < 2; ++q) {
+                if (rl[q] <= 0) continue;
+                put->t.h.push_back({x.T + (size_t)r0[q] * kw, kw, W + k0 + (size_t)r0[q] * ld, ld, kw, rl[q], 0, 0, 0});
+                put->t.h.push_back({x.Z + r0[q], n, W + r0[q] + (size_t)k0 * ld, ld, rl[q], kw, 0, 0, 0});
+            }
+        }
+        pan->t.upload(s);
+        for (auto& tb : gj->t) tb.upload(s);
+        gTZ->batch.finalize(s);
+        gUp->batch.finalize(s);
+        put->t.upload(s);
+        plan.add(std::move(pan));
+        plan.add(std::move(gj));
+        if (!gTZ->batch.empty()) plan.add(std::move(gTZ));
+        if (!gUp->batch.empty()) plan.add(std::move(gUp));
+        plan.add(std::move(put));
+    }
+    auto sc = std::make_unique<ScatterStep>();
+    for (auto& x : ws) sc->t.h.push_back({x.W, x.p->n, x.p->X, x.p->ldx, x.p->n, x.ipiv});
+    sc->t.upload(s);
+    plan.add(std::move(sc));
+    (void)nmax;
 }
 
 void plan_gram_svd(Plan& plan, const std::vector<SvdProblem>& probs, double tol, int max_rank,

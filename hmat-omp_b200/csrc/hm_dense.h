@@ -12,8 +12,8 @@
 
 namespace hm {
 
-// Largest matrix inverted directly (in registers) by Gauss-Jordan; larger inverses are
-// split 2x2 (block elimination) down to this size.
+// Largest matrix inverted directly (in registers) by Gauss-Jordan; larger inverses run
+// the block Gauss-Jordan sweep with panel pivoting (plan_inverse).
 constexpr int GJ_MAX = 128;
 // Widest sketch (rsvd_rank + oversample) and full-SVD block the Jacobi kernels take.
 constexpr int SKETCH_MAX = 160;
@@ -309,8 +309,9 @@ struct IdentStep : Plan::Step {
     int nlaunch() const override { return t.h.empty() ? 0 : 1; }
 };
 
-// X_i = inv(A_i) for a batch of square FP64 matrices of any size (X may not alias A
-// when n is above the Gauss-Jordan threshold, 64 unless HM_GJ_MAX says otherwise).
+// X_i = inv(A_i) for a batch of square FP64 matrices (n <= 16384), with partial
+// pivoting at every size: Gauss-Jordan up to the threshold (64 unless HM_GJ_MAX says
+// otherwise), block Gauss-Jordan with panel pivoting above it.  X may alias A.
 // Appends the launches to `plan`.
 struct InvProblem {
     const double* A;

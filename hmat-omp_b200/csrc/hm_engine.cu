@@ -196,7 +196,7 @@ void Engine::check_status(const char* what) {
     HM_CUDA(cudaStreamSynchronize(stream_));
     if (st & ST_SINGULAR) throw Error(HM_ERR_SINGULAR, std::string(what) + ": singular pivot");
     if (st & ST_NONFINITE) throw Error(HM_ERR_NONFINITE, std::string(what) + ": non-finite values");
-    if (st & ST_TIMEOUT) throw Error(HM_ERR_CUDA, std::string(what) + ": tensor-core pipeline wait timed out");
+    if (st & ST_TIMEOUT) throw Error(HM_ERR_TIMEOUT, std::string(what) + ": tensor-core pipeline wait timed out");
     if (st & ST_NO_CONVERGE)
         throw Error(HM_ERR_NO_CONVERGE, std::string(what) + ": Jacobi sweep limit reached");
 }
@@ -279,6 +279,7 @@ struct Block {
 
 void Engine::begin_build(int N, int leaf) {
     HM_CHECK(N > 0 && leaf > 0, HM_ERR_ARG, "build: N and leaf_size must be positive");
+    HM_CUDA(cudaGetDevice(&device_));
     N_ = N;
     leaf_ = leaf;
     built_ = factored_ = false;

@@ -127,8 +127,9 @@ class Engine {
         const double *D, *U, *V, *B;
         int N;
         bool built;
+        int device;   // the CUDA device the operator's storage lives on
     };
-    View view() const { return {&nodes_, &leaves_, &levels_, dD.p, dU.p, dV.p, dB.p, N_, built_}; }
+    View view() const { return {&nodes_, &leaves_, &levels_, dD.p, dU.p, dV.p, dB.p, N_, built_, device_}; }
 
   protected:
     void plan_levels();
@@ -163,6 +164,7 @@ class Engine {
     Kind kind_;
     cudaStream_t stream_ = nullptr;
     int N_ = 0, leaf_ = 0;
+    int device_ = 0;   // current device when the operator was built (or loaded)
     std::vector<Node> nodes_;
     std::vector<std::vector<int>> levels_;   // internal nodes by depth
     std::vector<int> leaves_;

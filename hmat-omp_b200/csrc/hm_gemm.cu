@@ -672,6 +672,8 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
     if (have_tuned) pipe_bn_ = tuned.bn;
     // FP64 batches: the FP64 MMA kernel when the table's tc flag or HM_FP64_DMMA asks
     use_dmma_ = std::is_same<T, double>::value && pipe_bn_ && (fp64_dmma_forced() || (have_tuned && tuned.tc));
+    if (kernel_mode_ == 1) use_dmma_ = std::is_same<T, double>::value && pipe_bn_;
+    if (kernel_mode_ == 2) use_dmma_ = false;
     if (pipe_bn_) {
         // 64-row tiles when the batch's problems are short enough that 128-row (or
         // 256-row) tiles would pad more than a quarter of the rows
@@ -715,7 +717,14 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
     }
     use_tc_ = false;
     if constexpr (std::is_same<T, float>::value) {
-        if (pipe_bn_ && tc_allowed_ && !has_chains_ && (!have_tuned || tuned.tc)) finalize_tc(s);
+        if (kernel_mode_ == 1) {
+            HM_CHECK(pipe_bn_ && !has_chains_, HM_ERR_UNSUPPORTED, "tensor-core GEMM: batch not eligible");
+            finalize_tc(s, true);
+            HM_CHECK(use_tc_, HM_ERR_UNSUPPORTED,
+                     "tensor-core GEMM: operands not TMA-addressable (16-byte aligned, ld a multiple of 4)");
+        } else if (kernel_mode_ == 0 && pipe_bn_ && tc_allowed_ && !has_chains_ && (!have_tuned || tuned.tc)) {
+            finalize_tc(s);
+        }
     }
     if (!hz_.empty()) {
         dz_.alloc(hz_.size());
@@ -730,7 +739,7 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
 // operands the TMA can address run on the tensor cores (3xTF32); short-k batches keep
 // the FMA kernel, which is as fast there.
 template <typename T>
-void GemmBatch<T>::finalize_tc(cudaStream_t s) {
+void GemmBatch<T>::finalize_tc(cudaStream_t s, bool force) {
     if constexpr (std::is_same<T, float>::value) {
         std::vector<GemmDesc<float>> dv(h_);
         long long kblocks = 0;
@@ -744,7 +753,7 @@ void GemmBatch<T>::finalize_tc(cudaStream_t s) {
             tt += tiles;
             kblocks += (long long)d.tiles_m * d.tiles_n * ceil_div(std::max(d.k, 1), tc::BK);
         }
-        if (tt == 0 || kblocks < 4LL * tt) return;
+        if (tt == 0 || (!force && kblocks < 4LL * tt)) return;
         std::vector<CUtensorMap> maps;
         if (!tc::encode_maps(dv, pipe_bn_, maps)) return;
         std::vector<int> tp((size_t)tt);
@@ -833,10 +842,10 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) cons
             const auto* maps = reinterpret_cast<const CUtensorMap*>(tcmaps_.p);
             int* st = status ? status : tcstatus_.p;
             const int sms = sm_count();
-            if (pipe_bn_ == 32) tc::launch<32>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
-            else if (pipe_bn_ == 64) tc::launch<64>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
-            else if (pipe_bn_ == 96) tc::launch<96>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
-            else tc::launch<128>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st);
+            if (pipe_bn_ == 32) tc::launch<32>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);
+            else if (pipe_bn_ == 64) tc::launch<64>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);
+            else if (pipe_bn_ == 96) tc::launch<96>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);
+            else tc::launch<128>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);
             HM_CUDA(cudaGetLastError());
             return;
         }

@@ -122,8 +122,16 @@ class GemmBatch {
     std::string choice() const;
     // Upload the table (once); later launches reuse it (and may be graph-captured).
     void finalize(cudaStream_t s);
-    void finalize_tc(cudaStream_t s);
+    void finalize_tc(cudaStream_t s, bool force = false);
     bool on_tensor_cores() const { return use_tc_; }
+    bool on_fp64_mma() const { return use_dmma_; }
+    // Kernel selection for finalize: 0 the built-in rules and tile table; 1 the tensor-core
+    // kernel (tcgen05 for FP32 -- finalize throws HM_ERR_UNSUPPORTED if the operands are
+    // not TMA-addressable; the FP64 MMA kernel for FP64); 2 the warp-tiled FMA kernel.
+    void set_kernel(int mode) { kernel_mode_ = mode; }
+    // Test of the tensor-core kernel's timeout path: its producer issues no copies and its
+    // role waits give up after ~0.5 ms, so the launch sets ST_TIMEOUT with nothing in flight.
+    void set_test_stall(bool on) { tc_stall_ = on; }
     // whether finalize may put this (FP32) batch on the tensor cores
     void allow_tensor_cores(bool on) { tc_allowed_ = on; }
     // status: device status word for the tensor-core kernel's bounded waits (may be null
@@ -169,7 +177,8 @@ class GemmBatch {
     bool use_dmma_ = false;              // FP64 batch on the FP64 MMA kernel (same tables)
     DBuf<int> tmap_;                     // its tile -> problem table
     // FP32 batches with long k on the tensor cores: tile count, tables, tensor maps
-    bool use_tc_ = false, tc_allowed_ = true;
+    bool use_tc_ = false, tc_allowed_ = true, tc_stall_ = false;
+    int kernel_mode_ = 0;
     int tc_tiles_ = 0;
     DBuf<GemmDesc<T>> tcd_;
     DBuf<int> tct_;

@@ -34,6 +34,9 @@
 //              next tile's MMAs.
 // Every wait on an mbarrier gives up after about a second of clock, sets ST_TIMEOUT in
 // the status word and makes all roles leave; the tensor memory is always released.
+// Teardown waits (copies and MMAs already issued) keep the one-second bound even when a
+// role wait gave up early.  A stall switch (tests of this path only) makes the producer
+// issue nothing and shortens the role waits, so they run out with nothing in flight.
 #pragma once
 
 namespace tc {
@@ -168,15 +171,23 @@ __device__ __forceinline__ float tf32_rn(float x) {
     return __uint_as_float(r);
 }
 
-// Wait for phase `parity` of barrier b, at most about a second; false on timeout (and
+// Clock cycles a role wait (wait_bar) polls before it gives up: about a second.
+constexpr long long ROLE_WAIT_CYCLES = 2000000000ll;
+// With the stall switch (a test of the timeout path, set only through the batched-GEMM
+// entry point's HM_GEMM_TEST_STALL flag) the producer issues no copy and the role waits
+// give up after this many cycles instead (~0.5 ms).
+constexpr long long STALL_WAIT_CYCLES = 1ll << 20;
+
+// Wait for phase `parity` of barrier b, at most `limit` cycles; false on timeout (and
 // the CTA-wide abort flag is raised).
-__device__ __forceinline__ bool wait_bar(uint32_t b, uint32_t parity, volatile int* abort_flag, int* status) {
+__device__ __forceinline__ bool wait_bar(uint32_t b, uint32_t parity, volatile int* abort_flag, int* status,
+                                         long long limit) {
     if (mbar_try(b, parity)) return true;
     const long long t0 = clock64();
     for (;;) {
         if (mbar_try(b, parity)) return true;
         if (*abort_flag) return false;
-        if (clock64() - t0 > 2000000000ll) {
+        if (clock64() - t0 > limit) {
             *abort_flag = 1;
             atomicOr(status, ST_TIMEOUT);
             return false;
@@ -199,9 +210,10 @@ __device__ __forceinline__ void wait_bar_final(uint32_t b, uint32_t parity, int*
 
 // The same wait taken by a whole warp: lane 0 polls, the warp follows its verdict
 // (keeps the warp converged for the .sync.aligned tensor-memory loads that follow).
-__device__ __forceinline__ bool wait_bar_warp(uint32_t b, uint32_t parity, volatile int* abort_flag, int* status) {
+__device__ __forceinline__ bool wait_bar_warp(uint32_t b, uint32_t parity, volatile int* abort_flag, int* status,
+                                              long long limit) {
     int ok = 0;
-    if ((threadIdx.x & 31) == 0) ok = wait_bar(b, parity, abort_flag, status) ? 1 : 0;
+    if ((threadIdx.x & 31) == 0) ok = wait_bar(b, parity, abort_flag, status, limit) ? 1 : 0;
     return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
@@ -239,7 +251,7 @@ __device__ __forceinline__ TileInfo decode(const GemmDesc<float>* __restrict__ d
 template <int BN>
 __global__ void __launch_bounds__(NT, 1)
 gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restrict__ tile_problem, int ntiles,
-                 const CUtensorMap* __restrict__ tmaps, int* status) {
+                 const CUtensorMap* __restrict__ tmaps, int* status, int stall) {
     using S = Shape<BN>;
     constexpr int ST = S::ST;
     extern __shared__ unsigned char smraw[];
@@ -292,13 +304,14 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
     tc_after();
     const uint32_t tmem = s_tmem;
     volatile int* abort_flag = &s_abort;
+    const long long lim = stall ? STALL_WAIT_CYCLES : ROLE_WAIT_CYCLES;
 
     if (warp == 0) {
         // ------------------------------ TMA producer ------------------------------
         if (lane == 0) {
             int slot = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            for (int tile = blockIdx.x; tile < ntiles && ok && !stall; tile += gridDim.x) {
                 const TileInfo ti = decode<BN>(descs, tile_problem, tile);
                 const GemmDesc<float>& D = descs[ti.p];
                 const bool a_mn = D.opA == OP_N, b_mn = D.opB == OP_T;
@@ -306,7 +319,7 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
                 const CUtensorMap* mb = ma + 1;
                 for (int kt = 0; kt < ti.nk; ++kt, ++slot) {
                     const int st = slot % ST;
-                    if (!wait_bar(empty(st), ((slot / ST) & 1) ^ 1, abort_flag, status)) { ok = false; break; }
+                    if (!wait_bar(empty(st), ((slot / ST) & 1) ^ 1, abort_flag, status, lim)) { ok = false; break; }
                     const uint32_t base = stage0 + (uint32_t)st * S::STAGE;
                     const uint32_t bbase = base + 2 * S::A_BYTES;
                     const int k0 = ti.kb + kt * BK;
@@ -339,7 +352,7 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
             const TileInfo ti = decode<BN>(descs, tile_problem, tile);
             for (int kt = 0; kt < ti.nk; ++kt, ++slot) {
                 const int st = slot % ST;
-                if (!wait_bar_warp(raw(st), (slot / ST) & 1, abort_flag, status)) { ok = false; break; }
+                if (!wait_bar_warp(raw(st), (slot / ST) & 1, abort_flag, status, lim)) { ok = false; break; }
                 const uint32_t base = stage0 + (uint32_t)st * S::STAGE;
                 constexpr int CA = S::A_BYTES / 16, CB = S::B_BYTES / 16;
                 constexpr int NCH = (CA + CB + NCONV - 1) / NCONV;
@@ -390,7 +403,7 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
                 const int nt = min(BN, D.n - ti.n0);
                 const int ninst = (nt + 15) / 16 * 16;
                 const int acc = accn & 1;
-                if (!wait_bar(tempty(acc), ((accn >> 1) & 1) ^ 1, abort_flag, status)) break;
+                if (!wait_bar(tempty(acc), ((accn >> 1) & 1) ^ 1, abort_flag, status, lim)) break;
                 tc_after();
                 const uint32_t dt = tmem + (uint32_t)(acc * S::ACC_COLS);
                 const uint32_t idesc = idesc_tf32(a_mn, b_mn, ninst);
@@ -403,7 +416,7 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
                 const uint32_t a_lay = a_mn ? 1u : 2u, b_lay = b_mn ? 1u : 2u;
                 for (int kt = 0; kt < ti.nk; ++kt, ++slot) {
                     const int st = slot % ST;
-                    if (!wait_bar(full(st), (slot / ST) & 1, abort_flag, status)) { ok = false; break; }
+                    if (!wait_bar(full(st), (slot / ST) & 1, abort_flag, status, lim)) { ok = false; break; }
                     tc_after();
                     const uint32_t base = stage0 + (uint32_t)st * S::STAGE;
                     const uint32_t ahi = base, alo = base + S::A_BYTES;
@@ -469,10 +482,10 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
                 mbar_arrive(cfree);
             }
             const int acc = accn & 1;
-            if (!wait_bar_warp(tfull(acc), (accn >> 1) & 1, abort_flag, status)) break;
-            if (!wait_bar_warp(cfree, accn & 1, abort_flag, status)) break;
+            if (!wait_bar_warp(tfull(acc), (accn >> 1) & 1, abort_flag, status, lim)) break;
+            if (!wait_bar_warp(cfree, accn & 1, abort_flag, status, lim)) break;
             if (rd && c_tma) {
-                if (!wait_bar_warp(cfull, rdn & 1, abort_flag, status)) break;
+                if (!wait_bar_warp(cfull, rdn & 1, abort_flag, status, lim)) break;
                 if (leader) c_pending = false;
             }
             tc_after();
@@ -517,7 +530,7 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
             fence_async_smem();
             mbar_arrive(cdone);
             if (leader) {
-                if (!wait_bar(cdone, accn & 1, abort_flag, status)) break;
+                if (!wait_bar(cdone, accn & 1, abort_flag, status, lim)) break;
                 if (via_tma) {
                     if (split) tma2d_add(mc, ti.m0, ti.n0, smem_u32(cbuf));
                     else tma2d_store(mc, ti.m0, ti.n0, smem_u32(cbuf));
@@ -543,12 +556,12 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
 
 template <int BN>
 void launch(int tiles, int sms, cudaStream_t s, const GemmDesc<float>* d, const int* tile_problem,
-            const CUtensorMap* tmaps, int* status) {
+            const CUtensorMap* tmaps, int* status, int stall) {
     using S = Shape<BN>;
     static size_t cur = 0;
     ensure_dyn_smem(gemm_tc32_kernel<BN>, S::SMEM, cur);
     const int grid = std::max(1, std::min(tiles, sms));
-    gemm_tc32_kernel<BN><<<grid, NT, S::SMEM, s>>>(d, tile_problem, tiles, tmaps, status);
+    gemm_tc32_kernel<BN><<<grid, NT, S::SMEM, s>>>(d, tile_problem, tiles, tmaps, status, stall);
 }
 
 // Whether the tensor-core kernel can take a problem: the TMA wants 16-byte aligned bases

@@ -2,20 +2,23 @@
 // any device allocation.
 //
 // Who needs it: code that may not call cudaMalloc at the moment it multiplies — a
-// solver loop being captured into a CUDA graph (an allocation inside a capture is an
-// error), a real-time or callback thread that must not block in the allocator, or an
-// application that hands out all device memory through its own pool.  Such callers
-// build the operator once at set-up (that build allocates) and then multiply here.
+// real-time or callback thread that must not block in the device allocator, or an
+// application that hands out all device memory through its own pool and forbids other
+// allocations.  Such callers build the operator once at set-up (that build allocates)
+// and then multiply here.
 //
 // The per-node intermediates (t = V^T x, delta = B t) and the launch tables live in one
 // file-scope __device__ array of NOALLOC_SCRATCH_BYTES (32 MiB).  Every GPU that loads
 // the library holds that array until the process exits.  In host code the array's name
 // is only a host-side stand-in, so its device address is fetched with
 // cudaGetSymbolAddress once per device (the first call on a device, with that device
-// current) and cached; that first call should therefore happen before any stream
-// capture.  All calls share the array and it keeps the last call's contents: the split-K
-// partial sums are zeroed by the launch itself before accumulation, and two calls whose
-// work overlaps on the GPU (e.g. on two streams) race on the array.
+// current) and cached.  The operator's device must be the current device.  All calls
+// share the array and it keeps the last call's contents: the split-K partial sums are
+// zeroed by the launch itself before accumulation, and two calls whose work overlaps on
+// the GPU (e.g. on two streams, or two handles) race on the array.  Each call copies its
+// launch tables from host memory into the array with cudaMemcpyAsync; a copy from
+// pageable host memory first waits for the work already queued on the stream, so the
+// call returns once the stream has reached it.
 #include <mutex>
 
 #include "hm_engine.h"
@@ -51,6 +54,13 @@ void multiply_noalloc(const Engine::View& v, const double* dx, int s, int ldx, d
                       cudaStream_t st) {
     HM_CHECK(v.built, HM_ERR_STATE, "multiply before build");
     HM_CHECK(dx && dy && s >= 1 && ldx >= v.N && ldy >= v.N, HM_ERR_ARG, "multiply_noalloc: bad arguments");
+    {   // the scratch address is per device: the operator's device must be current
+        int cur = 0;
+        HM_CUDA(cudaGetDevice(&cur));
+        HM_CHECK(cur == v.device, HM_ERR_ARG,
+                 "multiply_noalloc: the current device (" + std::to_string(cur) + ") is not the operator's (" +
+                     std::to_string(v.device) + ")");
+    }
     const std::vector<Node>& nodes = *v.nodes;
     const std::vector<std::vector<int>>& levels = *v.levels;
     // 1) scratch offsets for t and delta of every internal node (first in the array)
@@ -151,7 +161,7 @@ void multiply_noalloc(const Engine::View& v, const double* dx, int s, int ldx, d
                            reinterpret_cast<const ZeroRegion<double>*>(base + p.zero), p.nz, st);
         count_launch((p.nd ? 1 : 0) + (p.nz ? 1 : 0));
     }
-    // the host-side tables above are pageable: each copy completed its staging before
+    // the host-side tables above are pageable: each copy has staged them before
     // returning, so they may go out of scope now
 }
 

@@ -19,7 +19,8 @@ LIB_PATH = os.path.join(HERE, "libhmat_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "hmat_b200.h")
 
 HM_OK, HM_ERR_ARG, HM_ERR_CUDA, HM_ERR_SINGULAR, HM_ERR_NO_CONVERGE = 0, 1, 2, 3, 4
-HM_ERR_NONFINITE, HM_ERR_STATE, HM_ERR_UNSUPPORTED, HM_ERR_IR = 5, 6, 7, 8
+HM_ERR_NONFINITE, HM_ERR_STATE, HM_ERR_UNSUPPORTED, HM_ERR_IR, HM_ERR_TIMEOUT = 5, 6, 7, 8, 9
+GEMM_AUTO, GEMM_TENSOR_CORES, GEMM_FMA, GEMM_TEST_STALL = 0, 1, 2, 16
 SKETCH_REFERENCE_UNIFORM, SKETCH_REFERENCE_NORMAL, SKETCH_DEVICE_NORMAL = 0, 1, 2
 FP64, MIXED = 0, 1
 KERNEL_CAUCHY, KERNEL_GAUSSIAN, KERNEL_COULOMB = 1, 2, 3
@@ -111,6 +112,11 @@ def load() -> C.CDLL:
         getattr(L, f).restype = C.c_size_t
     L.hm_save.argtypes = [C.c_void_p, C.c_char_p]
     L.hm_load.argtypes = [C.c_void_p, C.c_char_p]
+    PPd = C.POINTER(C.c_void_p)
+    for f, T in (("hm_gemm_batched_f32_device", C.c_float), ("hm_gemm_batched_f64_device", C.c_double)):
+        getattr(L, f).argtypes = [C.c_void_p, C.c_int, _ip, _ip, _ip, T, PPd, _ip, C.c_int, PPd, _ip, C.c_int, T,
+                                  PPd, _ip, C.c_int, C.c_int]
+    L.hm_inverse_batched_device.argtypes = [C.c_void_p, C.c_int, _ip, PPd, _ip, PPd, _ip]
     L.hm_tile_table_load.argtypes = [C.c_char_p]
     L.hm_tile_table_size.argtypes = []
     _lib = L
@@ -344,6 +350,37 @@ class _Handle:
         if out.size:
             self._check(self._L.hm_get_factor(self._h, node, which, _d(out), C.byref(r), C.byref(c)))
         return out.reshape(c.value, r.value).T.copy()
+
+
+class Dense(_Handle):
+    """Batched dense building blocks on the device (no tree): the products of
+    Matrix::operator* (matrix.h:93-104) and the inverses of Matrix::inverse
+    (matrix.h:133-149) for many independent matrices per launch.  Arguments are lists of
+    device pointers (e.g. ``torch.Tensor.data_ptr()``) and sizes."""
+
+    def __init__(self):
+        super().__init__(0.0)
+
+    @staticmethod
+    def _ia(v):
+        return np.ascontiguousarray(v, dtype=np.int32)
+
+    def gemm(self, m, n, k, alpha, A, lda, opA, B, ldb, opB, beta, Cs, ldc, ksplit=0, flags=GEMM_AUTO,
+             dtype="f32"):
+        cnt = len(m)
+        PP = C.c_void_p * max(cnt, 1)
+        arrs = [self._ia(v) for v in (m, n, k, lda, ldb, ldc)]
+        ip = [a.ctypes.data_as(_ip) for a in arrs]
+        f = self._L.hm_gemm_batched_f32_device if dtype == "f32" else self._L.hm_gemm_batched_f64_device
+        self._check(f(self._h, cnt, ip[0], ip[1], ip[2], alpha, PP(*A), ip[3], opA, PP(*B), ip[4], opB, beta,
+                      PP(*Cs), ip[5], ksplit, flags))
+
+    def inverse(self, n, A, lda, X, ldx):
+        cnt = len(n)
+        PP = C.c_void_p * max(cnt, 1)
+        na, la, lx = self._ia(n), self._ia(lda), self._ia(ldx)
+        self._check(self._L.hm_inverse_batched_device(self._h, cnt, na.ctypes.data_as(_ip), PP(*A),
+                                                      la.ctypes.data_as(_ip), PP(*X), lx.ctypes.data_as(_ip)))
 
 
 class HODLRMatrix(_Handle):

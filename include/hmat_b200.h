@@ -41,7 +41,8 @@ enum {
     HM_ERR_NONFINITE = 5,    /* non-finite input or result */
     HM_ERR_STATE = 6,        /* call out of order (e.g. solve before build) */
     HM_ERR_UNSUPPORTED = 7,  /* size or option outside what this build supports */
-    HM_ERR_IR = 8            /* iterative refinement did not reach ir_tol */
+    HM_ERR_IR = 8,           /* iterative refinement did not reach ir_tol */
+    HM_ERR_TIMEOUT = 9       /* a device-side wait of a kernel's own pipeline gave up (bounded waits) */
 };
 
 /* ---- sketch sources for the randomized SVD (compression.h:78) ---- */
@@ -241,16 +242,52 @@ HM_API int hm_gradients(hm_handle* h, const double* x, int ldx, const double* la
 HM_API int hm_get_gradient(const hm_handle* h, int node, int which, double* out, int* rows, int* cols);
 
 /* multiply(x) like hm_multiply_device, but allocating no device memory: for callers
- * that may not call cudaMalloc when they multiply (a loop being captured into a CUDA
- * graph, a real-time or callback thread, an application that owns all device memory
+ * that may not call cudaMalloc when they multiply (a real-time or callback thread that
+ * must not block in the device allocator, an application that owns all device memory
  * through its own pool).  No counterpart in the reference.  Intermediates and launch
  * tables live in one fixed 32 MiB device array that every GPU loading the library
- * keeps until exit; operators needing more fail with HM_ERR_UNSUPPORTED.  The first
- * call on a device looks up that array's device address (make it before any stream
- * capture).  All calls share the array: calls whose work overlaps on the GPU race.
- * dx/dy: device, N x nrhs, column-major, on the handle's stream. */
+ * keeps until exit; operators needing more fail with HM_ERR_UNSUPPORTED.  The operator's
+ * device must be current (HM_ERR_ARG otherwise); the first call on a device looks up
+ * that array's device address.  All calls share the array: calls whose work overlaps on
+ * the GPU race.  Each call copies its launch tables from host memory, which waits for
+ * the work already queued on the stream.  dx/dy: device, N x nrhs, column-major, on the
+ * handle's stream. */
 HM_API int hm_multiply_device_noalloc(hm_handle* h, const double* dx, int nrhs, int ldx, double* dy,
                                       int ldy);
+
+/* ---- dense building blocks on the device ----
+ * Kernel choice for the batched GEMMs. */
+enum {
+    HM_GEMM_AUTO = 0,          /* the library's own rules (tile table, tensor-core eligibility) */
+    HM_GEMM_TENSOR_CORES = 1,  /* FP32: the tcgen05 kernel (TF32 hi/lo split, FP32 accumulation);
+                                  FP64: the FP64 MMA kernel.  HM_ERR_UNSUPPORTED when the operands
+                                  are not 16-byte aligned with leading dimensions a multiple of 4 */
+    HM_GEMM_FMA = 2,           /* the warp-tiled FMA kernel */
+    HM_GEMM_TEST_STALL = 16    /* or-ed with HM_GEMM_TENSOR_CORES (FP32): exercises the timeout path.
+                                  The kernel's producer issues no copy, so its pipeline waits run out
+                                  (after ~0.5 ms) with nothing in flight and the call returns
+                                  HM_ERR_TIMEOUT; C is left unspecified.  For tests. */
+};
+/* Matrix::operator* (matrix.h:93-104: C = A * B through dgemm_) for `count` independent
+ * products in one launch: C_i = alpha op(A_i) op(B_i) + beta C_i, C_i m_i x n_i, inner
+ * dimension k_i, op = transpose when opA / opB is 1.  Size and pointer arrays are host
+ * memory; the matrices are device memory, column-major.  ksplit: 0 lets the library split
+ * long inner dimensions across CTAs (partial products added atomically; only when beta is
+ * 0 or 1), 1 keeps one CTA per output tile.  Runs on the handle's stream; synchronises. */
+HM_API int hm_gemm_batched_f32_device(hm_handle* h, int count, const int* m, const int* n, const int* k,
+                                      float alpha, const float* const* A, const int* lda, int opA,
+                                      const float* const* B, const int* ldb, int opB, float beta,
+                                      float* const* C, const int* ldc, int ksplit, int flags);
+HM_API int hm_gemm_batched_f64_device(hm_handle* h, int count, const int* m, const int* n, const int* k,
+                                      double alpha, const double* const* A, const int* lda, int opA,
+                                      const double* const* B, const int* ldb, int opB, double beta,
+                                      double* const* C, const int* ldc, int ksplit, int flags);
+/* Matrix::inverse (matrix.h:133-149: getrf + getri) for `count` square FP64 device matrices:
+ * X_i = inv(A_i), n_i <= 16384, with partial pivoting at every size (Gauss-Jordan up to 64,
+ * block Gauss-Jordan with panel pivoting above).  X may alias A.  HM_ERR_SINGULAR when a
+ * pivot is zero or non-finite.  Runs on the handle's stream; synchronises. */
+HM_API int hm_inverse_batched_device(hm_handle* h, int count, const int* n, const double* const* A,
+                                     const int* lda, double* const* X, const int* ldx);
 
 /* ---- instrumentation (no counterpart in the reference, which only wall-clocks its
  *      drivers: main_hodlr.cpp:14-24) ---- */

@@ -31,6 +31,10 @@ CASES = {
     "hodlr_single_leaf_50": dict(kind="hodlr", op="gaussian", N=50, leaf=64, tol=1e-8,
                                  rsvd_rank=64, seed=16, xseed=6, nrhs=1, h=0.05, shift=1e-2,
                                  pseed=7),
+    # non-symmetric leaves of 256 whose leading 128 x 128 block is zero (singular) while the
+    # leaf is regular: getrf's partial pivoting handles them (matrix.h:120-131)
+    "hodlr_pivot_leaf_1024": dict(kind="hodlr", op="pivot_leaf", N=1024, leaf=256, tol=1e-10,
+                                  rsvd_rank=32, seed=17, xseed=9, nrhs=2, pseed=11),
     # HSS: configuration-2 operator (Gaussian h = 0.05 + 1e-2 I, sorted uniform points)
     "hss_gauss_512": dict(kind="hss", op="gaussian", N=512, leaf=64, tol=1e-10, rsvd_rank=64,
                           seed=21, xseed=7, nrhs=1, h=0.05, shift=1e-2, pseed=2),
@@ -62,6 +66,19 @@ def make_matrix(c) -> np.ndarray:
         return A
     if c["op"] == "gaussian":
         return O.gaussian_matrix(points(c, N), c["h"], c["shift"])
+    if c["op"] == "pivot_leaf":
+        # smooth off-diagonal part (the reference driver's kernel), leaf diagonal blocks
+        # [[0, B], [C, E]]: singular leading half, regular leaf
+        x = np.arange(N) / (N - 1)
+        A = 1.0 / (x[:, None] + x[None, :] + 1.0)
+        rng = np.random.default_rng(c["pseed"])
+        L, h = c["leaf"], c["leaf"] // 2
+        for s0 in range(0, N, L):
+            B = 2.0 * np.eye(h) + 0.3 * rng.standard_normal((h, h)) / np.sqrt(h)
+            C = 2.0 * np.eye(h) + 0.3 * rng.standard_normal((h, h)) / np.sqrt(h)
+            E = 0.3 * rng.standard_normal((h, h)) / np.sqrt(h)
+            A[s0:s0 + L, s0:s0 + L] = np.block([[np.zeros((h, h)), B], [C, E]])
+        return A
     if c["op"] == "coulomb":
         return O.coulomb_matrix(points(c, N))
     raise ValueError(c["op"])

@@ -6,7 +6,8 @@ injection) on seeded inputs and stores what the reference computed: tree layout 
 ranks, multiply(x), and solve(b).  The reference has no test vectors of its own
 (its drivers only print errors), so these files are its known answers.
 
-    python tests/golden/make_golden.py        # rewrites tests/golden/*.npz
+    python tests/golden/make_golden.py           # rewrites tests/golden/*.npz
+    python tests/golden/make_golden.py NAME ...  # only the named cases
 
 Inputs are regenerated from the parameters stored in each file (``cases.py``), so
 only outputs are stored.
@@ -27,8 +28,10 @@ import ref  # noqa: E402
 from cases import CASES, make_matrix, make_vectors  # noqa: E402
 
 
-def main():
+def main(names=None):
     for name, c in CASES.items():
+        if names and name not in names:
+            continue
         A = make_matrix(c)
         N = A.shape[0]
         x, b = make_vectors(c, N)
@@ -53,4 +56,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

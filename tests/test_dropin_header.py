@@ -5,7 +5,8 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_INC = os.path.join(os.environ.get("HMAT_REFERENCE", "/root/reference"), "include")
+REF_INC = os.path.join(os.environ.get("HMAT_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference")),
+                       "include")
 
 
 def test_dropin_header_compiles(tmp_path):

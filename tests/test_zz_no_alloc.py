@@ -1,6 +1,6 @@
 """hm_multiply_device_noalloc: the multiply for callers that may not allocate device
-memory when they multiply (e.g. inside a CUDA-graph capture, a real-time thread, or an
-application whose memory pool owns the whole GPU).  It keeps its intermediates in a
+memory when they multiply (a real-time or callback thread that must not block in the
+allocator, or an application whose memory pool owns the whole GPU).  It keeps its intermediates in a
 fixed device array instead of allocating, and must give the same result as
 hm_multiply_device.  This file is collected last so that a failure here cannot hide
 the other tests' results."""
