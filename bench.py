@@ -87,35 +87,56 @@ def parse():
 # --------------------------------------------------------------------------------------
 # CPU reference (oracle/_ref: the reference's OpenMP HODLR solve)
 # --------------------------------------------------------------------------------------
-def reference_sample(n_small=(4096, 8192), nrhs=64, leaf=256, rank=96, reps=1):
-    """Time HODLRMatrixOMP::solve (the reference has no separate factor: its solve is
-    factor+solve) on Coulomb problems of the workload's kind at CPU-feasible sizes, fit
-    t ~ N^alpha and scale to the benchmark N.  Returns dict."""
-    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")  # run_tests.sh:7
+REF_FIT_SIZES = (2048, 4096, 8192)   # HODLRMatrixOMP::solve sizes timed for the N-scaling fit
+REF_N = 8192                         # largest measured size: the like-for-like point
+
+
+def reference_problem(N, leaf, rank, nrhs):
+    """The headline's operator at a CPU-feasible size: Coulomb 2-D on Morton-sorted points
+    (seed 3), dense A, b ~ N(0,1) (seed 3), and the reference's tree/compression built by its
+    serial HODLRMatrix::build_from_dense (hodlr_routines.h:20-63)."""
     import hmat_oracle as O
     import ref
+    A = O.coulomb_matrix(morton_points(N, 3))
+    R = ref.RefHODLR(A, leaf, 1e-10, rank, seed=0)
+    b = np.random.default_rng(3).standard_normal((N, nrhs))
+    return A, R, b
+
+
+def reference_points(sizes=REF_FIT_SIZES, nrhs=64, leaf=256, rank=96):
+    """Measured HODLRMatrixOMP::solve times (the reference has no separate factor: its
+    solve is factor+solve, hodlr_routines_omp.h:137-240) at CPU-feasible sizes, one warm
+    call then the minimum of two timed calls."""
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")  # run_tests.sh:7
+    import ref
     out = {}
-    for N in n_small:
-        p = morton_points(N, 3)
-        A = O.coulomb_matrix(p)
-        R = ref.RefHODLR(A, leaf, 1e-10, rank, seed=0)
-        b = np.random.default_rng(3).standard_normal((N, nrhs))
+    for N in sizes:
+        A, R, b = reference_problem(N, leaf, rank, nrhs)
+        R.solve_omp(b)
         ts = []
-        for _ in range(reps):
+        for _ in range(2):
             t0 = time.perf_counter()
             R.solve_omp(b)
             ts.append(time.perf_counter() - t0)
         out[N] = min(ts)
         R.close()
-    threads = ref.lib().hmref_omp_max_threads()
-    return out, threads
+    return out, ref.lib().hmref_omp_max_threads()
 
 
-def extrapolate(times: dict, N: int):
-    ns = sorted(times)
-    a = np.log(times[ns[-1]] / times[ns[0]]) / np.log(ns[-1] / ns[0])
-    a = float(min(max(a, 1.5), 2.5))
-    return times[ns[-1]] * (N / ns[-1]) ** a, a
+def fit_power_law(times: dict):
+    """Least-squares fit t = c N^alpha over the measured points (alpha not clamped)."""
+    ns = np.array(sorted(times), dtype=float)
+    ts = np.array([times[int(n)] for n in ns])
+    alpha, logc = np.polyfit(np.log(ns), np.log(ts), 1)
+    return float(alpha), float(np.exp(logc))
+
+
+def extrapolation(times: dict, N: int, nrhs: int):
+    alpha, c = fit_power_law(times)
+    t = c * N ** alpha
+    return {"N": N, "extrapolated": True, "rhs_per_s": nrhs / t, "ms_per_step": t * 1e3, "alpha": alpha,
+            "fit_points_s": {str(k): round(v, 4) for k, v in sorted(times.items())},
+            "why": f"a dense FP64 A at N={N} is {8 * N * N / 2**30:.0f} GiB: the reference cannot build it"}
 
 
 def run_reference(args):
@@ -127,41 +148,38 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent)"}))
         return
     os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
-    # alpha from two sample sizes, then timed steps at the larger sample
-    times, threads = reference_sample()
-    t_full, alpha = extrapolate(times, args.n)
-    import hmat_oracle as O
-    import ref as R_
-    Ns = 8192
-    A = O.coulomb_matrix(morton_points(Ns, 3))
-    R = R_.RefHODLR(A, args.leaf, 1e-10, args.rank, seed=0)
-    b = np.random.default_rng(3).standard_normal((Ns, args.nrhs))
+    times, threads = reference_points(nrhs=args.nrhs, leaf=args.leaf, rank=args.rank)
+    # timed steps at the largest measured size, on that size's own problem
+    A, R, b = reference_problem(REF_N, args.leaf, args.rank, args.nrhs)
     for _ in range(args.warmup):
         R.solve_omp(b)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        R.solve_omp(b)
+        x = R.solve_omp(b)
     per = (time.perf_counter() - t0) / args.steps
+    resid = float((np.linalg.norm(b - A @ x, axis=0) / np.linalg.norm(b, axis=0)).max())
     R.close()
-    t_step_full = per * (args.n / Ns) ** alpha
-    v = args.nrhs / t_step_full
-    sample = (f"HODLRMatrixOMP::solve, 64 RHS, Coulomb 2-D N={Ns} leaf {args.leaf} rsvd_rank {args.rank} "
-              f"(measured {per:.3f} s/step), scaled to N={args.n} by the measured N^{alpha:.2f} law "
-              f"(sizes {sorted(times)})")
+    v = args.nrhs / per
+    sample = (f"HODLRMatrixOMP::solve (factor+solve), {args.nrhs} RHS, Coulomb 2-D N={REF_N} leaf {args.leaf} "
+              f"rsvd_rank {args.rank}, {threads} OpenMP threads, OPENBLAS_NUM_THREADS=1: measured {per:.3f} s/step")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step_full * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": workload_config(args),
+        "data": "synthetic", "config": workload_config(args, N=REF_N),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "measured_at_N": REF_N,
+        "rel_residual_vs_dense_A": resid,
+        "extrapolated": extrapolation(times, args.n, args.nrhs),
     }))
 
 
-def workload_config(args):
+def workload_config(args, N=None):
+    N = args.n if N is None else N
     return {
-        "workload": f"hodlr_coulomb2d_N{args.n}_leaf{args.leaf}_rank{args.rank}_nrhs{args.nrhs}",
-        "N": args.n, "leaf": args.leaf, "max_rank": args.rank, "sketch_width": args.rank + 10,
+        "workload": f"hodlr_coulomb2d_N{N}_leaf{args.leaf}_rank{args.rank}_nrhs{args.nrhs}",
+        "N": N, "leaf": args.leaf, "max_rank": args.rank, "sketch_width": args.rank + 10,
         "nrhs": args.nrhs, "kernel": "1/(|p_i-p_j|+1e-3)+4*delta_ij, p~U[0,1]^2 seed 3, Morton order",
         "precision": "mixed: FP32 factor/solve sweeps, FP64 leaf+capacitance inverses, FP64 residual refinement",
         "ir_tol": 1e-10,
@@ -329,6 +347,7 @@ def run_ours(args):
     clocks = clk.stop()
     launches = (H.launch_count() - launches0) // max(1, args.steps)
     mixed_resid, mixed_iters = st.rel_residual, st.ir_iters
+    x_mixed = x.clone()
     # separate factor / solve split
     ms_factor, _ = timed(max(1, args.steps // 2), h.factor)
     ms_solve, _ = timed(max(1, args.steps // 2),
@@ -355,6 +374,14 @@ def run_ours(args):
     h.multiply_device(x.data_ptr(), s, N, y.data_ptr(), N)
     fp64_resid = float(((b - y).norm(dim=1) / b.norm(dim=1)).max())
     ms_f64_factor, _ = timed(max(1, args.steps // 2), h.factor)
+    x_fp64 = x.clone()
+
+    # ---- error against the exact kernel operator (generated FP64 entries, outside timing) ----
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    exact_mixed = float(h.residual_exact(b.data_ptr(), x_mixed.data_ptr(), s, N).max())
+    exact_fp64 = float(h.residual_exact(b.data_ptr(), x_fp64.data_ptr(), s, N).max())
+    t_exact = (time.perf_counter() - t0) / 2
 
     # ---- one profiled mixed step: per-kernel CUDA-event times ----
     h.set_precision(H.MIXED)
@@ -371,9 +398,14 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic", "config": workload_config(args),
         "mixed": {"ms_factor": ms_factor, "ms_solve": ms_solve, "ir_iters": mixed_iters,
-                  "rel_residual": mixed_resid},
+                  "rel_residual": mixed_resid, "rel_residual_vs_exact_A": exact_mixed},
         "fp64": {"ms_per_step": ms_fp64, "ms_factor": ms_f64_factor, "rhs_per_s": world * s / (ms_fp64 / 1e3),
-                 "rel_residual": fp64_resid},
+                 "rel_residual": fp64_resid, "rel_residual_vs_exact_A": exact_fp64},
+        "residual_definitions": {
+            "rel_residual": "max_j ||b_j - A~ x_j|| / ||b_j||, A~ the FP64 compressed operator (the refinement target)",
+            "rel_residual_vs_exact_A": "max_j ||b_j - A x_j|| / ||b_j||, A the exact Coulomb matrix, entries generated "
+                                       f"in FP64 on the device ({t_exact:.2f} s per evaluation, outside the timing); "
+                                       "bounded by the rank-96 compression error, not by the solve"},
         "mixed_over_fp64": ms_fp64 / ms_mixed,
         "build_s": t_build,
         "ranks": {"min": int(ranks.min()), "median": float(np.median(ranks)), "max": int(ranks.max())},
@@ -384,14 +416,21 @@ def run_ours(args):
         "profile": {k: {"launches": v[0], "ms": v[1], "flops": v[2], "bytes": v[3]} for k, v in prof.items()},
     }
     out["roofline"] = roofline(prof)
+    h.close()
+    if rank == 0:
+        out["like_for_like"] = like_for_like(args, stream)
     if rank == 0 and not args.no_cpu_baseline:
         try:
-            times, threads = reference_sample(reps=1)
-            t_full, alpha = extrapolate(times, N)
+            times, threads = reference_points(nrhs=s, leaf=args.leaf, rank=args.rank)
+            t = times[REF_N]
             out["cpu_baseline"] = {
-                "value": s / t_full, "unit": UNIT, "cores": threads, "kind": "reference",
-                "sample": f"HODLRMatrixOMP::solve (factor+solve), 64 RHS, Coulomb 2-D N in {sorted(times)} "
-                          f"(times {[round(times[k], 3) for k in sorted(times)]} s), scaled to N={N} by N^{alpha:.2f}"}
+                "value": s / t, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"HODLRMatrixOMP::solve (factor+solve), {s} RHS, Coulomb 2-D N={REF_N} leaf {args.leaf} "
+                          f"rsvd_rank {args.rank}: measured {t:.3f} s (the workload at N={N} is out of the "
+                          f"reference's reach: dense A of {8 * N * N / 2**30:.0f} GiB)",
+                "extrapolated": extrapolation(times, N, s)}
+            out["like_for_like"]["reference_rhs_per_s"] = s / t
+            out["like_for_like"]["mixed_over_reference"] = out["like_for_like"]["mixed_rhs_per_s"] * t / s
         except Exception as e:  # the oracle library may be absent
             out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                                    "sample": f"unavailable: {e}"}
@@ -399,6 +438,43 @@ def run_ours(args):
         print(json.dumps(out))
     if world > 1:
         dist.destroy_process_group()
+
+
+def like_for_like(args, stream):
+    """The GPU path on the reference arm's measured problem: N = REF_N, same kernel, points,
+    leaf, rank cap and right-hand-side count; factor+solve per step, mixed and FP64, device
+    CUDA events (inputs resident), plus the exact-operator residual."""
+    import torch
+    import hmat_b200 as H
+    N, s = REF_N, args.nrhs
+    pts = morton_points(N, 3)
+    h = H.HODLRMatrix(1e-10, rsvd_rank=args.rank, oversample=10, max_rank=args.rank,
+                      sketch=H.SKETCH_DEVICE_NORMAL, seed=0, precision=H.MIXED, ir_tol=1e-10, ir_max_iter=30)
+    h.set_stream(stream.cuda_stream)
+    h.build_from_kernel(H.KERNEL_COULOMB, pts, [1e-3, 4.0], args.leaf)
+    b = torch.from_numpy(np.random.default_rng(3).standard_normal((N, s)).T.copy()).cuda()
+    x = torch.empty_like(b)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"N": N, "leaf": args.leaf, "max_rank": args.rank, "nrhs": s}
+    for name, prec in (("mixed", H.MIXED), ("fp64", H.FP64)):
+        h.set_precision(prec)
+        for _ in range(3):
+            h.factor()
+            h.solve_device(b.data_ptr(), s, N, x.data_ptr(), N)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        K = 20
+        for _ in range(K):
+            h.factor()
+            h.solve_device(b.data_ptr(), s, N, x.data_ptr(), N)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / K
+        out[name + "_ms_per_step"] = ms
+        out[name + "_rhs_per_s"] = s / (ms / 1e3)
+        out[name + "_rel_residual_vs_exact_A"] = float(h.residual_exact(b.data_ptr(), x.data_ptr(), s, N).max())
+    h.close()
+    return out
 
 
 def run_batched(args):
@@ -488,14 +564,17 @@ def run_batched(args):
     }))
 
 
-# DRAM bytes / algorithmic bytes per step label, measured by ncu on the same step at
-# N = 65536 (profiles/traffic_factor_solve_coulomb_n65536.md); traffic grows with the
-# units processed, so the N = 2^18 traffic is the algorithmic bytes times this ratio.
-TRAFFIC_RATIO = {
-    "gemm_f32:factor.update_correct": 0.61, "gemm_f64:matvec.expand": 0.73, "gemm_f64:matvec.project": 0.79,
-    "tc_tf32x4:factor.update_project": 0.65, "gemm_f32:solve.correct": 0.72, "gemm_f32:solve.project": 0.98,
-    "tc_tf32x4:factor.leaf_apply": 0.45, "gemm_f32:factor.K": 0.98, "gauss_jordan_inverse": 0.51,
-}
+# Compute ceilings (TFLOP/s) of the pipes the hot steps run on.  Only the HBM copy
+# bandwidth and the bf16 tensor-core rate are measured on this hardware
+# (MEASURED_PEAKS.json); the others are derived from the bf16 rate or nominal B200 figures.
+def pipe_ceiling(name: str, bf16_tflops: float):
+    if name.startswith("tc_"):           # tcgen05 kind::tf32, TF32 hi/lo products per k-step
+        return bf16_tflops / 2 / 4, "tensor", "TF32 tensor rate = measured bf16 / 2, over 4 products per k-step"
+    if name.startswith("gemm_f32"):      # FP32 FFMA on the CUDA cores
+        return 74.0, "fma", "nominal FP32 FMA rate (not measured)"
+    if "f64" in name or name.startswith("gauss_jordan") or name.startswith("panel"):
+        return 37.0, "fma", "nominal FP64 rate (DFMA and DMMA; not measured)"
+    return None, "hbm", ""
 
 
 def roofline(prof: dict):
@@ -505,16 +584,26 @@ def roofline(prof: dict):
         src = "measured"
     except Exception:
         src = "fallback"
-    hbm = peaks.get("hbm_gbs", 6650.0)
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    bf16 = float(peaks.get("bf16_tflops", 1590.0))
     name, (n, ms, fl, by) = max(prof.items(), key=lambda kv: kv[1][1])
-    achieved = by / (ms / 1e3) / 1e9 if ms > 0 else 0.0
-    ratio = TRAFFIC_RATIO.get(name)
-    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "traffic": by * ratio if ratio else None, "launches": n,
-            "traffic_source": "ncu dram bytes at N=65536 scaled by units (profiles/traffic_factor_solve_coulomb_n65536.md)",
-            "peak_source": src, "achieved_tflops": fl / (ms / 1e3) / 1e12 if ms > 0 else 0.0,
-            "note": "algorithmic bytes of the step's launches / their CUDA-event time; an FMA-pipe GEMM "
-                    "(24-48 flop/byte), so the FMA pipe, not HBM, bounds it: see achieved_tflops"}
+    sec = ms / 1e3 if ms > 0 else float("inf")
+    ceiling, pipe, note = pipe_ceiling(name, bf16)
+    ai = fl / by if by > 0 else 0.0
+    t_hbm = by / (hbm * 1e9)
+    t_pipe = fl / (ceiling * 1e12) if ceiling else 0.0
+    base = {"kernel": name, "launches": n, "ms": ms, "flop_per_byte": ai, "peak_source": src,
+            "achieved_gbs": by / sec / 1e9, "achieved_tflops": fl / sec / 1e12,
+            "traffic": None,
+            "traffic_note": "DRAM bytes come from ncu captures of this kernel (committed summaries), not from this run"}
+    if t_hbm >= t_pipe:   # bytes / HBM bandwidth is the longer bound: HBM-bound
+        base.update({"bound": "hbm", "achieved": by / sec / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": by / sec / 1e9 / hbm})
+    else:                 # the pipe's flop rate is the longer bound
+        base.update({"bound": pipe, "achieved": fl / sec / 1e12, "peak": ceiling, "unit": "TFLOP/s",
+                     "frac": fl / sec / 1e12 / ceiling, "peak_note": note,
+                     "hbm_frac": by / sec / 1e9 / hbm})
+    return base
 
 
 def run_hss(args):

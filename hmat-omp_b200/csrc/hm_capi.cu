@@ -296,6 +296,10 @@ int hm_solve_exact_device(hm_handle* h, const double* db, int nrhs, int ldb, dou
     return guard(h, [&] { built(h).solve_exact_device(db, nrhs, ldb, dx, ldx, tol, max_iter, st); });
 }
 
+int hm_residual_exact(hm_handle* h, const double* b, int nrhs, int ldb, const double* x, int ldx, double* rel) {
+    return guard(h, [&] { built(h).residual_exact(b, ldb, x, ldx, nrhs, rel); });
+}
+
 int hm_solve_exact(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ldx, double tol, int max_iter,
                    hm_solve_stats* st) {
     return guard(h, [&] {

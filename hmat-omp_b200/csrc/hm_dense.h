@@ -207,6 +207,15 @@ inline bool tensor_cores_allowed(const char* label) {
     return list.find("," + l + ",") != std::string::npos;
 }
 
+// Whether HM_FP32_TENSOR_CORES names this label explicitly (then the tensor-core kernel
+// takes the batch even when its inner dimension is short).
+inline bool tensor_cores_named(const char* label) {
+    const char* e = std::getenv("HM_FP32_TENSOR_CORES");
+    if (!e || !*e || (e[0] == '1' && e[1] == 0) || (e[0] == '0' && e[1] == 0)) return false;
+    const std::string list = std::string(",") + e + ",";
+    return list.find("," + std::string(label) + ",") != std::string::npos;
+}
+
 template <typename T>
 struct GemmStep : Plan::Step {
     GemmBatch<T> batch;
@@ -218,7 +227,7 @@ struct GemmStep : Plan::Step {
         batch.set_tag(lbl);
         label = std::string(sizeof(T) == 8 ? "gemm_f64:" : "gemm_f32:") + lbl;
         label_tc = std::string("tc_tf32x4:") + lbl;
-        batch.allow_tensor_cores(tensor_cores_allowed(lbl));
+        batch.allow_tensor_cores(tensor_cores_allowed(lbl), tensor_cores_named(lbl));
     }
     void run(cudaStream_t s, int* st) const override { batch.launch(s, gp, st); }
     const char* name() const override {

@@ -1835,6 +1835,44 @@ void Engine::solve_exact_device(const double* db, int s, int ldb, double* dx, in
     }
 }
 
+// rel[j] = ||b_j - A x_j|| / ||b_j|| with A the exact kernel operator, its entries
+// generated inside the batched FP64 product (2 N^2 s flops; A never stored).
+void Engine::residual_exact(const double* db, int ldb, const double* dx, int ldx, int s, double* rel) {
+    HM_CHECK(built_, HM_ERR_STATE, "residual_exact before build");
+    HM_CHECK(gen_ != GEN_DENSE && sys_N_.size() == 1, HM_ERR_STATE,
+             "residual_exact needs a single operator built from a kernel (hm_*_build_from_kernel)");
+    HM_CHECK(s >= 1 && ldb >= N_ && ldx >= N_ && db && dx && rel, HM_ERR_ARG, "residual_exact: bad arguments");
+    const size_t n = (size_t)N_ * s;
+    if (s > ex_cols_) {
+        exB_.alloc(n);
+        exX_.alloc(n);
+        exR_.alloc(n);
+        exD_.alloc(n);
+        exNorm_.alloc(2 * (size_t)s);
+        ex_cols_ = s;
+        exact_plans_.clear();
+    }
+    cudaStream_t q = stream_;
+    HM_CUDA(cudaMemcpy2DAsync(exB_.p, (size_t)N_ * sizeof(double), db, (size_t)ldb * sizeof(double),
+                              (size_t)N_ * sizeof(double), s, cudaMemcpyDefault, q));
+    HM_CUDA(cudaMemcpy2DAsync(exX_.p, (size_t)N_ * sizeof(double), dx, (size_t)ldx * sizeof(double),
+                              (size_t)N_ * sizeof(double), s, cudaMemcpyDefault, q));
+    exact_plan(s).run(q, dstatus.p);   // exR = A x
+    HM_CUDA(cudaMemsetAsync(exNorm_.p, 0, 2 * (size_t)s * sizeof(double), q));
+    residual_kernel<<<dim3(std::min(64, ceil_div(N_, 256)), s), 256, 0, q>>>(exB_.p, exR_.p, nullptr, N_, s,
+                                                                           exNorm_.p, exNorm_.p + s);
+    HM_CUDA(cudaGetLastError());
+    count_launch();
+    std::vector<double> hn(2 * (size_t)s);
+    HM_CUDA(cudaMemcpyAsync(hn.data(), exNorm_.p, 2 * s * sizeof(double), cudaMemcpyDeviceToHost, q));
+    HM_CUDA(cudaStreamSynchronize(q));
+    check_status("residual_exact");
+    for (int j = 0; j < s; ++j) {
+        const double den = std::sqrt(hn[s + j]);
+        rel[j] = den > 0 ? std::sqrt(hn[j]) / den : std::sqrt(hn[j]);
+    }
+}
+
 void Engine::ensure_copy_stream() {
     if (copy_stream_) return;
     cudaStream_t cs = nullptr;

@@ -104,6 +104,8 @@ class Engine {
     // refinement against the exact kernel operator (matrix-free builds)
     void solve_exact_device(const double* db, int s, int ldb, double* dx, int ldx, double tol, int max_iter,
                             hm_solve_stats* st);
+    // per-column ||b - A x|| / ||b|| against the exact kernel operator (matrix-free builds)
+    void residual_exact(const double* db, int ldb, const double* dx, int ldx, int s, double* rel);
     // adjoint solve and gradient accumulation
     void solve_transpose_device(const double* dg, int s, int ldg, double* dl, int ldl);
     void gradients(const double* dx, int ldx, const double* dl, int ldl, int s, double* dparams);

@@ -723,7 +723,7 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
             HM_CHECK(use_tc_, HM_ERR_UNSUPPORTED,
                      "tensor-core GEMM: operands not TMA-addressable (16-byte aligned, ld a multiple of 4)");
         } else if (kernel_mode_ == 0 && pipe_bn_ && tc_allowed_ && !has_chains_ && (!have_tuned || tuned.tc)) {
-            finalize_tc(s);
+            finalize_tc(s, tc_any_k_);
         }
     }
     if (!hz_.empty()) {

@@ -133,7 +133,11 @@ class GemmBatch {
     // role waits give up after ~0.5 ms, so the launch sets ST_TIMEOUT with nothing in flight.
     void set_test_stall(bool on) { tc_stall_ = on; }
     // whether finalize may put this (FP32) batch on the tensor cores
-    void allow_tensor_cores(bool on) { tc_allowed_ = on; }
+    // any_k: also when the inner dimension is short (fewer than 4 k-blocks per tile)
+    void allow_tensor_cores(bool on, bool any_k = false) {
+        tc_allowed_ = on;
+        tc_any_k_ = any_k;
+    }
     // status: device status word for the tensor-core kernel's bounded waits (may be null
     // for batches that never take that kernel)
     void launch(cudaStream_t s, const GenParams& gp = GenParams(), int* status = nullptr) const;
@@ -177,7 +181,7 @@ class GemmBatch {
     bool use_dmma_ = false;              // FP64 batch on the FP64 MMA kernel (same tables)
     DBuf<int> tmap_;                     // its tile -> problem table
     // FP32 batches with long k on the tensor cores: tile count, tables, tensor maps
-    bool use_tc_ = false, tc_allowed_ = true, tc_stall_ = false;
+    bool use_tc_ = false, tc_allowed_ = true, tc_stall_ = false, tc_any_k_ = false;
     int kernel_mode_ = 0;
     int tc_tiles_ = 0;
     DBuf<GemmDesc<T>> tcd_;

@@ -92,6 +92,7 @@ def load() -> C.CDLL:
                                  C.POINTER(SolveStats)]
     L.hm_solve_exact_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_double,
                                         C.c_int, C.POINTER(SolveStats)]
+    L.hm_residual_exact.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, _dp]
     L.hm_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                   C.POINTER(SolveStats)]
     L.hm_batch_build_from_kernel.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _ip, _dp, C.c_int]
@@ -301,6 +302,20 @@ class _Handle:
                                            C.byref(st)))
         out = X.ravel() if vec else X
         return (out, st) if stats else out
+
+    def residual_exact(self, b, x, nrhs: int | None = None, ld: int | None = None) -> np.ndarray:
+        """Per-column ||b - A x|| / ||b|| against the exact kernel operator (matrix-free
+        builds).  b, x: numpy arrays (N or N x nrhs) or device pointers with nrhs and ld."""
+        if isinstance(b, np.ndarray):
+            B = np.asfortranarray(np.asarray(b, dtype=np.float64).reshape(self.N, -1))
+            X = np.asfortranarray(np.asarray(x, dtype=np.float64).reshape(self.N, -1))
+            rel = np.zeros(B.shape[1])
+            self._check(self._L.hm_residual_exact(self._h, B.ctypes.data, B.shape[1], self.N, X.ctypes.data,
+                                                  self.N, _d(rel)))
+            return rel
+        rel = np.zeros(nrhs)
+        self._check(self._L.hm_residual_exact(self._h, C.c_void_p(b), nrhs, ld, C.c_void_p(x), ld, _d(rel)))
+        return rel
 
     def solve_transpose(self, g: np.ndarray) -> np.ndarray:
         """lam = A^{-T} g (the adjoint solve)."""

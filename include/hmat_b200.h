@@ -225,6 +225,14 @@ HM_API int hm_solve_exact(hm_handle* h, const double* b, int nrhs, int ldb, doub
 HM_API int hm_solve_exact_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx,
                                  double tol, int max_iter, hm_solve_stats* stats);
 
+/* rel[j] = ||b_j - A x_j|| / ||b_j|| (j < nrhs, rel: host) with A the exact kernel matrix of an
+ * operator built by hm_*_build_from_kernel, its entries generated on the device (2 N^2 nrhs
+ * flops; A is never stored): the error of any solution against the exact operator rather
+ * than the compressed one.  The reference's drivers print this quantity against their dense
+ * A (main_hodlr.cpp:26-35).  Host or device b/x; synchronises. */
+HM_API int hm_residual_exact(hm_handle* h, const double* b, int nrhs, int ldb, const double* x, int ldx,
+                             double* rel);
+
 /* ---- adjoint (no counterpart in the reference) ----
  * A^T lam = g with the FP64 factorization run transposed in reverse level order
  * (the transpose of the Woodbury recursion of hodlr_routines.h:112-175); factors in FP64

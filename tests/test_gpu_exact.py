@@ -74,3 +74,16 @@ def test_dense_builds_are_refused():
     with pytest.raises(H.HmError) as e:
         m.solve_exact(np.ones(1024))
     assert e.value.code == H.HM_ERR_STATE
+
+
+def test_residual_exact_matches_dense_residual():
+    """hm_residual_exact (generated entries, A never stored) against the host residual
+    with the dense kernel matrix."""
+    N = 2048
+    m, A = _coulomb(N, H.FP64)
+    b = np.random.default_rng(7).standard_normal((N, 5))
+    x = m.solve(b)
+    rel = m.residual_exact(b, x)
+    ref = np.linalg.norm(b - A @ x, axis=0) / np.linalg.norm(b, axis=0)
+    assert np.allclose(rel, ref, rtol=1e-6, atol=1e-15)
+    assert rel.max() > 1e-9   # the compressed operator is not A: a visible residual
