@@ -623,25 +623,27 @@ static int gj_max() {
 
 // ---------------------------------------------------------------------------------
 // Block Gauss-Jordan with partial pivoting by panels (inverses above the Gauss-Jordan
-// threshold).  On a work copy W of A, for each panel of w columns K = [k0, k0 + kw):
-//   1. panel_pivot_kernel: Gaussian elimination with partial pivoting on the panel
-//      W[k0:, K] (in shared memory) chooses kw pivot rows, which are swapped into rows K
-//      across all n columns of W; the swaps are recorded in ipiv.
-//   2. Dinv = inv(W[K, K]) (Gauss-Jordan kernel);
-//   3. T = Dinv W[K, R], Z = -W[O, K] Dinv   (O, R: the rows / columns outside K);
-//   4. W[O, R] += Z W[K, R];
-//   5. W[K, K] = Dinv, W[K, R] = T, W[O, K] = Z.
-// This is the in-place (compact) Gauss-Jordan sweep a column block at a time, so
-// column c of W ends as column where[c] of inv(A), where[] being the row swaps applied
-// in order to the identity permutation (unscramble_kernel).  The pivot rows are those of
-// LU with partial pivoting of each panel, so the inverted pivot blocks W[K, K] are as
-// well conditioned as LU's diagonal blocks: a leaf whose leading block is singular while
-// the leaf is not (which getrf handles, matrix.h:120-131) inverts like any other.
+// threshold), in place on a column-major work copy W of A.  It is the sweep of the
+// transposed problem: pivots are chosen among columns, so every exchange moves whole
+// (contiguous) columns.  For each block of w rows K = [k0, k0 + kw), with O the other
+// indices:
+//   1. panel_pivot_kernel: Gaussian elimination with partial pivoting on the transposed
+//      panel W[K, k0:]^T (in shared memory) chooses kw pivot columns, which are swapped
+//      into columns K; the exchanges are recorded in ipiv.
+//   2. PD = inv(W[K, K]) (Gauss-Jordan kernel);
+//   3. T = W[O, K] PD,  Z = -PD W[K, O];
+//   4. W[O, O] += W[O, K] Z;
+//   5. W[K, K] = PD, W[O, K] = T, W[K, O] = Z.
+// At the end row c of W is row where[c] of inv(A), where[] being the exchanges applied in
+// order to the identity permutation (unscramble_kernel).  The pivots are those of LU with
+// partial pivoting of A^T panel by panel, so every inverted block W[K, K] is as well
+// conditioned as LU's diagonal blocks: a leaf whose leading block is singular while the
+// leaf is not (which getrf handles, matrix.h:120-131) inverts like any other.
 // ---------------------------------------------------------------------------------
 struct PanelDesc {
     double* W;
     int ld, n, k0, kw;
-    int* ipiv;    // n entries: row position i was swapped with row ipiv[i]
+    int* ipiv;    // n entries: column position i was exchanged with column ipiv[i]
 };
 
 struct ScatterDesc {
@@ -652,86 +654,157 @@ struct ScatterDesc {
     const int* ipiv;
 };
 
-// Panel width for order n: the (n - k0) x w panel fits in 128 KB of shared memory.
+// Panel width for order n: the padded (n + 1) x w panel fits in 136 KB of shared memory
+// (w = 64 up to n = 271).
 static int bgj_width(int n) {
     int w = 64;
-    while (w > 1 && (size_t)n * w * sizeof(double) > (size_t)128 * 1024) w /= 2;
+    while (w > 1 && (size_t)(n + 1) * w * sizeof(double) > (size_t)136 * 1024) w /= 2;
     return w;
+}
+static size_t panel_smem(int m, int kw) {
+    return (size_t)(m + 1) * kw * sizeof(double) + 2 * (size_t)m * sizeof(int);
 }
 
 __global__ void __launch_bounds__(256) panel_pivot_kernel(const PanelDesc* __restrict__ descs, int* status) {
-    extern __shared__ double pan[];   // m x kw, column-major, ld m
-    __shared__ double red_v[8];
-    __shared__ int red_i[8];
-    __shared__ int piv[64];
-    __shared__ int s_bad;
+    extern __shared__ double sm[];   // panel: (m + 1) x kw column-major (then the move buffer); 2m ints
+    __shared__ double red_v[2][8];
+    __shared__ int red_i[2][8];
+    __shared__ int prow[64];
+    __shared__ int mv_pos[128], mv_src[128];
+    __shared__ int s_bad, s_nmv;
     const PanelDesc d = descs[blockIdx.x];
-    const int m = d.n - d.k0, kw = d.kw, tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5;
+    const int m = d.n - d.k0, kw = d.kw, LDP = m + 1, tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    double* pan = sm;
+    int* at = reinterpret_cast<int*>(sm + (size_t)LDP * kw);
+    int* pos = at + m;
     if (tid == 0) s_bad = 0;
+    // logical panel element (i, j) = W[k0 + j, k0 + i]: rows K of the columns k0.. (contiguous in j)
     for (int e = tid; e < m * kw; e += nt) {
-        const int i = e % m, j = e / m;
-        pan[e] = d.W[(d.k0 + i) + (size_t)(d.k0 + j) * d.ld];
+        const int j = e % kw, i = e / kw;
+        pan[i + (size_t)j * LDP] = d.W[(d.k0 + j) + (size_t)(d.k0 + i) * d.ld];
     }
-    __syncthreads();
-    for (int j = 0; j < kw; ++j) {
-        // pivot: largest |pan[i, j]| over i >= j (ties to the lowest row)
-        double bv = -1.0;
-        int bi = j;
-        for (int i = j + tid; i < m; i += nt) {
-            const double v = fabs(pan[i + (size_t)j * m]);
-            if (v > bv) { bv = v; bi = i; }
-        }
+    // Right-looking elimination without row exchanges: a row chosen as pivot is flagged
+    // (bit k of `used` for row tid + k nt) and left in place.  Each thread updates its own
+    // rows and, in the same pass, offers its best candidate for the next column, so one
+    // barrier per column separates the steps.  Pivot: largest |value|, ties to the lowest
+    // row (the choice of LU with partial pivoting).
+    unsigned long long used = 0;
+    auto offer = [&](double bv, int bi, int buf) {
         for (int off = 16; off > 0; off >>= 1) {
             const double ov = __shfl_down_sync(0xffffffffu, bv, off);
             const int oi = __shfl_down_sync(0xffffffffu, bi, off);
             if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
         }
-        if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
-        __syncthreads();
-        if (tid == 0) {
-            double v = red_v[0];
-            int p = red_i[0];
-            for (int w = 1; w < (nt >> 5); ++w)
-                if (red_v[w] > v || (red_v[w] == v && red_i[w] < p)) { v = red_v[w]; p = red_i[w]; }
-            if (!(v > 0.0) || !isfinite(v)) { s_bad = 1; p = j; }
-            piv[j] = p;
+        if (lane == 0) { red_v[buf][warp] = bv; red_i[buf][warp] = bi; }
+    };
+    auto choose = [&](int buf) {
+        double v = red_v[buf][0];
+        int p = red_i[buf][0];
+        for (int w = 1; w < nw; ++w)
+            if (red_v[buf][w] > v || (red_v[buf][w] == v && red_i[buf][w] < p)) { v = red_v[buf][w]; p = red_i[buf][w]; }
+        return p;
+    };
+    __syncthreads();
+    {
+        double bv = -1.0;
+        int bi = 0x7fffffff;
+        for (int i = tid; i < m; i += nt) {
+            const double v = fabs(pan[i]);
+            if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
         }
-        __syncthreads();
-        const int p = piv[j];
-        if (p != j)
-            for (int c = tid; c < kw; c += nt) {
-                const double t = pan[j + (size_t)c * m];
-                pan[j + (size_t)c * m] = pan[p + (size_t)c * m];
-                pan[p + (size_t)c * m] = t;
+        offer(bv, bi, 0);
+    }
+    __syncthreads();
+    for (int j = 0; j < kw; ++j) {
+        const int p = choose(j & 1);
+        const bool pin = p >= 0 && p < m;   // false only when every candidate was NaN
+        const double pv = pin ? pan[p + (size_t)j * LDP] : 0.0;
+        const bool ok = pin && fabs(pv) > 0.0 && isfinite(pv);
+        if (tid == 0) {
+            prow[j] = p;
+            if (!ok) s_bad = 1;
+        }
+        if (pin && p % nt == tid) used |= 1ull << (p / nt);
+        const double rinv = ok ? 1.0 / pv : 0.0;
+        double bv = -1.0;
+        int bi = 0x7fffffff;
+        for (int k = 0, i = tid; i < m; ++k, i += nt) {
+            if ((used >> k) & 1ull) continue;
+            if (ok) {
+                // 8 columns at a time, every load of a chunk before its stores (the row is
+                // never the pivot row, but the compiler cannot know that)
+                const double l = pan[i + (size_t)j * LDP] * rinv;
+                double* ri = pan + i;
+                const double* rp = pan + p;
+                for (int c0 = j + 1; c0 < kw; c0 += 8) {
+                    double a[8], b[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const int c = c0 + u;
+                        a[u] = c < kw ? ri[(size_t)c * LDP] : 0.0;
+                        b[u] = c < kw ? rp[(size_t)c * LDP] : 0.0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (c0 + u < kw) ri[(size_t)(c0 + u) * LDP] = fma(-l, b[u], a[u]);
+                }
             }
-        __syncthreads();
-        const double pj = pan[j + (size_t)j * m];
-        if (pj != 0.0)
-            for (int i = j + 1 + tid; i < m; i += nt) {
-                const double l = pan[i + (size_t)j * m] / pj;
-                for (int c = j + 1; c < kw; ++c) pan[i + (size_t)c * m] -= l * pan[j + (size_t)c * m];
+            if (j + 1 < kw) {
+                const double v = fabs(pan[i + (size_t)(j + 1) * LDP]);
+                if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
             }
+        }
+        if (j + 1 < kw) offer(bv, bi, (j + 1) & 1);
         __syncthreads();
     }
+    // The pivot rows as the exchange sequence of LU with partial pivoting (position j
+    // exchanged with position ipiv[j]), and as one permutation of the columns k0..n-1:
+    // column k0 + i receives column k0 + at[i]; only the moved ones (at most 2 kw) are listed.
     if (tid == 0) {
         if (s_bad) atomicOr(status, ST_SINGULAR);
-        for (int j = 0; j < kw; ++j) d.ipiv[d.k0 + j] = d.k0 + piv[j];
-    }
-    // the same swaps on the whole rows of W, in order (each thread owns its columns)
-    for (int c = tid; c < d.n; c += nt) {
-        double* col = d.W + (size_t)c * d.ld;
+        for (int i = 0; i < m; ++i) at[i] = pos[i] = i;
         for (int j = 0; j < kw; ++j) {
-            const int a = d.k0 + j, b = d.k0 + piv[j];
-            if (a != b) { const double t = col[a]; col[a] = col[b]; col[b] = t; }
+            const int r = (prow[j] >= 0 && prow[j] < m) ? prow[j] : j;
+            const int q = pos[r] >= j ? pos[r] : j;   // a repeated row (only after a bad pivot) stays put
+            d.ipiv[d.k0 + j] = d.k0 + q;
+            const int a = at[j], b = at[q];
+            at[j] = b; at[q] = a;
+            pos[b] = j; pos[a] = q;
         }
+        int nmv = 0;
+        for (int i = 0; i < m && nmv < 128; ++i)
+            if (at[i] != i) { mv_pos[nmv] = i; mv_src[nmv] = at[i]; ++nmv; }
+        s_nmv = nmv;
+    }
+    __syncthreads();
+    const int nmv = s_nmv;
+    if (nmv == 0) return;
+    // move the columns through shared memory (the panel's space), rc rows at a time: all
+    // reads of a chunk, then all writes (coalesced along the rows)
+    const int rc = min(d.n, (int)(((size_t)LDP * kw) / (size_t)nmv));
+    for (int r0 = 0; r0 < d.n; r0 += rc) {
+        const int rows = min(rc, d.n - r0);
+        for (int e = tid; e < nmv * rows; e += nt) {
+            const int l = e / rows, r = e % rows;
+            pan[(size_t)l * rows + r] = d.W[(r0 + r) + (size_t)(d.k0 + mv_src[l]) * d.ld];
+        }
+        __syncthreads();
+        for (int e = tid; e < nmv * rows; e += nt) {
+            const int l = e / rows, r = e % rows;
+            d.W[(r0 + r) + (size_t)(d.k0 + mv_pos[l]) * d.ld] = pan[(size_t)l * rows + r];
+        }
+        __syncthreads();
     }
 }
 
-// X[:, where[c]] = W[:, c], where[] = the swaps of ipiv applied in order to the identity.
+// X[where[c], :] = W[c, :], where[] = the exchanges of ipiv applied in order to the
+// identity; done as the gather X[r, :] = W[src[r], :] with src the inverse of where
+// (coalesced writes, reads within the same column).
 __global__ void __launch_bounds__(256) unscramble_kernel(const ScatterDesc* __restrict__ descs) {
-    extern __shared__ int where[];
+    extern __shared__ int where[];   // where[n], then src[n]
     const ScatterDesc d = descs[blockIdx.x];
+    int* src = where + d.n;
     if (threadIdx.x == 0) {
         for (int i = 0; i < d.n; ++i) where[i] = i;
         for (int i = 0; i < d.n; ++i) {
@@ -740,10 +813,12 @@ __global__ void __launch_bounds__(256) unscramble_kernel(const ScatterDesc* __re
         }
     }
     __syncthreads();
+    for (int c = threadIdx.x; c < d.n; c += blockDim.x) src[where[c]] = c;
+    __syncthreads();
     const size_t total = (size_t)d.n * d.n;
-    for (size_t e = threadIdx.x; e < total; e += blockDim.x) {
-        const int i = (int)(e % d.n), c = (int)(e / d.n);
-        d.X[i + (size_t)where[c] * d.ldx] = d.W[i + (size_t)c * d.ldw];
+    for (size_t e = blockIdx.y * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.y * blockDim.x) {
+        const int r = (int)(e % d.n), j = (int)(e / d.n);
+        d.X[r + (size_t)j * d.ldx] = d.W[src[r] + (size_t)j * d.ldw];
     }
 }
 
@@ -753,7 +828,7 @@ struct PanelStep : Plan::Step {
     void run(cudaStream_t s, int* st) const override {
         if (t.h.empty()) return;
         size_t mx = 0;
-        for (auto& d : t.h) mx = std::max(mx, (size_t)(d.n - d.k0) * d.kw * sizeof(double));
+        for (auto& d : t.h) mx = std::max(mx, panel_smem(d.n - d.k0, d.kw));
         static size_t cur = 0;
         ensure_dyn_smem(panel_pivot_kernel, mx, cur);
         panel_pivot_kernel<<<t.size(), 256, mx, s>>>(t.d.p, st);
@@ -769,11 +844,12 @@ struct ScatterStep : Plan::Step {
         int mx = 0;
         for (auto& d : t.h) mx = std::max(mx, d.n);
         static size_t cur = 0;
-        ensure_dyn_smem(unscramble_kernel, (size_t)mx * sizeof(int), cur);
-        unscramble_kernel<<<t.size(), 256, (size_t)mx * sizeof(int), s>>>(t.d.p);
+        ensure_dyn_smem(unscramble_kernel, 2 * (size_t)mx * sizeof(int), cur);
+        const int gy = std::max(1, std::min(8, mx * mx / 16384));
+        unscramble_kernel<<<dim3(t.size(), gy), 256, 2 * (size_t)mx * sizeof(int), s>>>(t.d.p);
         HM_CUDA(cudaGetLastError());
     }
-    const char* name() const override { return "unscramble_columns"; }
+    const char* name() const override { return "unscramble"; }
     int nlaunch() const override { return t.h.empty() ? 0 : 1; }
     double bytes() const override {
         double b = 0;
@@ -798,21 +874,20 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
         plan.add(std::move(st));
     }
     if (large.empty()) return;
-    struct Work { const InvProblem* p; double *W, *Dinv, *T, *Z; int* ipiv; int w; };
+    struct Work { const InvProblem* p; double *W, *PD, *T, *Z; int* ipiv; int w; };
     std::vector<Work> ws;
-    int nmax = 0, steps = 0;
+    int steps = 0;
     auto cp = std::make_unique<CopyStep>();
     for (auto& p : large) {
         HM_CHECK(p.n <= 16384, HM_ERR_UNSUPPORTED, "inverse: order above 16384");
         Work x{&p, nullptr, nullptr, nullptr, nullptr, nullptr, bgj_width(p.n)};
         x.W = plan.scratch((size_t)p.n * p.n);
-        x.Dinv = plan.scratch((size_t)x.w * x.w);
-        x.T = plan.scratch((size_t)x.w * p.n);
-        x.Z = plan.scratch((size_t)p.n * x.w);
+        x.PD = plan.scratch((size_t)x.w * x.w);
+        x.T = plan.scratch((size_t)p.n * x.w);   // n x kw, ld n (rows O used)
+        x.Z = plan.scratch((size_t)x.w * p.n);   // kw x n, ld kw (columns O used)
         x.ipiv = plan.scratch_i(p.n);
         cp->t.h.push_back({p.A, p.lda, x.W, p.n, p.n, p.n, 0, 0, 0});
         ws.push_back(x);
-        nmax = std::max(nmax, p.n);
         steps = std::max(steps, ceil_div(p.n, x.w));
     }
     cp->t.upload(s);
@@ -829,30 +904,30 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
             const int kw = std::min(x.w, n - k0), e0 = k0 + kw, ld = n;
             double* W = x.W;
             pan->t.h.push_back({W, ld, n, k0, kw, x.ipiv});
-            gj->t[kw <= 32 ? 0 : 1].h.push_back({W + k0 + (size_t)k0 * ld, ld, x.Dinv, kw, kw});
-            // column ranges R1 = [0, k0), R2 = [e0, n); row ranges O1, O2 the same
+            gj->t[kw <= 32 ? 0 : 1].h.push_back({W + k0 + (size_t)k0 * ld, ld, x.PD, kw, kw});
+            // index ranges outside K: [0, k0) and [e0, n)
             const int r0[2] = {0, e0}, rl[2] = {k0, n - e0};
             for (int q = 0; q < 2; ++q) {
                 if (rl[q] <= 0) continue;
-                // T[:, Rq] = Dinv W[K, Rq]
-                gTZ->batch.add(kw, rl[q], kw, 1.0, x.Dinv, kw, OP_N, W + k0 + (size_t)r0[q] * ld, ld, OP_N, 0.0,
-                               x.T + (size_t)r0[q] * kw, kw);
-                // Z[Oq, :] = -W[Oq, K] Dinv
-                gTZ->batch.add(rl[q], kw, kw, -1.0, W + r0[q] + (size_t)k0 * ld, ld, OP_N, x.Dinv, kw, OP_N, 0.0,
-                               x.Z + r0[q], n);
+                // T[Oq, :] = W[Oq, K] PD
+                gTZ->batch.add(rl[q], kw, kw, 1.0, W + r0[q] + (size_t)k0 * ld, ld, OP_N, x.PD, kw, OP_N, 0.0,
+                               x.T + r0[q], n);
+                // Z[:, Oq] = -PD W[K, Oq]
+                gTZ->batch.add(kw, rl[q], kw, -1.0, x.PD, kw, OP_N, W + k0 + (size_t)r0[q] * ld, ld, OP_N, 0.0,
+                               x.Z + (size_t)r0[q] * kw, kw);
             }
             for (int qi = 0; qi < 2; ++qi)
                 for (int qj = 0; qj < 2; ++qj) {
                     if (rl[qi] <= 0 || rl[qj] <= 0) continue;
-                    // W[Oqi, Rqj] += Z[Oqi, :] W[K, Rqj]
-                    gUp->batch.add(rl[qi], rl[qj], kw, 1.0, x.Z + r0[qi], n, OP_N, W + k0 + (size_t)r0[qj] * ld, ld,
-                                   OP_N, 1.0, W + r0[qi] + (size_t)r0[qj] * ld, ld);
+                    // W[Oqi, Oqj] += W[Oqi, K] Z[:, Oqj]
+                    gUp->batch.add(rl[qi], rl[qj], kw, 1.0, W + r0[qi] + (size_t)k0 * ld, ld, OP_N,
+                                   x.Z + (size_t)r0[qj] * kw, kw, OP_N, 1.0, W + r0[qi] + (size_t)r0[qj] * ld, ld);
                 }
-            put->t.h.push_back({x.Dinv, kw, W + k0 + (size_t)k0 * ld, ld, kw, kw, 0, 0, 0});
+            put->t.h.push_back({x.PD, kw, W + k0 + (size_t)k0 * ld, ld, kw, kw, 0, 0, 0});
             for (int q = 0; q < 2; ++q) {
                 if (rl[q] <= 0) continue;
-                put->t.h.push_back({x.T + (size_t)r0[q] * kw, kw, W + k0 + (size_t)r0[q] * ld, ld, kw, rl[q], 0, 0, 0});
-                put->t.h.push_back({x.Z + r0[q], n, W + r0[q] + (size_t)k0 * ld, ld, rl[q], kw, 0, 0, 0});
+                put->t.h.push_back({x.T + r0[q], n, W + r0[q] + (size_t)k0 * ld, ld, rl[q], kw, 0, 0, 0});
+                put->t.h.push_back({x.Z + (size_t)r0[q] * kw, kw, W + k0 + (size_t)r0[q] * ld, ld, kw, rl[q], 0, 0, 0});
             }
         }
         pan->t.upload(s);
@@ -870,7 +945,6 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
     for (auto& x : ws) sc->t.h.push_back({x.W, x.p->n, x.p->X, x.p->ldx, x.p->n, x.ipiv});
     sc->t.upload(s);
     plan.add(std::move(sc));
-    (void)nmax;
 }
 
 void plan_gram_svd(Plan& plan, const std::vector<SvdProblem>& probs, double tol, int max_rank,
