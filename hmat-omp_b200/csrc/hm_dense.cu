@@ -15,6 +15,7 @@
 #include "hm_dense.h"
 
 #include <algorithm>
+#include <map>
 #include <cstdlib>
 #include <cmath>
 
@@ -609,14 +610,15 @@ void launch_ident(const DevTable<IdentDesc>& t, cudaStream_t s) {
 // ---------------------------------------------------------------------------------
 // Plans
 // ---------------------------------------------------------------------------------
-// Largest order inverted by one Gauss-Jordan kernel; larger ones go through the block
-// Gauss-Jordan sweep below, whose bulk runs as batched GEMMs.  64 by default;
-// HM_GJ_MAX (32, 64, 96 or 128) overrides it.
+// Largest order inverted by one Gauss-Jordan kernel (pivoting over all rows); larger
+// ones go through the block Gauss-Jordan sweep below, whose bulk runs as batched GEMMs.
+// 128 by default (every capacitance matrix of rank <= 64 per side is one launch per
+// level); HM_GJ_MAX (32, 64, 96 or 128) overrides it.
 static int gj_max() {
     static const int v = [] {
         const char* e = std::getenv("HM_GJ_MAX");
-        const int x = e ? std::atoi(e) : 64;
-        return (x == 32 || x == 64 || x == 96 || x == 128) ? x : 64;
+        const int x = e ? std::atoi(e) : 128;
+        return (x == 32 || x == 64 || x == 96 || x == 128) ? x : 128;
     }();
     return v;
 }
@@ -667,8 +669,7 @@ static size_t panel_smem(int m, int kw) {
 
 __global__ void __launch_bounds__(256) panel_pivot_kernel(const PanelDesc* __restrict__ descs, int* status) {
     extern __shared__ double sm[];   // panel: (m + 1) x kw column-major (then the move buffer); 2m ints
-    __shared__ double red_v[2][8];
-    __shared__ int red_i[2][8];
+    __shared__ unsigned red_k[2][8];
     __shared__ int prow[64];
     __shared__ int mv_pos[128], mv_src[128];
     __shared__ int s_bad, s_nmv;
@@ -687,48 +688,47 @@ __global__ void __launch_bounds__(256) panel_pivot_kernel(const PanelDesc* __res
     // Right-looking elimination without row exchanges: a row chosen as pivot is flagged
     // (bit k of `used` for row tid + k nt) and left in place.  Each thread updates its own
     // rows and, in the same pass, offers its best candidate for the next column, so one
-    // barrier per column separates the steps.  Pivot: largest |value|, ties to the lowest
-    // row (the choice of LU with partial pivoting).
-    unsigned long long used = 0;
-    auto offer = [&](double bv, int bi, int buf) {
-        for (int off = 16; off > 0; off >>= 1) {
-            const double ov = __shfl_down_sync(0xffffffffu, bv, off);
-            const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-        }
-        if (lane == 0) { red_v[buf][warp] = bv; red_i[buf][warp] = bi; }
+    // barrier per column separates the steps.  Candidates are compared by a 32-bit key:
+    // the high word of |value| with its low ib bits replaced by (mask - row), so one warp
+    // max-reduction picks a pivot within a relative 2^(ib - 20) of the largest (ties to
+    // the lowest row), which keeps partial pivoting's stability bound.
+    const int ib = 32 - __clz(max(m - 1, 1));
+    const unsigned mask = (1u << ib) - 1u;
+    auto key = [&](double v, int i) -> unsigned {
+        if (!(v == v)) return 0u;   // NaN never wins
+        const unsigned hi = (unsigned)((unsigned long long)__double_as_longlong(fabs(v)) >> 32);
+        return (hi & ~mask) | (mask - (unsigned)i);
+    };
+    auto offer = [&](unsigned k, int buf) {
+        k = __reduce_max_sync(0xffffffffu, k);
+        if (lane == 0) red_k[buf][warp] = k;
     };
     auto choose = [&](int buf) {
-        double v = red_v[buf][0];
-        int p = red_i[buf][0];
-        for (int w = 1; w < nw; ++w)
-            if (red_v[buf][w] > v || (red_v[buf][w] == v && red_i[buf][w] < p)) { v = red_v[buf][w]; p = red_i[buf][w]; }
-        return p;
+        unsigned k = red_k[buf][0];
+        for (int w = 1; w < nw; ++w) k = max(k, red_k[buf][w]);
+        return k;
     };
+    unsigned long long used = 0;
     __syncthreads();
     {
-        double bv = -1.0;
-        int bi = 0x7fffffff;
-        for (int i = tid; i < m; i += nt) {
-            const double v = fabs(pan[i]);
-            if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
-        }
-        offer(bv, bi, 0);
+        unsigned best = 0;
+        for (int i = tid; i < m; i += nt) best = max(best, key(pan[i], i));
+        offer(best, 0);
     }
     __syncthreads();
     for (int j = 0; j < kw; ++j) {
-        const int p = choose(j & 1);
-        const bool pin = p >= 0 && p < m;   // false only when every candidate was NaN
+        const unsigned kb = choose(j & 1);
+        const int p = (int)(mask - (kb & mask));
+        const bool pin = kb != 0u && p >= 0 && p < m;   // false when no candidate is a number
         const double pv = pin ? pan[p + (size_t)j * LDP] : 0.0;
         const bool ok = pin && fabs(pv) > 0.0 && isfinite(pv);
         if (tid == 0) {
-            prow[j] = p;
+            prow[j] = pin ? p : -1;
             if (!ok) s_bad = 1;
         }
         if (pin && p % nt == tid) used |= 1ull << (p / nt);
         const double rinv = ok ? 1.0 / pv : 0.0;
-        double bv = -1.0;
-        int bi = 0x7fffffff;
+        unsigned best = 0;
         for (int k = 0, i = tid; i < m; ++k, i += nt) {
             if ((used >> k) & 1ull) continue;
             if (ok) {
@@ -750,35 +750,36 @@ __global__ void __launch_bounds__(256) panel_pivot_kernel(const PanelDesc* __res
                         if (c0 + u < kw) ri[(size_t)(c0 + u) * LDP] = fma(-l, b[u], a[u]);
                 }
             }
-            if (j + 1 < kw) {
-                const double v = fabs(pan[i + (size_t)(j + 1) * LDP]);
-                if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; }
-            }
+            if (j + 1 < kw) best = max(best, key(pan[i + (size_t)(j + 1) * LDP], i));
         }
-        if (j + 1 < kw) offer(bv, bi, (j + 1) & 1);
+        if (j + 1 < kw) offer(best, (j + 1) & 1);
         __syncthreads();
     }
     // The pivot rows as the exchange sequence of LU with partial pivoting (position j
     // exchanged with position ipiv[j]), and as one permutation of the columns k0..n-1:
     // column k0 + i receives column k0 + at[i]; only the moved ones (at most 2 kw) are listed.
+    for (int i = tid; i < m; i += nt) at[i] = pos[i] = i;
+    if (tid == 0) s_nmv = 0;
+    __syncthreads();
     if (tid == 0) {
         if (s_bad) atomicOr(status, ST_SINGULAR);
-        for (int i = 0; i < m; ++i) at[i] = pos[i] = i;
         for (int j = 0; j < kw; ++j) {
             const int r = (prow[j] >= 0 && prow[j] < m) ? prow[j] : j;
             const int q = pos[r] >= j ? pos[r] : j;   // a repeated row (only after a bad pivot) stays put
             d.ipiv[d.k0 + j] = d.k0 + q;
-            const int a = at[j], b = at[q];
-            at[j] = b; at[q] = a;
-            pos[b] = j; pos[a] = q;
+            const int x = at[j], y = at[q];
+            at[j] = y; at[q] = x;
+            pos[y] = j; pos[x] = q;
         }
-        int nmv = 0;
-        for (int i = 0; i < m && nmv < 128; ++i)
-            if (at[i] != i) { mv_pos[nmv] = i; mv_src[nmv] = at[i]; ++nmv; }
-        s_nmv = nmv;
     }
     __syncthreads();
-    const int nmv = s_nmv;
+    for (int i = tid; i < m; i += nt)   // the moved positions, in any order (at most 2 kw)
+        if (at[i] != i) {
+            const int sl = atomicAdd(&s_nmv, 1);
+            if (sl < 128) { mv_pos[sl] = i; mv_src[sl] = at[i]; }
+        }
+    __syncthreads();
+    const int nmv = min(s_nmv, 128);
     if (nmv == 0) return;
     // move the columns through shared memory (the panel's space), rc rows at a time: all
     // reads of a chunk, then all writes (coalesced along the rows)

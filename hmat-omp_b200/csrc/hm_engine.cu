@@ -1426,14 +1426,22 @@ void Engine::plan_factor(FactorStore<T>& fs) {
                 const int ldw = C.len();
                 T* Tt = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)q * w, 1)))
                             : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)q * w, 1)));
-                T* Dt = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)p * w, 1)))
-                            : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)p * w, 1)));
+                // delta = P t in two blocks (rows of U1, rows of U2), each with its leading
+                // dimension a multiple of 4 elements so the correction's operands are
+                // addressable by the tensor-core kernel's TMA
+                const int ld1 = (p1 + 3) / 4 * 4, ld2 = (p2 + 3) / 4 * 4;
+                T* D1 = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)ld1 * w, 1)))
+                            : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)ld1 * w, 1)));
+                T* D2 = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)ld2 * w, 1)))
+                            : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)ld2 * w, 1)));
                 gT->batch.add(q1, w, L.len(), T(1), Vt + L.offV, L.len(), OP_T, W, ldw, OP_N, T(0), Tt, q);
                 gT->batch.add(q2, w, R.len(), T(1), Vt + R.offV, R.len(), OP_T, W + L.len(), ldw, OP_N,
                               T(0), Tt + q1, q);
-                gD->batch.add(p, w, q, T(1), Pn, p, OP_N, Tt, q, OP_N, T(0), Dt, p);
-                gC->batch.add(L.len(), w, p1, T(-1), fs.Q.p + L.offU, L.len(), OP_N, Dt, p, OP_N, T(1), W, ldw);
-                gC->batch.add(R.len(), w, p2, T(-1), fs.Q.p + R.offU, R.len(), OP_N, Dt + p1, p, OP_N,
+                gD->batch.add(p1, w, q, T(1), Pn, p, OP_N, Tt, q, OP_N, T(0), D1, std::max(ld1, 1));
+                gD->batch.add(p2, w, q, T(1), Pn + p1, p, OP_N, Tt, q, OP_N, T(0), D2, std::max(ld2, 1));
+                gC->batch.add(L.len(), w, p1, T(-1), fs.Q.p + L.offU, L.len(), OP_N, D1, std::max(ld1, 1), OP_N,
+                              T(1), W, ldw);
+                gC->batch.add(R.len(), w, p2, T(-1), fs.Q.p + R.offU, R.len(), OP_N, D2, std::max(ld2, 1), OP_N,
                               T(1), W + L.len(), ldw);
             }
         }

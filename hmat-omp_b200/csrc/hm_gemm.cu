@@ -744,8 +744,15 @@ void GemmBatch<T>::finalize_tc(cudaStream_t s, bool force) {
         std::vector<GemmDesc<float>> dv(h_);
         long long kblocks = 0;
         int tt = 0;
+        static const bool dbg = std::getenv("HM_TC_DEBUG") != nullptr;
         for (auto& d : dv) {
-            if (!tc::tma_ok(d)) return;
+            if (!tc::tma_ok(d)) {
+                if (dbg)
+                    fprintf(stderr, "[tc] %s: operand not TMA-addressable (A%%16=%d B%%16=%d lda=%d ldb=%d)\n",
+                            tag_.c_str(), (int)(reinterpret_cast<uintptr_t>(d.A) & 15),
+                            (int)(reinterpret_cast<uintptr_t>(d.B) & 15), d.lda, d.ldb);
+                return;
+            }
             d.tiles_m = ceil_div(d.m, tc::BM);
             d.tiles_n = ceil_div(d.n, pipe_bn_);
             d.tile0 = tt;
@@ -755,7 +762,10 @@ void GemmBatch<T>::finalize_tc(cudaStream_t s, bool force) {
         }
         if (tt == 0 || (!force && kblocks < 4LL * tt)) return;
         std::vector<CUtensorMap> maps;
-        if (!tc::encode_maps(dv, pipe_bn_, maps)) return;
+        if (!tc::encode_maps(dv, pipe_bn_, maps)) {
+            if (dbg) fprintf(stderr, "[tc] %s: tensor-map encoding refused\n", tag_.c_str());
+            return;
+        }
         std::vector<int> tp((size_t)tt);
         for (size_t i = 0; i < dv.size(); ++i)
             std::fill(tp.begin() + dv[i].tile0, tp.begin() + dv[i].tile0 + dv[i].tiles_m * dv[i].tiles_n * dv[i].ksplit,
