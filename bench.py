@@ -8,6 +8,7 @@ b ~ N(0,1).  One step = factor + solve of the 64 right-hand sides; the mixed pat
 refines against the FP64 compressed operator to relative residual <= 1e-10.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload headline|batched|hss|adjoint] [--shard subtree]
 
 Prints one JSON line (rank 0).  --impl reference times the reference's own OpenMP
 solve (the oracle library compiled from the reference sources) on the host cores.
@@ -81,6 +82,8 @@ def parse():
     ap.add_argument("--workload", default="headline", choices=["headline", "batched", "hss", "adjoint"])
     ap.add_argument("--systems", type=int, default=512)
     ap.add_argument("--refine", type=int, default=1, help="FP64 refinement steps (batched workload)")
+    ap.add_argument("--shard", default="none", choices=["none", "subtree"],
+                    help="subtree: one headline system sharded over the ranks by subtrees (FP64)")
     return ap.parse_args()
 
 
@@ -276,6 +279,7 @@ def run_ours(args):
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    torch.cuda.set_stream(torch.cuda.Stream(device=dev))   # a real stream: the library launches on it
     stream = torch.cuda.current_stream()
 
     def barrier():
@@ -440,6 +444,73 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_shard(args):
+    """One headline system (Coulomb 2-D, N = 2^18, leaf 256, ranks <= 96, 64 RHS) sharded
+    over the ranks by subtrees (hmat_shard.py): rank g keeps its depth-log2(P) subtree in
+    its own engine handle and its rows of the top couplings; a step is the FP64
+    factorization (local engine + top levels) and the solve, with NCCL all-reduces of the
+    top levels' small matrices.  Every rank builds the whole operator (the top-level
+    compression is not sharded).  Strong scaling: the work is fixed as P grows."""
+    import torch
+    import torch.distributed as dist
+    import hmat_b200 as H
+    import hmat_shard as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_stream(torch.cuda.Stream(device=dev))   # a real stream: the library launches on it
+    stream = torch.cuda.current_stream()
+    N, s = args.n, args.nrhs
+    h = H.HODLRMatrix(1e-10, rsvd_rank=args.rank, oversample=10, max_rank=args.rank, sketch=H.SKETCH_DEVICE_NORMAL,
+                      seed=0, precision=H.FP64)
+    h.set_stream(stream.cuda_stream)
+    h.build_from_kernel(H.KERNEL_COULOMB, morton_points(N, 3), [1e-3, 4.0], args.leaf)
+    plan = S.partition(N, args.leaf, world)
+    r0, r1 = plan.owner_range(rank)
+    if world == 1:
+        local, top, table = S.EngineLocalSolver.from_handle(h), {}, {}
+    else:
+        nodes = S.nodes_from_handle(h, (r0, r1))
+        sub, top, table = S.rank_share(plan, rank, nodes)
+        local = S.EngineLocalSolver(sub, r0, args.leaf, stream.cuda_stream)
+        top = S.to_torch_share(top, dev)
+        h.close()
+    sh = S.ShardedHODLR(plan, rank, local, top, table, S.TorchOps(dev), S.torch_allreduce)
+    b = torch.from_numpy(np.random.default_rng(3).standard_normal((N, s))[r0:r1].copy()).to(dev)
+
+    def step():
+        local.factor()
+        sh.factored = False
+        return sh.solve(b)
+
+    for _ in range(args.warmup):
+        step()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = reduce_over_ranks(ev0.elapsed_time(ev1) / args.steps, "max", world, dev)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "sharded HODLR factor+solve RHS/s (one Coulomb 2-D system over all ranks, FP64)",
+            "value": s / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": dict(workload_config(args), parallelism=f"subtree shards x{world}"),
+            "collectives_per_step": sh.collectives // max(1, args.steps + args.warmup)}))
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def like_for_like(args, stream):
     """The GPU path on the reference arm's measured problem: N = REF_N, same kernel, points,
     leaf, rank cap and right-hand-side count; factor+solve per step, mixed and FP64, device
@@ -496,6 +567,7 @@ def run_batched(args):
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    torch.cuda.set_stream(torch.cuda.Stream(device=dev))   # a real stream: the library launches on it
     rng = np.random.default_rng(4)
     nall = args.systems
     Ns_all = np.exp(rng.uniform(np.log(1024), np.log(32768), nall)).astype(int)
@@ -618,6 +690,7 @@ def run_hss(args):
     x = np.sort(np.random.default_rng(2).random(N))
     h = H.HSSMatrix(1e-10, rsvd_rank=64, max_rank=64, oversample=10, sketch=H.SKETCH_DEVICE_NORMAL, seed=0,
                     refine_steps=1)
+    torch.cuda.set_stream(torch.cuda.Stream())   # a real stream: the library launches on it
     stream = torch.cuda.current_stream()
     h.set_stream(stream.cuda_stream)
     torch.cuda.synchronize()
@@ -775,6 +848,8 @@ def main():
         # single-system workloads: rank 0 runs and prints; other ranks have nothing to do
         if int(os.environ.get("RANK", "0")) == 0:
             (run_hss if args.workload == "hss" else run_adjoint)(args)
+    elif args.shard == "subtree":
+        run_shard(args)
     else:
         run_ours(args)
 

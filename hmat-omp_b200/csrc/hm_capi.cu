@@ -296,6 +296,11 @@ int hm_solve_exact_device(hm_handle* h, const double* db, int nrhs, int ldb, dou
     return guard(h, [&] { built(h).solve_exact_device(db, nrhs, ldb, dx, ldx, tol, max_iter, st); });
 }
 
+int hm_solve_gmres(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ldx, double tol, int restart,
+                   int max_iter, hm_solve_stats* st) {
+    return guard(h, [&] { built(h).solve_gmres_device(b, nrhs, ldb, x, ldx, tol, restart, max_iter, st); });
+}
+
 int hm_residual_exact(hm_handle* h, const double* b, int nrhs, int ldb, const double* x, int ldx, double* rel) {
     return guard(h, [&] { built(h).residual_exact(b, ldb, x, ldx, nrhs, rel); });
 }

@@ -1843,6 +1843,25 @@ void Engine::solve_exact_device(const double* db, int s, int ldb, double* dx, in
     }
 }
 
+// dx = A~^{-1} db once with the handle's factorization (ld N both): the FP64 solve, or in
+// mixed precision one FP32 sweep without refinement (a preconditioner application).
+void Engine::precondition_device(const double* db, int s, double* dx) {
+    HM_CHECK(built_, HM_ERR_STATE, "precondition before build");
+    if (!factored_) factor();
+    if (opts_.precision != HM_MIXED) {
+        solve_fp64(db, s, N_, dx, N_);
+        return;
+    }
+    ensure_io(s);
+    const size_t n = (size_t)N_ * s;
+    to_float_kernel<<<grid_for(n), 256, 0, stream_>>>(db, ioXf.p, n);
+    count_launch();
+    solve_plan<float>(f32_, uniform(s)).run(stream_, dstatus.p);   // ioYf = A32^{-1} float(b)
+    accumulate_kernel<<<grid_for(n), 256, 0, stream_>>>(dx, ioYf.p, n, 1);
+    count_launch();
+    HM_CUDA(cudaGetLastError());
+}
+
 // rel[j] = ||b_j - A x_j|| / ||b_j|| with A the exact kernel operator, its entries
 // generated inside the batched FP64 product (2 N^2 s flops; A never stored).
 void Engine::residual_exact(const double* db, int ldb, const double* dx, int ldx, int s, double* rel) {

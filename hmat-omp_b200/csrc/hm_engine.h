@@ -104,6 +104,12 @@ class Engine {
     // refinement against the exact kernel operator (matrix-free builds)
     void solve_exact_device(const double* db, int s, int ldb, double* dx, int ldx, double tol, int max_iter,
                             hm_solve_stats* st);
+    // flexible GMRES(restart) against the exact kernel operator, right-preconditioned by
+    // the compressed factorization (hm_krylov.cu)
+    void solve_gmres_device(const double* db, int s, int ldb, double* dx, int ldx, double tol, int restart,
+                            int max_iter, hm_solve_stats* st);
+    // dx = A~^{-1} db with the handle's factorization, once (mixed: one FP32 sweep); ld N
+    void precondition_device(const double* db, int s, double* dx);
     // per-column ||b - A x|| / ||b|| against the exact kernel operator (matrix-free builds)
     void residual_exact(const double* db, int ldb, const double* dx, int ldx, int s, double* rel);
     // adjoint solve and gradient accumulation

@@ -92,6 +92,8 @@ def load() -> C.CDLL:
                                  C.POINTER(SolveStats)]
     L.hm_solve_exact_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_double,
                                         C.c_int, C.POINTER(SolveStats)]
+    L.hm_solve_gmres.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_int,
+                                 C.c_int, C.POINTER(SolveStats)]
     L.hm_residual_exact.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, _dp]
     L.hm_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                   C.POINTER(SolveStats)]
@@ -300,6 +302,20 @@ class _Handle:
         st = SolveStats()
         self._check(self._L.hm_solve_exact(self._h, _d(B), B.shape[1], self.N, _d(X), self.N, tol, max_iter,
                                            C.byref(st)))
+        out = X.ravel() if vec else X
+        return (out, st) if stats else out
+
+    def solve_gmres(self, b: np.ndarray, tol: float = 1e-12, restart: int = 30, max_iter: int = 200,
+                    stats: bool = False):
+        """Flexible GMRES against the exact kernel operator, preconditioned by the
+        compressed factorization (matrix-free builds)."""
+        b = np.asarray(b, dtype=np.float64)
+        vec = b.ndim == 1
+        B = np.asfortranarray(b.reshape(self.N, -1))
+        X = np.zeros_like(B, order="F")
+        st = SolveStats()
+        self._check(self._L.hm_solve_gmres(self._h, B.ctypes.data, B.shape[1], self.N, X.ctypes.data, self.N, tol,
+                                           restart, max_iter, C.byref(st)))
         out = X.ravel() if vec else X
         return (out, st) if stats else out
 

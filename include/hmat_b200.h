@@ -225,6 +225,18 @@ HM_API int hm_solve_exact(hm_handle* h, const double* b, int nrhs, int ldb, doub
 HM_API int hm_solve_exact_device(hm_handle* h, const double* db, int nrhs, int ldb, double* dx, int ldx,
                                  double tol, int max_iter, hm_solve_stats* stats);
 
+/* Krylov solve against the exact operator (no counterpart in the reference): flexible
+ * GMRES(restart) for A x = b, A the exact kernel matrix of an operator built by
+ * hm_*_build_from_kernel (entries generated on the device, A never stored), right-
+ * preconditioned by the compressed factorization in the handle's precision; every column
+ * runs its own Arnoldi process, all in shared launches.  Converges where hm_solve_exact's
+ * stationary refinement diverges (compression error times ||A~^{-1}|| above one).  Stops
+ * when max_j ||b_j - A x_j|| / ||b_j|| <= tol (stats: iterations, that residual) or returns
+ * HM_ERR_IR after max_iter iterations (x holds the last iterate).  Host or device b/x;
+ * synchronises. */
+HM_API int hm_solve_gmres(hm_handle* h, const double* b, int nrhs, int ldb, double* x, int ldx, double tol,
+                          int restart, int max_iter, hm_solve_stats* stats);
+
 /* rel[j] = ||b_j - A x_j|| / ||b_j|| (j < nrhs, rel: host) with A the exact kernel matrix of an
  * operator built by hm_*_build_from_kernel, its entries generated on the device (2 N^2 nrhs
  * flops; A is never stored): the error of any solution against the exact operator rather
