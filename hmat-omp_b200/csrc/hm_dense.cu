@@ -948,6 +948,64 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
     plan.add(std::move(sc));
 }
 
+// Inverses of symmetric positive definite matrices: elimination without pivoting is
+// backward stable for them, so the large ones are split 2 x 2 recursively down to
+// Gauss-Jordan blocks of order <= 64 (X11 = inv(A11), T = X11 A12, W = A21 X11,
+// S = A22 - A21 T, X22 = inv(S), X12 = -T X22, X21 = -X22 W, X11 -= X12 W): fewer,
+// larger batched GEMMs than the pivoted sweep.  A zero or non-finite pivot (a matrix that
+// was not SPD after all) still raises ST_SINGULAR in the Gauss-Jordan blocks.
+void plan_inverse_spd(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t s) {
+    std::vector<InvProblem> small, large;
+    for (auto& p : probs) {
+        if (p.n <= 0) continue;
+        (p.n <= 64 ? small : large).push_back(p);
+    }
+    if (!small.empty()) plan_inverse(plan, small, s);
+    if (large.empty()) return;
+    std::vector<InvProblem> sub11, sub22;
+    auto copyS = std::make_unique<CopyStep>();
+    auto g1 = std::make_unique<GemmStep<double>>("inverse.spd");
+    auto g2 = std::make_unique<GemmStep<double>>("inverse.spd");
+    auto g3 = std::make_unique<GemmStep<double>>("inverse.spd");
+    auto g4 = std::make_unique<GemmStep<double>>("inverse.spd");
+    for (auto& p : large) {
+        HM_CHECK(p.A != p.X, HM_ERR_ARG, "SPD block inverse cannot run in place");
+        const int a = p.n / 2, b = p.n - a;
+        const double* A11 = p.A;
+        const double* A12 = p.A + (size_t)a * p.lda;
+        const double* A21 = p.A + a;
+        const double* A22 = p.A + a + (size_t)a * p.lda;
+        double* X11 = p.X;
+        double* X12 = p.X + (size_t)a * p.ldx;
+        double* X21 = p.X + a;
+        double* X22 = p.X + a + (size_t)a * p.ldx;
+        double* T = plan.scratch((size_t)a * b);
+        double* W = plan.scratch((size_t)b * a);
+        double* S = plan.scratch((size_t)b * b);
+        sub11.push_back({A11, p.lda, X11, p.ldx, a});
+        copyS->t.h.push_back({A22, p.lda, S, b, b, b, 0, 0, 0});
+        g1->batch.add(a, b, a, 1.0, X11, p.ldx, OP_N, A12, p.lda, OP_N, 0.0, T, a);
+        g1->batch.add(b, a, a, 1.0, A21, p.lda, OP_N, X11, p.ldx, OP_N, 0.0, W, b);
+        g2->batch.add(b, b, a, -1.0, A21, p.lda, OP_N, T, a, OP_N, 1.0, S, b);
+        sub22.push_back({S, b, X22, p.ldx, b});
+        g3->batch.add(a, b, b, -1.0, T, a, OP_N, X22, p.ldx, OP_N, 0.0, X12, p.ldx);
+        g3->batch.add(b, a, b, -1.0, X22, p.ldx, OP_N, W, b, OP_N, 0.0, X21, p.ldx);
+        g4->batch.add(a, a, b, -1.0, X12, p.ldx, OP_N, W, b, OP_N, 1.0, X11, p.ldx);
+    }
+    copyS->t.upload(s);
+    plan.add(std::move(copyS));
+    plan_inverse_spd(plan, sub11, s);
+    g1->batch.finalize(s);
+    plan.add(std::move(g1));
+    g2->batch.finalize(s);
+    plan.add(std::move(g2));
+    plan_inverse_spd(plan, sub22, s);
+    g3->batch.finalize(s);
+    plan.add(std::move(g3));
+    g4->batch.finalize(s);
+    plan.add(std::move(g4));
+}
+
 void plan_gram_svd(Plan& plan, const std::vector<SvdProblem>& probs, double tol, int max_rank,
                    cudaStream_t s, int rounds) {
     if (probs.empty()) return;

@@ -330,6 +330,9 @@ struct InvProblem {
     int n;
 };
 void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t s);
+// The same for matrices known to be symmetric positive definite: unpivoted 2 x 2 block
+// elimination above order 64 (backward stable for SPD).  X may not alias A.
+void plan_inverse_spd(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t s);
 
 // Gram/Jacobi SVD of tall X_i (rows x k): X = L diag(sigma) R^T with L (rows x k)
 // orthonormal columns and R (k x k) orthogonal, sigma sorted descending; optionally

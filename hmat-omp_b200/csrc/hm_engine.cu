@@ -299,6 +299,7 @@ void Engine::begin_build(int N, int leaf) {
     grads_ready_ = false;
     gen_ = GEN_DENSE;
     gp_ = GenParams();
+    leaves_spd_ = false;
     nodes_ = kind_ == HODLR ? hodlr_tree(N, leaf) : hss_tree(N, leaf);
     sys_N_ = {N};
     sys_off_ = {0};
@@ -384,6 +385,8 @@ void Engine::build_batch_kernel(int gen, const double* pts, int dim, int nsys, c
     src.gp.p0v = dSysP0.p;
     src.gp.p1v = dSysP1.p;
     build_hodlr(src);
+    leaves_spd_ = true;
+    for (int k = 0; k < nsys; ++k) leaves_spd_ = leaves_spd_ && kernel_spd(gen, p0s[k], p1s[k]);
     built_ = true;  // no kernel-parameter gradient for batches (gen_ stays dense)
 }
 
@@ -494,6 +497,7 @@ void Engine::build_kernel(int gen, const double* pts, size_t npts, int dim, int 
     else build_hss(src);
     gen_ = src.gen;
     gp_ = src.gp;
+    leaves_spd_ = kernel_spd(gen, p0, p1);
     built_ = true;
 }
 
@@ -1294,7 +1298,8 @@ void Engine::plan_factor(FactorStore<T>& fs) {
             const Node& n = nodes_[l];
             inv.push_back({dD.p + n.offD, n.len(), dDinv.p + n.offD, n.len(), n.len()});
         }
-        plan_inverse(plan, inv, s);
+        if (leaves_spd_) plan_inverse_spd(plan, inv, s);   // SPD leaves: no pivoting needed
+        else plan_inverse(plan, inv, s);
     }
     if (dMinv.n < std::max<size_t>(offM, 1)) dMinv.alloc(std::max<size_t>(offM, 1));
     sizeM_ = offM;
@@ -1426,22 +1431,14 @@ void Engine::plan_factor(FactorStore<T>& fs) {
                 const int ldw = C.len();
                 T* Tt = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)q * w, 1)))
                             : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)q * w, 1)));
-                // delta = P t in two blocks (rows of U1, rows of U2), each with its leading
-                // dimension a multiple of 4 elements so the correction's operands are
-                // addressable by the tensor-core kernel's TMA
-                const int ld1 = (p1 + 3) / 4 * 4, ld2 = (p2 + 3) / 4 * 4;
-                T* D1 = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)ld1 * w, 1)))
-                            : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)ld1 * w, 1)));
-                T* D2 = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)ld2 * w, 1)))
-                            : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)ld2 * w, 1)));
+                T* Dt = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)p * w, 1)))
+                            : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)p * w, 1)));
                 gT->batch.add(q1, w, L.len(), T(1), Vt + L.offV, L.len(), OP_T, W, ldw, OP_N, T(0), Tt, q);
                 gT->batch.add(q2, w, R.len(), T(1), Vt + R.offV, R.len(), OP_T, W + L.len(), ldw, OP_N,
                               T(0), Tt + q1, q);
-                gD->batch.add(p1, w, q, T(1), Pn, p, OP_N, Tt, q, OP_N, T(0), D1, std::max(ld1, 1));
-                gD->batch.add(p2, w, q, T(1), Pn + p1, p, OP_N, Tt, q, OP_N, T(0), D2, std::max(ld2, 1));
-                gC->batch.add(L.len(), w, p1, T(-1), fs.Q.p + L.offU, L.len(), OP_N, D1, std::max(ld1, 1), OP_N,
-                              T(1), W, ldw);
-                gC->batch.add(R.len(), w, p2, T(-1), fs.Q.p + R.offU, R.len(), OP_N, D2, std::max(ld2, 1), OP_N,
+                gD->batch.add(p, w, q, T(1), Pn, p, OP_N, Tt, q, OP_N, T(0), Dt, p);
+                gC->batch.add(L.len(), w, p1, T(-1), fs.Q.p + L.offU, L.len(), OP_N, Dt, p, OP_N, T(1), W, ldw);
+                gC->batch.add(R.len(), w, p2, T(-1), fs.Q.p + R.offU, R.len(), OP_N, Dt + p1, p, OP_N,
                               T(1), W + L.len(), ldw);
             }
         }

@@ -221,6 +221,13 @@ class Engine {
     // the build's operator source (kernel generator and its parameters) and gradients
     int gen_ = GEN_DENSE;
     GenParams gp_;
+    // every diagonal (leaf) block is symmetric positive definite: Gaussian and Coulomb
+    // kernels with positive scale and non-negative shift (positive definite radial
+    // functions), set by the kernel builds; dense builds and imports stay false
+    bool leaves_spd_ = false;
+    static bool kernel_spd(int gen, double p0, double p1) {
+        return (gen == GEN_GAUSSIAN || gen == GEN_COULOMB) && p0 > 0 && p1 >= 0;
+    }
     DBuf<double> gD_, gU_, gV_, gB_, gAcc_;
     std::map<int, Plan> grad_plans_;   // per column count, recorded once per operator
     bool grads_ready_ = false;

@@ -254,6 +254,7 @@ void Engine::load(const char* path) {
         gp_.dim = dim;
         gp_.p0 = p0;
         gp_.p1 = p1;
+        leaves_spd_ = kernel_spd(gen, p0, p1);
     }
     built_ = true;
 }
