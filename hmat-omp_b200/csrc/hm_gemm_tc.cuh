@@ -492,8 +492,10 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
             const uint32_t tbase = tmem + (uint32_t)(acc * S::ACC_COLS) + ((uint32_t)(32 * q) << 16);
             const uint32_t cb0 = smem_u32(cbuf) + 4u * row;   // this row of column 0 of the C tile
             // 16 columns per round: the main and correction accumulators, then the round's
-            // C reads all issued together, then the results
-#pragma unroll
+            // C reads all issued together, then the results (the 16-column body is unrolled;
+            // the outer loop is not, to keep the kernel's code small: instruction fetch
+            // stalls led this kernel's profile)
+#pragma unroll 1
             for (int c = 0; c < BN / 16; ++c) {
                 if (16 * c >= nt) break;
                 float v[16], w[16], cc[16];
