@@ -14,6 +14,7 @@ struct hm_handle {
     cudaStream_t own = nullptr;
     cudaStream_t stream = nullptr;
     std::unique_ptr<hm::Engine> eng;
+    std::vector<int> fix12, fix21;   // rank profile for the next HODLR builds
 };
 
 namespace {
@@ -41,6 +42,7 @@ hm::Engine& engine(hm_handle* h, hm::Engine::Kind kind) {
     if (!h->eng || h->eng->kind() != kind) {
         h->eng = std::make_unique<hm::Engine>(h->opts, kind);
         h->eng->set_stream(h->stream);
+        h->eng->set_rank_profile(h->fix12, h->fix21);
     }
     return *h->eng;
 }
@@ -219,6 +221,21 @@ int hm_hss_build_from_dense(hm_handle* h, const double* A, int N, int lda, int l
                                   (size_t)N * sizeof(double), N, cudaMemcpyHostToDevice, h->stream));
         engine(h, hm::Engine::HSS).build_dense_device(d.p, N, N, leaf);
         HM_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int hm_set_rank_profile(hm_handle* h, int nnodes, const int* rank12, const int* rank21) {
+    return guard(h, [&] {
+        if (!rank12 || !rank21 || nnodes <= 0) {
+            h->fix12.clear();
+            h->fix21.clear();
+        } else {
+            for (int i = 0; i < nnodes; ++i)
+                HM_CHECK(rank12[i] >= 0 && rank21[i] >= 0, HM_ERR_ARG, "rank profile: negative rank");
+            h->fix12.assign(rank12, rank12 + nnodes);
+            h->fix21.assign(rank21, rank21 + nnodes);
+        }
+        if (h->eng) h->eng->set_rank_profile(h->fix12, h->fix21);
     });
 }
 

@@ -948,6 +948,141 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
     plan.add(std::move(sc));
 }
 
+// ---------------------------------------------------------------------------------
+// Shifted CholeskyQR3 (Fukaya, Kannan, Nakatsukasa, Yamamoto, Yanagisawa; SIAM J. Sci.
+// Comput. 2020): X = Q R by Gram matrices.  Pass 1 factors G + s I with the shift
+// s = 11 (m k + k (k + 1)) u tr(G), which brings cond(X R^{-1}) to about u^{-1/2}; passes
+// 2 and 3 are plain CholeskyQR (CholeskyQR2), each X <- X R^{-1}.  chol_rinv_kernel
+// factors one Gram matrix in shared memory and returns R^{-1} (upper triangular).  A pivot
+// at or below 1e-24 of the largest diagonal entry marks a direction the sketch does not
+// contain (a rank-deficient X): its column of R^{-1} is zero, so Q gets a zero column
+// there rather than amplified rounding noise, and the later passes keep it zero.
+// ---------------------------------------------------------------------------------
+struct CholDesc {
+    const double* G;
+    int ldg;
+    double* Rinv;   // k x k, upper triangular (zeros below)
+    int ldr;
+    int k, rows;
+    int shift;      // 1: shifted pass
+};
+
+__global__ void __launch_bounds__(256) chol_rinv_kernel(const CholDesc* __restrict__ descs) {
+    extern __shared__ double L[];   // k x k, column-major, ld k (lower triangle used); then k flags
+    const CholDesc d = descs[blockIdx.x];
+    const int k = d.k, tid = threadIdx.x, nt = blockDim.x;
+    int* dead = reinterpret_cast<int*>(L + (size_t)k * k);
+    __shared__ double s_diag_max, s_shift;
+    for (int e = tid; e < k * k; e += nt) {
+        const int i = e % k, j = e / k;
+        L[e] = i >= j ? d.G[i + (size_t)j * d.ldg] : 0.0;
+    }
+    for (int j = tid; j < k; j += nt) dead[j] = 0;
+    __syncthreads();
+    if (tid == 0) {
+        double tr = 0.0, mx = 0.0;
+        for (int j = 0; j < k; ++j) {
+            tr += L[j + (size_t)j * k];
+            mx = fmax(mx, L[j + (size_t)j * k]);
+        }
+        const double u = 1.1102230246251565e-16;
+        s_shift = d.shift ? 11.0 * ((double)d.rows * k + (double)k * (k + 1)) * u * tr : 0.0;
+        s_diag_max = mx + s_shift;
+    }
+    __syncthreads();
+    if (d.shift)
+        for (int j = tid; j < k; j += nt) L[j + (size_t)j * k] += s_shift;
+    __syncthreads();
+    const double floor_piv = 1e-24 * s_diag_max;
+    for (int j = 0; j < k; ++j) {
+        // column j: pivot, scale, then the trailing lower triangle
+        const double piv = L[j + (size_t)j * k];
+        const bool ok = piv > floor_piv && isfinite(piv);
+        const double r = ok ? sqrt(piv) : 1.0;
+        __syncthreads();
+        if (tid == 0) {
+            L[j + (size_t)j * k] = r;
+            if (!ok) dead[j] = 1;
+        }
+        for (int i = j + 1 + tid; i < k; i += nt) L[i + (size_t)j * k] = ok ? L[i + (size_t)j * k] / r : 0.0;
+        __syncthreads();
+        const int m = k - j - 1;
+        for (int e = tid; e < m * m; e += nt) {
+            const int i = j + 1 + e % m, c = j + 1 + e / m;
+            if (i >= c) L[i + (size_t)c * k] -= L[i + (size_t)j * k] * L[c + (size_t)j * k];
+        }
+        __syncthreads();
+    }
+    // R^{-1} = (L^{-1})^T: column c of L^{-1} by forward substitution (one thread per
+    // column), written as row c of R^{-1}; dead directions give zero columns of R^{-1}
+    for (int c = tid; c < k; c += nt) {
+        double* out = d.Rinv;
+        for (int i = 0; i < k; ++i) {
+            double v = 0.0;
+            if (i >= c) {
+                double acc = i == c ? 1.0 : 0.0;
+                for (int t = c; t < i; ++t) acc -= L[i + (size_t)t * k] * out[c + (size_t)t * d.ldr];
+                v = acc / L[i + (size_t)i * k];
+            }
+            out[c + (size_t)i * d.ldr] = v;   // R^{-1}(c, i) = L^{-1}(i, c)
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < k * k; e += nt) {
+        const int i = e % k, j = e / k;
+        if (dead[j] || dead[i]) d.Rinv[i + (size_t)j * d.ldr] = 0.0;
+    }
+}
+
+namespace {
+struct CholStep : Plan::Step {
+    DevTable<CholDesc> t;
+    void run(cudaStream_t s, int*) const override {
+        if (t.h.empty()) return;
+        int kmax = 1;
+        for (auto& d : t.h) kmax = std::max(kmax, d.k);
+        const size_t smem = (size_t)kmax * kmax * sizeof(double) + (size_t)kmax * sizeof(int);
+        static size_t cur = 0;
+        ensure_dyn_smem(chol_rinv_kernel, smem, cur);
+        chol_rinv_kernel<<<t.size(), 256, smem, s>>>(t.d.p);
+        HM_CUDA(cudaGetLastError());
+    }
+    const char* name() const override { return "cholesky_rinv"; }
+    int nlaunch() const override { return t.h.empty() ? 0 : 1; }
+};
+}  // namespace
+
+void plan_cholqr3(Plan& plan, const std::vector<QrProblem>& probs, cudaStream_t s) {
+    if (probs.empty()) return;
+    struct W { const QrProblem* p; const double* X; int ldx; };
+    std::vector<W> ws;
+    for (auto& p : probs)
+        if (p.rows > 0 && p.k > 0) ws.push_back({&p, p.X, p.ldx});
+    for (int pass = 0; pass < 3; ++pass) {
+        auto gram = std::make_unique<GemmStep<double>>("build.cholqr_gram");
+        auto chol = std::make_unique<CholStep>();
+        auto rot = std::make_unique<GemmStep<double>>("build.cholqr_apply");
+        for (auto& w : ws) {
+            const int k = w.p->k, m = w.p->rows;
+            double* G = plan.scratch((size_t)k * k);
+            double* Ri = plan.scratch((size_t)k * k);
+            double* Xn = pass == 2 ? w.p->Q : plan.scratch((size_t)m * k);
+            const int ldn = pass == 2 ? w.p->ldq : m;
+            gram->batch.add(k, k, m, 1.0, w.X, w.ldx, OP_T, w.X, w.ldx, OP_N, 0.0, G, k);
+            chol->t.h.push_back({G, k, Ri, k, k, m, pass == 0 ? 1 : 0});
+            rot->batch.add(m, k, k, 1.0, w.X, w.ldx, OP_N, Ri, k, OP_N, 0.0, Xn, ldn);
+            w.X = Xn;
+            w.ldx = ldn;
+        }
+        gram->batch.finalize(s);
+        chol->t.upload(s);
+        rot->batch.finalize(s);
+        plan.add(std::move(gram));
+        plan.add(std::move(chol));
+        plan.add(std::move(rot));
+    }
+}
+
 // Inverses of symmetric positive definite matrices: elimination without pivoting is
 // backward stable for them, so the large ones are split 2 x 2 recursively down to
 // Gauss-Jordan blocks of order <= 64 (X11 = inv(A11), T = X11 A12, W = A21 X11,

@@ -334,6 +334,18 @@ void plan_inverse(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t
 // elimination above order 64 (backward stable for SPD).  X may not alias A.
 void plan_inverse_spd(Plan& plan, const std::vector<InvProblem>& probs, cudaStream_t s);
 
+// Orthonormal basis Q_i (rows x k) of range(X_i) by shifted CholeskyQR3 (Gram matrices,
+// batched Cholesky, X R^{-1}); directions X_i does not contain give zero columns.  Q may
+// not alias X.
+struct QrProblem {
+    const double* X;
+    int ldx;
+    int rows, k;
+    double* Q;
+    int ldq;
+};
+void plan_cholqr3(Plan& plan, const std::vector<QrProblem>& probs, cudaStream_t s);
+
 // Gram/Jacobi SVD of tall X_i (rows x k): X = L diag(sigma) R^T with L (rows x k)
 // orthonormal columns and R (k x k) orthogonal, sigma sorted descending; optionally
 // the truncation rank.  Each round rotates X by the eigenvectors of its Gram matrix

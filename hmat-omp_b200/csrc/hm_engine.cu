@@ -583,6 +583,26 @@ void Engine::build_hodlr(const Source& src) {
             if (b.rsvd) om.emplace_back(b.omega, (size_t)b.n * b.k);
         make_sketches(dOmega, om);
     }
+    // Mixed-precision matrix-free builds: the sketch, power-iteration and projection
+    // products run in FP32 on the tensor cores with A's entries generated in the kernel;
+    // Omega in FP32, each block 16-byte aligned for the TMA
+    const bool tc_sketch = opts_.precision == HM_MIXED && !src.dense();
+    DBuf<float> dOmega32;
+    std::vector<size_t> om32(blocks.size(), 0);
+    if (tc_sketch && omega_total) {
+        size_t tot32 = 0;
+        for (auto& b : blocks)
+            if (b.rsvd) { om32[b.slot] = tot32; tot32 = align_up(tot32 + (size_t)b.n * b.k, 4); }
+        dOmega32.alloc(std::max<size_t>(tot32, 1));
+        Plan cv;
+        auto st = std::make_unique<CopyStep>();
+        for (auto& b : blocks)
+            if (b.rsvd) st->t.h.push_back({dOmega.p + b.omega, b.n, dOmega32.p + om32[b.slot], b.n, b.n, b.k, 0, 0, 1});
+        st->t.upload(stream_);
+        cv.add(std::move(st));
+        cv.run(stream_, dstatus.p);
+        HM_CUDA(cudaStreamSynchronize(stream_));
+    }
     // per-block sigma and rank
     std::vector<size_t> sig_off(blocks.size());
     size_t sig_total = 0;
@@ -626,7 +646,119 @@ void Engine::build_hodlr(const Source& src) {
             plan_gram_svd(plan, sv, opts_.tol, opts_.max_rank, stream_);
         }
         // ---- randomized SVDs (compression.h:67-99) ----
-        if (!rs.empty()) {
+        if (!rs.empty() && tc_sketch) {
+            // FP32 products of generated A on the tensor cores (FP32 accumulation of TF32
+            // hi/lo splits), basis by shifted CholeskyQR3 in FP64, small SVD in FP64
+            struct W { double *Y, *Q, *X, *Ub; float *Y32, *Q32, *X32; };
+            std::vector<W> ws(rs.size());
+            auto mk32 = [&](const char* tag) {
+                auto g = std::make_unique<GemmStep<float>>(CFG_64x64, src.gen);
+                g->gp = src.gp;
+                g->batch.set_tag(tag);
+                g->label = std::string("gemm_gen_f32:") + tag;
+                g->label_tc = std::string("tc_tf32x4_gen:") + tag;
+                return g;
+            };
+            for (size_t i = 0; i < rs.size(); ++i) {
+                Block* b = rs[i];
+                ws[i].Y = plan.scratch((size_t)b->m * b->k);
+                ws[i].Q = plan.scratch((size_t)b->m * b->k);
+                ws[i].X = plan.scratch((size_t)b->n * b->k);
+                ws[i].Ub = plan.scratch((size_t)b->k * b->k);
+                ws[i].Y32 = plan.scratch_f((size_t)b->m * b->k);
+                ws[i].Q32 = plan.scratch_f(std::max((size_t)b->m, (size_t)b->n) * b->k);
+                ws[i].X32 = plan.scratch_f((size_t)b->n * b->k);
+            }
+            auto to64 = [&](const std::vector<std::tuple<float*, double*, int, int>>& l) {
+                auto st = std::make_unique<CopyStep>();
+                for (auto& t : l) st->t.h.push_back({std::get<0>(t), std::get<2>(t), std::get<1>(t), std::get<2>(t),
+                                                     std::get<2>(t), std::get<3>(t), 0, 1, 0});
+                st->t.upload(stream_);
+                plan.add(std::move(st));
+            };
+            auto to32 = [&](const std::vector<std::tuple<double*, float*, int, int>>& l) {
+                auto st = std::make_unique<CopyStep>();
+                for (auto& t : l) st->t.h.push_back({std::get<0>(t), std::get<2>(t), std::get<1>(t), std::get<2>(t),
+                                                     std::get<2>(t), std::get<3>(t), 0, 0, 1});
+                st->t.upload(stream_);
+                plan.add(std::move(st));
+            };
+            // Y = A_blk Omega  (compression.h:79), then Q = orthonormal basis of range(Y)
+            auto sketchY = [&](bool from_omega) {
+                auto g = mk32("build.sketch");
+                std::vector<std::tuple<float*, double*, int, int>> cv;
+                for (size_t i = 0; i < rs.size(); ++i) {
+                    Block* b = rs[i];
+                    const float* Bm = from_omega ? dOmega32.p + om32[b->slot] : ws[i].Q32;
+                    g->batch.add(b->m, b->k, b->n, 1.0f, nullptr, 0, OP_N, Bm, b->n, OP_N, 0.0f, ws[i].Y32, b->m,
+                                 nullptr, 0, b->r0, b->c0);
+                    cv.emplace_back(ws[i].Y32, ws[i].Y, b->m, b->k);
+                }
+                g->batch.finalize(stream_);
+                plan.add(std::move(g));
+                to64(cv);
+                std::vector<QrProblem> qr;
+                for (size_t i = 0; i < rs.size(); ++i)
+                    qr.push_back({ws[i].Y, rs[i]->m, rs[i]->m, rs[i]->k, ws[i].Q, rs[i]->m});
+                plan_cholqr3(plan, qr, stream_);
+            };
+            // X = A_blk^T Q (the projection, compression.h:87, and the power iteration's Z)
+            auto project = [&]() {
+                std::vector<std::tuple<double*, float*, int, int>> c32;
+                for (size_t i = 0; i < rs.size(); ++i) c32.emplace_back(ws[i].Q, ws[i].Q32, rs[i]->m, rs[i]->k);
+                to32(c32);
+                auto g = mk32("build.project");
+                std::vector<std::tuple<float*, double*, int, int>> cv;
+                for (size_t i = 0; i < rs.size(); ++i) {
+                    Block* b = rs[i];
+                    g->batch.add(b->n, b->k, b->m, 1.0f, nullptr, 0, OP_T, ws[i].Q32, b->m, OP_N, 0.0f, ws[i].X32, b->n,
+                                 nullptr, 0, b->r0, b->c0);
+                    cv.emplace_back(ws[i].X32, ws[i].X, b->n, b->k);
+                }
+                g->batch.finalize(stream_);
+                plan.add(std::move(g));
+                to64(cv);
+            };
+            sketchY(true);
+            for (int it = 0; it < opts_.power_iters; ++it) {  // extension
+                project();
+                std::vector<QrProblem> qr;
+                for (size_t i = 0; i < rs.size(); ++i) {
+                    double* Z = plan.scratch((size_t)rs[i]->n * rs[i]->k);
+                    qr.push_back({ws[i].X, rs[i]->n, rs[i]->n, rs[i]->k, Z, rs[i]->n});
+                }
+                plan_cholqr3(plan, qr, stream_);
+                std::vector<std::tuple<double*, float*, int, int>> c32;
+                for (size_t i = 0; i < rs.size(); ++i) c32.emplace_back(qr[i].Q, ws[i].Q32, rs[i]->n, rs[i]->k);
+                to32(c32);
+                sketchY(false);
+            }
+            project();
+            // SVD of Q^T A (compression.h:90): X = V_b S U_b^T, then U = Q U_b (compression.h:94)
+            std::vector<SvdProblem> sv;
+            for (size_t i = 0; i < rs.size(); ++i) {
+                Block* b = rs[i];
+                Node& cc = nodes_[b->ccol];
+                SvdProblem q{};
+                q.X = ws[i].X; q.ldx = b->n; q.rows = b->n; q.k = b->k;
+                q.L = dV.p + cc.offV; q.ldl = cc.len();
+                q.R = ws[i].Ub; q.ldr = b->k;
+                q.sigma = dSig.p + sig_off[b->slot];
+                q.rank = dRank.p + b->slot;
+                q.sort = true;
+                sv.push_back(q);
+            }
+            plan_gram_svd(plan, sv, opts_.tol, opts_.max_rank, stream_);
+            auto gU = std::make_unique<GemmStep<double>>();
+            for (size_t i = 0; i < rs.size(); ++i) {
+                Block* b = rs[i];
+                Node& cr = nodes_[b->crow];
+                gU->batch.add(b->m, b->k, b->k, 1.0, ws[i].Q, b->m, OP_N, ws[i].Ub, b->k, OP_N, 0.0,
+                              dU.p + cr.offU, cr.len());
+            }
+            gU->batch.finalize(stream_);
+            plan.add(std::move(gU));
+        } else if (!rs.empty()) {
             struct W { double *Y, *Q, *X, *Ub; };
             std::vector<W> ws(rs.size());
             auto mkA = [&]() {
@@ -734,6 +866,16 @@ void Engine::build_hodlr(const Source& src) {
     if (sig_total)
         HM_CUDA(cudaMemcpyAsync(sig.data(), dSig.p, sig_total * sizeof(double), cudaMemcpyDeviceToHost, stream_));
     HM_CUDA(cudaStreamSynchronize(stream_));
+    // kept rank of every block: the truncation rule's, or a fixed profile (set_rank_profile)
+    if (!fix12_.empty())
+        HM_CHECK(fix12_.size() == nodes_.size() && fix21_.size() == nodes_.size() && kind_ == HODLR &&
+                     sys_N_.size() == 1,
+                 HM_ERR_ARG, "rank profile: its node count does not match this HODLR tree");
+    for (auto& b : blocks) {
+        int r = std::min(ranks[b.slot], b.k);
+        if (!fix12_.empty()) r = std::max(1, std::min(b.k, (b.which == 0 ? fix12_ : fix21_)[b.node]));
+        ranks[b.slot] = r;
+    }
     std::vector<int> r12(nodes_.size(), 0), r21(nodes_.size(), 0);
     std::vector<double> s12, s21;
     size_t tot = 0;

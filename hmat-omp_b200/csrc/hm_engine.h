@@ -73,6 +73,12 @@ class Engine {
     const std::vector<Node>& nodes() const { return nodes_; }
 
     void set_stream(cudaStream_t s) { stream_ = s; }
+    // Fixed kept ranks for the next HODLR builds (B_12 / B_21 size per node, pre-order),
+    // instead of the truncation rule; empty vectors restore the rule.
+    void set_rank_profile(const std::vector<int>& r12, const std::vector<int>& r21) {
+        fix12_ = r12;
+        fix21_ = r21;
+    }
     void set_precision(int p) {
         if (p != opts_.precision) factored_ = false;
         opts_.precision = p;
@@ -225,6 +231,7 @@ class Engine {
     // kernels with positive scale and non-negative shift (positive definite radial
     // functions), set by the kernel builds; dense builds and imports stay false
     bool leaves_spd_ = false;
+    std::vector<int> fix12_, fix21_;   // fixed rank profile (empty: the truncation rule)
     static bool kernel_spd(int gen, double p0, double p1) {
         return (gen == GEN_GAUSSIAN || gen == GEN_COULOMB) && p0 > 0 && p1 >= 0;
     }

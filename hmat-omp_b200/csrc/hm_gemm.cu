@@ -584,7 +584,8 @@ static int pow2_ceil(long long v) {
 
 template <typename T>
 std::string GemmBatch<T>::choice() const {
-    return std::to_string(pipe_bn_) + "," + std::to_string(pipe_shape_) + "," + (use_tc_ || use_dmma_ ? "1" : "0");
+    return std::to_string(gen_tc_ ? gen_bn_ : pipe_bn_) + "," + std::to_string(pipe_shape_) + "," +
+           (use_tc_ || use_dmma_ ? "1" : "0");
 }
 
 // HM_FP64_BIG=1 gives FP64 batches without a table entry that would take the default
@@ -725,6 +726,9 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         } else if (kernel_mode_ == 0 && pipe_bn_ && tc_allowed_ && !has_chains_ && (!have_tuned || tuned.tc)) {
             finalize_tc(s, tc_any_k_);
         }
+        gen_tc_ = false;
+        if (gen_ != GEN_DENSE && cfg_ == CFG_64x64 && tc_allowed_ && kernel_mode_ != 2 && !h_.empty())
+            finalize_tc_gen(s);
     }
     if (!hz_.empty()) {
         dz_.alloc(hz_.size());
@@ -784,6 +788,61 @@ void GemmBatch<T>::finalize_tc(cudaStream_t s, bool force) {
     }
 }
 
+template <typename T>
+void GemmBatch<T>::finalize_tc_gen(cudaStream_t s) {
+    if constexpr (std::is_same<T, float>::value) {
+        static const bool dbg = std::getenv("HM_TC_DEBUG") != nullptr;
+        int nmax = 0;
+        for (auto& d : h_) nmax = std::max(nmax, d.n);
+        if (nmax > 128) return;
+        const int bn = nmax <= 32 ? 32 : nmax <= 64 ? 64 : nmax <= 96 ? 96 : 128;
+        std::vector<GemmDesc<float>> dv(h_);
+        int tt = 0;
+        for (auto& d : dv) {
+            if (!tc::tma_ok(d, true)) {
+                if (dbg) fprintf(stderr, "[tc] %s: sketch operand not TMA-addressable (ldb=%d)\n", tag_.c_str(), d.ldb);
+                return;
+            }
+            d.tiles_m = ceil_div(d.m, tc::BM);
+            d.tiles_n = ceil_div(d.n, bn);
+            d.tile0 = tt;
+            tt += d.tiles_m * d.tiles_n * d.ksplit;
+        }
+        if (tt == 0) return;
+        std::vector<CUtensorMap> maps;
+        if (!tc::encode_maps(dv, bn, maps, true)) {
+            if (dbg) fprintf(stderr, "[tc] %s: tensor-map encoding refused\n", tag_.c_str());
+            return;
+        }
+        std::vector<int> tp((size_t)tt);
+        for (size_t i = 0; i < dv.size(); ++i)
+            std::fill(tp.begin() + dv[i].tile0, tp.begin() + dv[i].tile0 + dv[i].tiles_m * dv[i].tiles_n * dv[i].ksplit,
+                      (int)i);
+        tcd_.alloc(dv.size());
+        tct_.alloc(tp.size());
+        tcmaps_.alloc(maps.size() * sizeof(CUtensorMap));
+        tcstatus_.alloc(1);
+        tcstatus_.zero(s);
+        HM_CUDA(cudaMemcpyAsync(tcd_.p, dv.data(), dv.size() * sizeof(GemmDesc<float>), cudaMemcpyHostToDevice, s));
+        HM_CUDA(cudaMemcpyAsync(tct_.p, tp.data(), tp.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        HM_CUDA(cudaMemcpyAsync(tcmaps_.p, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s));
+        HM_CUDA(cudaStreamSynchronize(s));   // the host vectors are locals
+        tc_tiles_ = tt;
+        gen_bn_ = bn;
+        gen_tc_ = true;
+        use_tc_ = true;
+    }
+}
+
+template <int GEN>
+static void launch_tc_gen(int bn, int tiles, int sms, cudaStream_t s, const GemmDesc<float>* d, const int* tp,
+                          const CUtensorMap* maps, int* st, int stall, const GenParams& gp) {
+    if (bn == 32) tc::launch<32, GEN>(tiles, sms, s, d, tp, maps, st, stall, gp);
+    else if (bn == 64) tc::launch<64, GEN>(tiles, sms, s, d, tp, maps, st, stall, gp);
+    else if (bn == 96) tc::launch<96, GEN>(tiles, sms, s, d, tp, maps, st, stall, gp);
+    else tc::launch<128, GEN>(tiles, sms, s, d, tp, maps, st, stall, gp);
+}
+
 static int sm_count() {
     static int n = 0;
     if (!n) {
@@ -805,6 +864,7 @@ void GemmBatch<T>::clear() {
     tct_.release();
     tcmaps_.release();
     use_tc_ = false;
+    gen_tc_ = false;
     total_tiles_ = 0;
     finalized_ = false;
 }
@@ -852,6 +912,14 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) cons
             const auto* maps = reinterpret_cast<const CUtensorMap*>(tcmaps_.p);
             int* st = status ? status : tcstatus_.p;
             const int sms = sm_count();
+            if (gen_tc_) {
+                const int stall = tc_stall_ ? 1 : 0;
+                if (gen_ == GEN_CAUCHY) launch_tc_gen<GEN_CAUCHY>(gen_bn_, tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall, gp);
+                else if (gen_ == GEN_GAUSSIAN) launch_tc_gen<GEN_GAUSSIAN>(gen_bn_, tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall, gp);
+                else launch_tc_gen<GEN_COULOMB>(gen_bn_, tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall, gp);
+                HM_CUDA(cudaGetLastError());
+                return;
+            }
             if (pipe_bn_ == 32) tc::launch<32>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);
             else if (pipe_bn_ == 64) tc::launch<64>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);
             else if (pipe_bn_ == 96) tc::launch<96>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);

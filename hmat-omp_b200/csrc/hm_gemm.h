@@ -123,6 +123,9 @@ class GemmBatch {
     // Upload the table (once); later launches reuse it (and may be graph-captured).
     void finalize(cudaStream_t s);
     void finalize_tc(cudaStream_t s, bool force = false);
+    // FP32 batches whose A is generated from a kernel: the tcgen05 kernel evaluates A's
+    // entries into its stages (the TMA brings B only)
+    void finalize_tc_gen(cudaStream_t s);
     bool on_tensor_cores() const { return use_tc_; }
     bool on_fp64_mma() const { return use_dmma_; }
     // Kernel selection for finalize: 0 the built-in rules and tile table; 1 the tensor-core
@@ -183,6 +186,8 @@ class GemmBatch {
     // FP32 batches with long k on the tensor cores: tile count, tables, tensor maps
     bool use_tc_ = false, tc_allowed_ = true, tc_stall_ = false, tc_any_k_ = false;
     int kernel_mode_ = 0;
+    bool gen_tc_ = false;   // generated-A batch on the tensor cores
+    int gen_bn_ = 0;        // its tile width
     int tc_tiles_ = 0;
     DBuf<GemmDesc<T>> tcd_;
     DBuf<int> tct_;

@@ -217,6 +217,33 @@ __device__ __forceinline__ bool wait_bar_warp(uint32_t b, uint32_t parity, volat
     return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
+// Entry (r, c) of a generated operator for the tensor-core path: coordinate differences
+// and squared distances in FP64 (no cancellation for close points), the exp / sqrt /
+// reciprocal in FP32 (the hi/lo TF32 split carries FP32 accuracy, no more).
+template <int GEN>
+__device__ __forceinline__ float gen_entry_f32(const GenParams& g, int r, int c) {
+    const double p0 = g.p0v ? g.p0v[g.row_sys[r]] : g.p0;
+    const double p1 = g.p1v ? g.p1v[g.row_sys[r]] : g.p1;
+    float v = 0.f;
+    if constexpr (GEN == GEN_CAUCHY) {
+        v = 1.0f / (float)(g.pts[r] - g.pts[g.N + c]);
+        if (r == c) v += (float)p0;
+    } else {
+        double d2 = 0.0;
+        for (int t = 0; t < g.dim; ++t) {
+            const double d = g.pts[(size_t)r * g.dim + t] - g.pts[(size_t)c * g.dim + t];
+            d2 = fma(d, d, d2);
+        }
+        if constexpr (GEN == GEN_GAUSSIAN) {
+            v = __expf(-(float)(d2 / (2.0 * p0 * p0)));
+        } else {
+            v = 1.0f / (sqrtf((float)d2) + (float)p0);
+        }
+        if (r == c) v += (float)p1;
+    }
+    return v;
+}
+
 // C goes through the TMA (load for beta != 0, store / reduce-add) only when aligned;
 // otherwise the epilogue reads and writes it row by row
 __host__ __device__ inline bool c_tma_ok(const float* C, int ldc) {
@@ -248,10 +275,13 @@ __device__ __forceinline__ TileInfo decode(const GemmDesc<float>* __restrict__ d
     return t;
 }
 
-template <int BN>
+// GEN != GEN_DENSE: A is not read from memory but evaluated by the converter warps from
+// the kernel generator (entry (ga_r0 + i, ga_c0 + k) of op(A), or its transpose for
+// opA = OP_T) straight into the K-major stage layout; the TMA brings only B.
+template <int BN, int GEN>
 __global__ void __launch_bounds__(NT, 1)
 gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restrict__ tile_problem, int ntiles,
-                 const CUtensorMap* __restrict__ tmaps, int* status, int stall) {
+                 const CUtensorMap* __restrict__ tmaps, int* status, int stall, const GenParams gp) {
     using S = Shape<BN>;
     constexpr int ST = S::ST;
     extern __shared__ unsigned char smraw[];
@@ -314,7 +344,7 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
             for (int tile = blockIdx.x; tile < ntiles && ok && !stall; tile += gridDim.x) {
                 const TileInfo ti = decode<BN>(descs, tile_problem, tile);
                 const GemmDesc<float>& D = descs[ti.p];
-                const bool a_mn = D.opA == OP_N, b_mn = D.opB == OP_T;
+                const bool a_mn = GEN == GEN_DENSE && D.opA == OP_N, b_mn = D.opB == OP_T;
                 const CUtensorMap* ma = tmaps + 3 * ti.p;
                 const CUtensorMap* mb = ma + 1;
                 for (int kt = 0; kt < ti.nk; ++kt, ++slot) {
@@ -323,12 +353,14 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
                     const uint32_t base = stage0 + (uint32_t)st * S::STAGE;
                     const uint32_t bbase = base + 2 * S::A_BYTES;
                     const int k0 = ti.kb + kt * BK;
-                    mbar_expect(raw(st), (uint32_t)(S::A_BYTES + S::B_BYTES));
-                    if (a_mn) {
+                    mbar_expect(raw(st), (uint32_t)((GEN == GEN_DENSE ? S::A_BYTES : 0) + S::B_BYTES));
+                    if constexpr (GEN == GEN_DENSE) {
+                        if (a_mn) {
 #pragma unroll
-                        for (int c = 0; c < BM / 32; ++c) tma2d(base + 4096u * c, ma, ti.m0 + 32 * c, k0, raw(st));
-                    } else {
-                        tma2d(base, ma, k0, ti.m0, raw(st));
+                            for (int c = 0; c < BM / 32; ++c) tma2d(base + 4096u * c, ma, ti.m0 + 32 * c, k0, raw(st));
+                        } else {
+                            tma2d(base, ma, k0, ti.m0, raw(st));
+                        }
                     }
                     if (b_mn) {
 #pragma unroll
@@ -350,14 +382,16 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
         bool ok = true;
         for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
             const TileInfo ti = decode<BN>(descs, tile_problem, tile);
+            const GemmDesc<float>& D = descs[ti.p];
             for (int kt = 0; kt < ti.nk; ++kt, ++slot) {
                 const int st = slot % ST;
                 if (!wait_bar_warp(raw(st), (slot / ST) & 1, abort_flag, status, lim)) { ok = false; break; }
                 const uint32_t base = stage0 + (uint32_t)st * S::STAGE;
                 constexpr int CA = S::A_BYTES / 16, CB = S::B_BYTES / 16;
                 constexpr int NCH = (CA + CB + NCONV - 1) / NCONV;
-                // all of this thread's 16-byte chunks are read first (independent loads),
-                // then split and written back
+                const int k0 = ti.kb + kt * BK;
+                // all of this thread's 16-byte chunks are read (or, for a generated A,
+                // evaluated) first, then split and written back
                 float x[NCH][4];
                 uint32_t off[NCH], lof[NCH];
 #pragma unroll
@@ -366,9 +400,25 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
                     if (e >= CA + CB) continue;
                     off[i] = e < CA ? (uint32_t)e * 16 : (uint32_t)(2 * S::A_BYTES + (e - CA) * 16);
                     lof[i] = off[i] + (e < CA ? S::A_BYTES : S::B_BYTES);
-                    asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];\n"
-                                 : "=f"(x[i][0]), "=f"(x[i][1]), "=f"(x[i][2]), "=f"(x[i][3])
-                                 : "r"(base + off[i]));
+                    if (GEN != GEN_DENSE && e < CA) {
+                        // K-major line r (128 bytes), physical chunk e % 8 = logical k-group
+                        // ((e % 8) ^ (r % 8)) of the 128-byte swizzle
+                        const int r = e >> 3, kg = (e & 7) ^ (r & 7);
+                        const int row = ti.m0 + r;
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int kk = k0 + 4 * kg + u;
+                            float v = 0.f;
+                            if (row < D.m && kk < ti.ke)
+                                v = D.opA == OP_N ? gen_entry_f32<GEN>(gp, D.ga_r0 + row, D.ga_c0 + kk)
+                                                  : gen_entry_f32<GEN>(gp, D.ga_r0 + kk, D.ga_c0 + row);
+                            x[i][u] = v;
+                        }
+                    } else {
+                        asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];\n"
+                                     : "=f"(x[i][0]), "=f"(x[i][1]), "=f"(x[i][2]), "=f"(x[i][3])
+                                     : "r"(base + off[i]));
+                    }
                 }
 #pragma unroll
                 for (int i = 0; i < NCH; ++i) {
@@ -399,7 +449,7 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
             for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
                 const TileInfo ti = decode<BN>(descs, tile_problem, tile);
                 const GemmDesc<float>& D = descs[ti.p];
-                const bool a_mn = D.opA == OP_N, b_mn = D.opB == OP_T;
+                const bool a_mn = GEN == GEN_DENSE && D.opA == OP_N, b_mn = D.opB == OP_T;
                 const int nt = min(BN, D.n - ti.n0);
                 const int ninst = (nt + 15) / 16 * 16;
                 const int acc = accn & 1;
@@ -556,26 +606,27 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
     }
 }
 
-template <int BN>
+template <int BN, int GEN = GEN_DENSE>
 void launch(int tiles, int sms, cudaStream_t s, const GemmDesc<float>* d, const int* tile_problem,
-            const CUtensorMap* tmaps, int* status, int stall) {
+            const CUtensorMap* tmaps, int* status, int stall, const GenParams& gp = GenParams()) {
     using S = Shape<BN>;
     static size_t cur = 0;
-    ensure_dyn_smem(gemm_tc32_kernel<BN>, S::SMEM, cur);
+    ensure_dyn_smem(gemm_tc32_kernel<BN, GEN>, S::SMEM, cur);
     const int grid = std::max(1, std::min(tiles, sms));
-    gemm_tc32_kernel<BN><<<grid, NT, S::SMEM, s>>>(d, tile_problem, tiles, tmaps, status, stall);
+    gemm_tc32_kernel<BN, GEN><<<grid, NT, S::SMEM, s>>>(d, tile_problem, tiles, tmaps, status, stall, gp);
 }
 
 // Whether the tensor-core kernel can take a problem: the TMA wants 16-byte aligned bases
 // and leading dimensions that are multiples of 4 floats.
-inline bool tma_ok(const GemmDesc<float>& d) {
-    return (reinterpret_cast<uintptr_t>(d.A) & 15) == 0 && (reinterpret_cast<uintptr_t>(d.B) & 15) == 0 &&
-           d.lda % 4 == 0 && d.ldb % 4 == 0 && d.kscale == nullptr;
+inline bool tma_ok(const GemmDesc<float>& d, bool gen_a = false) {
+    return (gen_a || ((reinterpret_cast<uintptr_t>(d.A) & 15) == 0 && d.lda % 4 == 0)) &&
+           (reinterpret_cast<uintptr_t>(d.B) & 15) == 0 && d.ldb % 4 == 0 && d.kscale == nullptr;
 }
 
 // Tensor maps of every problem's operands (3 per problem: A, B, C), in the box shapes
 // the kernel issues.  Returns false if the driver refuses one.
-inline bool encode_maps(const std::vector<GemmDesc<float>>& probs, int bn, std::vector<CUtensorMap>& out) {
+inline bool encode_maps(const std::vector<GemmDesc<float>>& probs, int bn, std::vector<CUtensorMap>& out,
+                        bool gen_a = false) {
     static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
     if (!enc) {
         cudaDriverEntryPointQueryResult q;
@@ -589,7 +640,7 @@ inline bool encode_maps(const std::vector<GemmDesc<float>>& probs, int bn, std::
     for (size_t i = 0; i < probs.size(); ++i) {
         const GemmDesc<float>& d = probs[i];
         const cuuint64_t k = (cuuint64_t)std::max(d.k, 1);
-        for (int w = 0; w < 2; ++w) {
+        for (int w = gen_a ? 1 : 0; w < 2; ++w) {   // a generated A has no tensor map
             const bool mn = w == 0 ? d.opA == OP_N : d.opB == OP_T;
             const cuuint64_t rows = (cuuint64_t)(w == 0 ? d.m : d.n);
             const int ld = w == 0 ? d.lda : d.ldb;

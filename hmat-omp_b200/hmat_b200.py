@@ -79,6 +79,7 @@ def load() -> C.CDLL:
         getattr(L, f).argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int]
     L.hm_hodlr_build_from_dense_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
     PP = C.POINTER(C.c_void_p)
+    L.hm_set_rank_profile.argtypes = [C.c_void_p, C.c_int, _ip, _ip]
     L.hm_hodlr_import.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip, PP, PP, PP, PP, PP]
     L.hm_num_nodes.argtypes = [C.c_void_p]
     L.hm_export_tree.argtypes = [C.c_void_p] + [_ip] * 6
@@ -359,6 +360,16 @@ class _Handle:
         if out.size:
             self._check(self._L.hm_get_gradient(self._h, node, which, _d(out), C.byref(r), C.byref(c)))
         return out.reshape(c.value, r.value).T.copy()
+
+    def set_rank_profile(self, rank12=None, rank21=None) -> None:
+        """Fix each block's kept rank for the next builds (None clears): node i keeps
+        rank12[i] / rank21[i] singular triplets, e.g. tree()["rank12"] of an earlier build."""
+        if rank12 is None:
+            self._check(self._L.hm_set_rank_profile(self._h, 0, None, None))
+            return
+        a = np.ascontiguousarray(rank12, dtype=np.int32)
+        b = np.ascontiguousarray(rank21, dtype=np.int32)
+        self._check(self._L.hm_set_rank_profile(self._h, a.size, a.ctypes.data_as(_ip), b.ctypes.data_as(_ip)))
 
     def save(self, path: str) -> None:
         """Write the built operator to `path` (hm_save)."""

@@ -150,6 +150,16 @@ HM_API int hm_hss_build_from_kernel(hm_handle* h, int kernel, const double* poin
 HM_API int hm_save(hm_handle* h, const char* path);
 HM_API int hm_load(hm_handle* h, const char* path);
 
+/* Fix the kept rank of every compressed block for the next HODLR builds on this handle
+ * (no counterpart in the reference, whose compress_rsvd truncates by tolerance,
+ * compression.h:42-46): node i's B_12 / B_21 keep rank12[i] / rank21[i] singular triplets
+ * (pre-order, as hm_export_tree lists them; capped by the sketch width, at least 1)
+ * instead of #{S > tol S_0}.  A profile exported from one build and set before rebuilding
+ * with perturbed kernel parameters gives an operator that is a smooth function of those
+ * parameters (finite differences without re-truncation).  nnodes must equal the next
+ * tree's node count (HM_ERR_ARG at build otherwise); NULL arrays or nnodes <= 0 clear it. */
+HM_API int hm_set_rank_profile(hm_handle* h, int nnodes, const int* rank12, const int* rank21);
+
 /* Upload a HODLR tree built elsewhere (e.g. by HODLRMatrix::build_from_dense) so the
  * device path can multiply/solve with exactly those factors.  Nodes in pre-order
  * (root, left subtree, right subtree); per node pointers to host column-major

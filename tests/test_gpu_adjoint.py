@@ -172,3 +172,35 @@ def test_factor_gradients_against_finite_differences():
         fd = (4 * central(eps) - central(2 * eps)) / 3
         setattr(node, attr, M0)
         assert abs(G[i, j] - fd) <= 1e-5 * max(abs(fd), 1e-3 * abs(L)), (attr, G[i, j], fd)
+
+
+def test_rank_profile_freezes_ranks():
+    """hm_set_rank_profile: a rebuild at a perturbed length scale keeps the ranks of the
+    h0 build exactly; a raised profile is honoured up to the sketch width; a profile for
+    another tree is refused."""
+    N = 8192
+    pts = points(N)
+    m = build(N, pts=pts)
+    tr = m.tree()
+    r12, r21 = tr["rank12"].copy(), tr["rank21"].copy()
+    m2 = H.HODLRMatrix(1e-12, rsvd_rank=RANK, max_rank=RANK, oversample=10, power_iters=1,
+                       sketch=H.SKETCH_DEVICE_NORMAL, seed=1)
+    m2.set_rank_profile(r12, r21)
+    m2.build_from_kernel(H.KERNEL_GAUSSIAN, pts.reshape(-1, 1), [H0 * 1.01, SHIFT], LEAF)
+    t2 = m2.tree()
+    assert np.array_equal(t2["rank12"], r12) and np.array_equal(t2["rank21"], r21)
+    inner = tr["is_leaf"] == 0
+    up12, up21 = r12.copy(), r21.copy()
+    up12[inner] += 3
+    up21[inner] += 3
+    m2.set_rank_profile(up12, up21)
+    m2.build_from_kernel(H.KERNEL_GAUSSIAN, pts.reshape(-1, 1), [H0, SHIFT], LEAF)
+    t3 = m2.tree()
+    assert np.all(t3["rank12"][inner] == np.minimum(up12[inner], RANK + 10))
+    # the raised ranks keep (tiny) extra singular triplets: same operator to ~1e-12
+    x = np.random.default_rng(3).standard_normal(N)
+    assert O.rel_err(m.multiply(x), m2.multiply(x)) < 1e-10
+    m2.set_rank_profile(r12[:-1], r21[:-1])
+    with pytest.raises(H.HmError) as e:
+        m2.build_from_kernel(H.KERNEL_GAUSSIAN, pts.reshape(-1, 1), [H0, SHIFT], LEAF)
+    assert e.value.code == H.HM_ERR_ARG
