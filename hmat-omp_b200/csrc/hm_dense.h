@@ -189,29 +189,37 @@ class Plan {
 };
 bool graphs_enabled();
 
-// Which labelled FP32 steps may run on the tensor cores.  By default the three bulk
-// updates of the factorization (leaf_apply, update_project, update_small).  The rest of
-// the mixed-precision path feeds the refinement more directly: on the tensor cores the
-// projection K = V^T Q (amplified by the capacitance matrices) or the solve sweeps
-// weaken the refinement contraction (measured at N = 2^18, 64 right-hand sides: residual
-// after two sweeps 5.4e-11 with the default set, 2.6e-10 with K added, 1.1e-10 with the
-// solve's leaf step added; 1.3e-11 with no tensor cores).  HM_FP32_TENSOR_CORES
-// overrides: "0" none, "1" every eligible step, otherwise a comma-separated label list.
+// Which labelled FP32 steps may run on the tensor cores.  By default the bulk updates of
+// the factorization (leaf_apply, update_project, update_small, update_correct) and the
+// solve's correction (solve.correct: k = a node's rank, short).  The rest of the
+// mixed-precision path feeds the refinement more directly: on the tensor cores the
+// projection K = V^T Q (amplified by the capacitance matrices) or the solve's long-k
+// steps weaken the refinement contraction (measured at N = 2^18, 64 right-hand sides:
+// residual after two sweeps 2.6e-10 with K added, 1.1e-10 with the solve's leaf step
+// added, against 5.5e-11 with the default set).  HM_FP32_TENSOR_CORES overrides: "0"
+// none, "1" every eligible step, otherwise a comma-separated label list.
 inline bool tensor_cores_allowed(const char* label) {
     const char* e = std::getenv("HM_FP32_TENSOR_CORES");
     const std::string l(label);
-    if (!e || !*e) return l == "factor.leaf_apply" || l == "factor.update_project" || l == "factor.update_small";
+    if (!e || !*e)
+        return l == "factor.leaf_apply" || l == "factor.update_project" || l == "factor.update_small" ||
+               l == "factor.update_correct" || l == "solve.correct";
     if (e[0] == '1' && e[1] == 0) return true;
     if (e[0] == '0' && e[1] == 0) return false;
     const std::string list = std::string(",") + e + ",";
     return list.find("," + l + ",") != std::string::npos;
 }
 
-// Whether HM_FP32_TENSOR_CORES names this label explicitly (then the tensor-core kernel
-// takes the batch even when its inner dimension is short).
+// Whether the tensor-core kernel takes this label's batches even when their inner
+// dimension is short (fewer than 4 k-blocks per tile): the default short-k steps, or the
+// labels HM_FP32_TENSOR_CORES names explicitly.
 inline bool tensor_cores_named(const char* label) {
     const char* e = std::getenv("HM_FP32_TENSOR_CORES");
-    if (!e || !*e || (e[0] == '1' && e[1] == 0) || (e[0] == '0' && e[1] == 0)) return false;
+    if (!e || !*e) {   // the default short-k steps (3 k-blocks of 32 per tile)
+        const std::string l(label);
+        return l == "factor.update_correct" || l == "solve.correct";
+    }
+    if ((e[0] == '1' && e[1] == 0) || (e[0] == '0' && e[1] == 0)) return false;
     const std::string list = std::string(",") + e + ",";
     return list.find("," + std::string(label) + ",") != std::string::npos;
 }

@@ -25,6 +25,9 @@
 
 namespace hm {
 
+// Rows of P in the FP32 factor store: p1 rounded up to a multiple of 4, then p2.
+static inline int padded_p(int p1, int p2) { return (p1 + 3) / 4 * 4 + p2; }
+
 template <> Plan& Engine::solve_plan<double>(FactorStore<double>& fs, const std::vector<int>& sc);
 template <> Plan& Engine::solve_plan<float>(FactorStore<float>& fs, const std::vector<int>& sc);
 
@@ -1420,8 +1423,13 @@ void Engine::plan_factor(FactorStore<T>& fs) {
         const int p = L.rankU + R.rankU, q = L.rankV + R.rankV;
         n.offM = offM;
         offM += (size_t)q * q;
-        n.offP = offP;
-        offP += (size_t)p * q;
+        if constexpr (F32) {
+            n.offP32 = offP;
+            offP += (size_t)padded_p(L.rankU, R.rankU) * q;
+        } else {
+            n.offP = offP;
+            offP += (size_t)p * q;
+        }
     }
     size_t totU = 1, totV = 1, totD = 1;
     for (auto& n : nodes_) {
@@ -1553,18 +1561,22 @@ void Engine::plan_factor(FactorStore<T>& fs) {
                 ident->t.h.push_back({Minv, q, q1, q, 1.0});
                 if (q2) gTop->batch.add(q1, q, q2, -1.0, X, q, OP_N, Minv + q1, q, OP_N, 1.0, Minv, q);
             }
-            // P = B^ Minv: P[0:p1,:] = B12 Minv[q1:,:], P[p1:,:] = B21 Minv[0:q1,:]
+            // P = B^ Minv: P[0:p1,:] = B12 Minv[q1:,:], P[o2:o2+p2,:] = B21 Minv[0:q1,:]
+            // (o2 = p1 in FP64; in FP32 p1 rounded up to 4, the gap rows zero)
+            const int pp = F32 ? padded_p(p1, p2) : p, o2 = F32 ? pp - p2 : p1;
             double* P64;
             if constexpr (F32) {
-                P64 = lp.scratch(std::max<size_t>((size_t)p * q, 1));
-                if ((size_t)p * q) cvP->t.h.push_back(flat_copy(P64, false, fs.P.p + n.offP, true, (size_t)p * q));
+                P64 = lp.scratch(std::max<size_t>((size_t)pp * q, 1));
+                if (o2 > p1 && q) ident->t.h.push_back({P64 + p1, pp, o2 - p1, q, 0.0});
+                if ((size_t)pp * q) cvP->t.h.push_back(flat_copy(P64, false, fs.P.p + n.offP32, true, (size_t)pp * q));
             } else {
                 P64 = fs.P.p + n.offP;
             }
-            gP->batch.add(p1, q, q2, 1.0, B12, p1, OP_N, Minv + q1, q, OP_N, 0.0, P64, p);
-            gP->batch.add(p2, q, q1, 1.0, B21, p2, OP_N, Minv, q, OP_N, 0.0, P64 + p1, p);
+            gP->batch.add(p1, q, q2, 1.0, B12, p1, OP_N, Minv + q1, q, OP_N, 0.0, P64, pp);
+            gP->batch.add(p2, q, q1, 1.0, B21, p2, OP_N, Minv, q, OP_N, 0.0, P64 + o2, pp);
             // every basis block on n's path: W <- A_n^{-1} W (given blockdiag-solved W)
-            const T* Pn = fs.P.p + n.offP;
+            const T* Pn = fs.P.p + (F32 ? n.offP32 : n.offP);
+            const int ldD = F32 ? (pp + 3) / 4 * 4 : p;
             for (int c : path_of(id)) {
                 const Node& C = nodes_[c];
                 const int w = C.rankU;
@@ -1573,14 +1585,14 @@ void Engine::plan_factor(FactorStore<T>& fs) {
                 const int ldw = C.len();
                 T* Tt = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)q * w, 1)))
                             : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)q * w, 1)));
-                T* Dt = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)p * w, 1)))
-                            : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)p * w, 1)));
+                T* Dt = F32 ? reinterpret_cast<T*>(lp.scratch_f(std::max<size_t>((size_t)ldD * w, 1)))
+                            : reinterpret_cast<T*>(lp.scratch(std::max<size_t>((size_t)ldD * w, 1)));
                 gT->batch.add(q1, w, L.len(), T(1), Vt + L.offV, L.len(), OP_T, W, ldw, OP_N, T(0), Tt, q);
                 gT->batch.add(q2, w, R.len(), T(1), Vt + R.offV, R.len(), OP_T, W + L.len(), ldw, OP_N,
                               T(0), Tt + q1, q);
-                gD->batch.add(p, w, q, T(1), Pn, p, OP_N, Tt, q, OP_N, T(0), Dt, p);
-                gC->batch.add(L.len(), w, p1, T(-1), fs.Q.p + L.offU, L.len(), OP_N, Dt, p, OP_N, T(1), W, ldw);
-                gC->batch.add(R.len(), w, p2, T(-1), fs.Q.p + R.offU, R.len(), OP_N, Dt + p1, p, OP_N,
+                gD->batch.add(pp, w, q, T(1), Pn, pp, OP_N, Tt, q, OP_N, T(0), Dt, ldD);
+                gC->batch.add(L.len(), w, p1, T(-1), fs.Q.p + L.offU, L.len(), OP_N, Dt, ldD, OP_N, T(1), W, ldw);
+                gC->batch.add(R.len(), w, p2, T(-1), fs.Q.p + R.offU, R.len(), OP_N, Dt + o2, ldD, OP_N,
                               T(1), W + L.len(), ldw);
             }
         }
@@ -1752,14 +1764,17 @@ static void add_solve(Plan& pl, const std::vector<Node>& nodes, const std::vecto
             if (s == 0) continue;
             T* Tt = F32 ? reinterpret_cast<T*>(pl.scratch_f(std::max<size_t>((size_t)q * s, 1)))
                         : reinterpret_cast<T*>(pl.scratch(std::max<size_t>((size_t)q * s, 1)));
-            T* Dt = F32 ? reinterpret_cast<T*>(pl.scratch_f(std::max<size_t>((size_t)p * s, 1)))
-                        : reinterpret_cast<T*>(pl.scratch(std::max<size_t>((size_t)p * s, 1)));
+            // FP32: P in its padded layout (second block at o2 = p1 rounded up to 4)
+            const int pp = F32 ? padded_p(p1, p2) : p, o2 = F32 ? pp - p2 : p1;
+            const int ldD = F32 ? (pp + 3) / 4 * 4 : p;
+            T* Dt = F32 ? reinterpret_cast<T*>(pl.scratch_f(std::max<size_t>((size_t)ldD * s, 1)))
+                        : reinterpret_cast<T*>(pl.scratch(std::max<size_t>((size_t)ldD * s, 1)));
             gT->batch.add(q1, s, L.len(), T(1), Vt + L.offV, L.len(), OP_T, Z + L.start, N, OP_N, T(0), Tt, q);
             gT->batch.add(q2, s, R.len(), T(1), Vt + R.offV, R.len(), OP_T, Z + R.start, N, OP_N, T(0),
                           Tt + q1, q);
-            gD->batch.add(p, s, q, T(1), P + n.offP, p, OP_N, Tt, q, OP_N, T(0), Dt, p);
-            gC->batch.add(L.len(), s, p1, T(-1), Q + L.offU, L.len(), OP_N, Dt, p, OP_N, T(1), Z + L.start, N);
-            gC->batch.add(R.len(), s, p2, T(-1), Q + R.offU, R.len(), OP_N, Dt + p1, p, OP_N, T(1),
+            gD->batch.add(pp, s, q, T(1), P + (F32 ? n.offP32 : n.offP), pp, OP_N, Tt, q, OP_N, T(0), Dt, ldD);
+            gC->batch.add(L.len(), s, p1, T(-1), Q + L.offU, L.len(), OP_N, Dt, ldD, OP_N, T(1), Z + L.start, N);
+            gC->batch.add(R.len(), s, p2, T(-1), Q + R.offU, R.len(), OP_N, Dt + o2, ldD, OP_N, T(1),
                           Z + R.start, N);
         }
         gT->batch.finalize(st);

@@ -30,6 +30,9 @@ struct Node {
     size_t offB12 = 0, offB21 = 0;
     // factor storage (internal): Minv ((q1+q2)^2, FP64) and P ((p1+p2) x (q1+q2))
     size_t offM = 0, offP = 0;
+    // FP32 factor store: P with a zero gap after its first block (rows p1 .. p1 rounded up
+    // to 4), so delta's second block starts 16-byte aligned for the tensor-core kernel
+    size_t offP32 = 0;
 };
 
 class Engine;
