@@ -244,6 +244,17 @@ __device__ __forceinline__ float gen_entry_f32(const GenParams& g, int r, int c)
     return v;
 }
 
+// The same entry from a squared distance d2 (symmetric kernels; r, c: global indices).
+template <int GEN>
+__device__ __forceinline__ float gen_from_d2(const GenParams& g, int r, int c, double d2) {
+    const double p0 = g.p0v ? g.p0v[g.row_sys[r]] : g.p0;
+    float v;
+    if constexpr (GEN == GEN_GAUSSIAN) v = __expf(-(float)(d2 / (2.0 * p0 * p0)));
+    else v = 1.0f / (sqrtf((float)d2) + (float)p0);
+    if (r == c) v += (float)(g.p1v ? g.p1v[g.row_sys[r]] : g.p1);
+    return v;
+}
+
 // C goes through the TMA (load for beta != 0, store / reduce-add) only when aligned;
 // otherwise the epilogue reads and writes it row by row
 __host__ __device__ inline bool c_tma_ok(const float* C, int ldc) {
@@ -402,17 +413,42 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
                     lof[i] = off[i] + (e < CA ? S::A_BYTES : S::B_BYTES);
                     if (GEN != GEN_DENSE && e < CA) {
                         // K-major line r (128 bytes), physical chunk e % 8 = logical k-group
-                        // ((e % 8) ^ (r % 8)) of the 128-byte swizzle
+                        // ((e % 8) ^ (r % 8)) of the 128-byte swizzle.  A thread's chunks all
+                        // have the same k-group (r % 8 = (t / 8) % 8), so for the symmetric
+                        // kernels in 1-D or 2-D the four column points are loaded once per
+                        // stage and each row point once per chunk.
                         const int r = e >> 3, kg = (e & 7) ^ (r & 7);
                         const int row = ti.m0 + r;
+                        if ((GEN == GEN_GAUSSIAN || GEN == GEN_COULOMB) && gp.dim <= 2) {
+                            const bool nt = D.opA == OP_N;
+                            const int rowg = (nt ? D.ga_r0 : D.ga_c0) + row;   // the tile row's point
+                            const int colg0 = (nt ? D.ga_c0 : D.ga_r0) + k0 + 4 * kg;
+                            const bool two = gp.dim == 2;
+                            const double rx = row < D.m ? gp.pts[(size_t)rowg * gp.dim] : 0.0;
+                            const double ry = (row < D.m && two) ? gp.pts[(size_t)rowg * 2 + 1] : 0.0;
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const int kk = k0 + 4 * kg + u;
-                            float v = 0.f;
-                            if (row < D.m && kk < ti.ke)
-                                v = D.opA == OP_N ? gen_entry_f32<GEN>(gp, D.ga_r0 + row, D.ga_c0 + kk)
-                                                  : gen_entry_f32<GEN>(gp, D.ga_r0 + kk, D.ga_c0 + row);
-                            x[i][u] = v;
+                            for (int u = 0; u < 4; ++u) {
+                                const int kk = k0 + 4 * kg + u;
+                                float v = 0.f;
+                                if (row < D.m && kk < ti.ke) {
+                                    const int cg = colg0 + u;
+                                    const double dx = rx - gp.pts[(size_t)cg * gp.dim];
+                                    const double dy = two ? ry - gp.pts[(size_t)cg * 2 + 1] : 0.0;
+                                    v = gen_from_d2<GEN == GEN_GAUSSIAN ? GEN_GAUSSIAN : GEN_COULOMB>(
+                                        gp, rowg, cg, fma(dx, dx, dy * dy));
+                                }
+                                x[i][u] = v;
+                            }
+                        } else {
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                const int kk = k0 + 4 * kg + u;
+                                float v = 0.f;
+                                if (row < D.m && kk < ti.ke)
+                                    v = D.opA == OP_N ? gen_entry_f32<GEN>(gp, D.ga_r0 + row, D.ga_c0 + kk)
+                                                      : gen_entry_f32<GEN>(gp, D.ga_r0 + kk, D.ga_c0 + row);
+                                x[i][u] = v;
+                            }
                         }
                     } else {
                         asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];\n"
