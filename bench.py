@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--refine", type=int, default=1, help="FP64 refinement steps (batched workload)")
     ap.add_argument("--shard", default="none", choices=["none", "subtree"],
                     help="subtree: one headline system sharded over the ranks by subtrees (FP64)")
+    ap.add_argument("--hss-form", default="reference", choices=["reference", "nested"],
+                    help="hss workload: identity transfers (the reference's form) or nested bases")
     return ap.parse_args()
 
 
@@ -698,7 +700,7 @@ def run_hss(args):
     N, s, leaf = 65536, 32, 128
     x = np.sort(np.random.default_rng(2).random(N))
     h = H.HSSMatrix(1e-10, rsvd_rank=64, max_rank=64, oversample=10, sketch=H.SKETCH_DEVICE_NORMAL, seed=0,
-                    refine_steps=1)
+                    refine_steps=1, nested=args.hss_form == "nested")
     torch.cuda.set_stream(torch.cuda.Stream())   # a real stream: the library launches on it
     stream = torch.cuda.current_stream()
     h.set_stream(stream.cuda_stream)
@@ -728,6 +730,7 @@ def run_hss(args):
     ms = timed(step)
     ms_f = timed(h.factor)
     y = torch.empty_like(b)
+    ms_mv = timed(lambda: h.multiply_device(xs.data_ptr(), s, N, y.data_ptr(), N))
     h.multiply_device(xs.data_ptr(), s, N, y.data_ptr(), N)
     torch.cuda.synchronize()
     resid = float(torch.linalg.norm(y - b) / torch.linalg.norm(b))
@@ -747,9 +750,11 @@ def run_hss(args):
         "metric": "HSS factor+solve RHS/s (Gaussian 1-D, N=65536, 32 RHS, FP64)", "value": s / (ms / 1e3),
         "cpu_baseline": cpu,
         "unit": "RHS/s", "higher_is_better": True, "n_gpus": 1, "ms_per_step": ms, "ms_factor": ms_f,
+        "ms_multiply": ms_mv,
         "steps": args.steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic", "build_s": t_build,
         "rel_residual": resid, "exact_operator_refinement": exact, "hss_ranks": {"max": int(t["rank12"].max()), "leaf_mean": float(
-            t["rank12"][t["is_leaf"] == 1].mean())},
+            t["rank12"][t["is_leaf"] == 1].mean()), "depth1": [int(v) for v in t["rank12"][t["depth"] == 1]]},
+        "hss_form": args.hss_form,
         "config": {"workload": "hss_gaussian_N65536_leaf128", "N": N, "leaf": leaf, "tol": 1e-10, "max_rank": 64,
                    "nrhs": s, "h": 0.05, "shift": 1e-2, "points": "sorted U[0,1], seed 2", "build": "matrix-free",
                    "refine_steps": 1},

@@ -15,6 +15,7 @@ struct hm_handle {
     cudaStream_t stream = nullptr;
     std::unique_ptr<hm::Engine> eng;
     std::vector<int> fix12, fix21;   // rank profile for the next HODLR builds
+    bool hss_nested = false;          // next HSS builds: nested bases (hm_hss_set_nested)
 };
 
 namespace {
@@ -43,6 +44,7 @@ hm::Engine& engine(hm_handle* h, hm::Engine::Kind kind) {
         h->eng = std::make_unique<hm::Engine>(h->opts, kind);
         h->eng->set_stream(h->stream);
         h->eng->set_rank_profile(h->fix12, h->fix21);
+        h->eng->set_hss_nested(h->hss_nested);
     }
     return *h->eng;
 }
@@ -222,6 +224,17 @@ int hm_hss_build_from_dense(hm_handle* h, const double* A, int N, int lda, int l
         engine(h, hm::Engine::HSS).build_dense_device(d.p, N, N, leaf);
         HM_CUDA(cudaStreamSynchronize(h->stream));
     });
+}
+
+int hm_hss_set_nested(hm_handle* h, int nested) {
+    return guard(h, [&] {
+        h->hss_nested = nested != 0;
+        if (h->eng) h->eng->set_hss_nested(h->hss_nested);
+    });
+}
+
+int hm_hss_is_nested(const hm_handle* h) {
+    return h && h->eng && h->eng->kind() == hm::Engine::HSS && h->eng->hss_nested() ? 1 : 0;
 }
 
 int hm_set_rank_profile(hm_handle* h, int nnodes, const int* rank12, const int* rank21) {

@@ -1076,6 +1076,14 @@ void Engine::build_hss(const Source& src) {
         if (s.which == 0) { n.rankU = r; leafU_[s.leaf] = {s.out, r}; }
         else { n.rankV = r; leafV_[s.leaf] = {s.out, r}; }
     }
+    hss_.nested = false;
+    hss_.offR.clear();
+    hss_.offW.clear();
+    hss_.RW.release();
+    if (hss_nested_) {
+        build_hss_nested(src);
+        return;
+    }
     for (int i = (int)nodes_.size() - 1; i >= 0; --i) {
         Node& n = nodes_[i];
         if (n.is_leaf) continue;
@@ -1729,7 +1737,8 @@ Plan& Engine::matvec_plan(const std::vector<int>& sc) {
     auto it = mv_plans_.find(sc);
     if (it != mv_plans_.end()) return it->second;
     Plan& pl = mv_plans_[sc];
-    add_matvec(pl, nodes_, leaves_, levels_, dD.p, dU.p, dV.p, dB.p, ioX.p, ioY.p, N_, sc, stream_);
+    if (kind_ == HSS && hss_.nested) add_matvec_nested(pl, ioX.p, ioY.p, sc[0]);
+    else add_matvec(pl, nodes_, leaves_, levels_, dD.p, dU.p, dV.p, dB.p, ioX.p, ioY.p, N_, sc, stream_);
     return pl;
 }
 
@@ -2321,8 +2330,16 @@ void Engine::get_factor(int node, int which, double* out, int* rows, int* cols) 
             case 0: if (n.is_leaf) { src = dD.p + n.offD; r = c = ld = n.len(); } break;
             case 1: if (n.is_leaf) { src = dLeafB.p + leafU_[node].first; r = ld = n.len(); c = leafU_[node].second; } break;
             case 2: if (n.is_leaf) { src = dLeafB.p + leafV_[node].first; r = ld = n.len(); c = leafV_[node].second; } break;
-            case 3:  // R = I (hss_routines.h:86-87)
+            case 3:  // R = I (hss_routines.h:86-87); nested builds: the compressed transfer
             case 4: {  // W = I (hss_routines.h:89-90)
+                if (hss_.nested) {
+                    const auto& rk = which == 3 ? hss_.rankU : hss_.rankV;
+                    if (n.is_leaf || n.parent < 0 || rk[node] == 0) break;
+                    src = hss_.RW.p + (which == 3 ? hss_.offR[node] : hss_.offW[node]);
+                    r = ld = rk[n.left] + rk[n.right];
+                    c = rk[node];
+                    break;
+                }
                 const int k = which == 3 ? hss_.rankU[node] : hss_.rankV[node];
                 if (n.is_leaf || k == 0) break;
                 r = c = k;
@@ -2336,10 +2353,11 @@ void Engine::get_factor(int node, int which, double* out, int* rows, int* cols) 
             case 5: {  // B = [[0, B12], [B21, 0]] at (0, lc.rank_V) and (lc.rank_U, 0) (hss_routines.h:105-107)
                 const auto& hu = hss_.rankU;
                 const auto& hv = hss_.rankV;
-                if (n.is_leaf || hu[node] == 0 || hv[node] == 0) break;
+                if (n.is_leaf) break;
                 const int lc = n.left, rc = n.right;
-                r = hu[node];
-                c = hv[node];
+                r = hu[lc] + hu[rc];   // = rank_U of the node in the reference form
+                c = hv[lc] + hv[rc];
+                if (r == 0 || c == 0) { r = c = 0; break; }
                 if (out) {
                     std::fill(out, out + (size_t)r * c, 0.0);
                     std::vector<double> b12((size_t)hu[lc] * hv[rc]), b21((size_t)hu[rc] * hv[lc]);

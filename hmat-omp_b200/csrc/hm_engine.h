@@ -82,6 +82,10 @@ class Engine {
         fix12_ = r12;
         fix21_ = r21;
     }
+    // Next HSS builds: nested bases with compressed transfers R / W (true) or the
+    // reference's identity transfers (false, the default).
+    void set_hss_nested(bool on) { hss_nested_ = on; }
+    bool hss_nested() const { return hss_.nested; }
     void set_precision(int p) {
         if (p != opts_.precision) factored_ = false;
         opts_.precision = p;
@@ -158,6 +162,10 @@ class Engine {
     void begin_build(int N, int leaf);
     void build_hodlr(const Source& src);
     void build_hss(const Source& src);
+    // nested-basis levels above the leaf strips (hm_hss_nested.cu)
+    void build_hss_nested(const Source& src);
+    // telescoping product of a nested-basis operator (hm_hss_nested.cu): X, Y ld N
+    void add_matvec_nested(Plan& pl, const double* X, double* Y, int s);
     void reduce_hss_coupling(const std::vector<std::vector<int>>& under);
     // Append steps materialising blocks (dense copy or generator fill).
     void add_block_fill(Plan& plan, const Source& src,
@@ -196,11 +204,18 @@ class Engine {
     // node (sums over its leaves) and the coupling blocks at those widths.  The operator
     // in nodes_/dU/dV/dB that factor, solve and multiply use is its recompressed
     // two-block form (reduce_hss_coupling).
+    // Nested-basis builds keep here their compressed transfers instead: R of internal node
+    // t is (rankU[left] + rankU[right]) x rankU[t] at RW + offR[t], W likewise, B12/B21
+    // at the nested ranks, and the root's ranks are 0 (it has no off-diagonal strip).
     struct HssForm {
         std::vector<int> rankU, rankV;
         std::vector<size_t> offB12, offB21;
         DBuf<double> B;
+        bool nested = false;
+        std::vector<size_t> offR, offW;
+        DBuf<double> RW;
     } hss_;
+    bool hss_nested_ = false;   // mode of the next HSS build
     bool built_ = false;
     // factorizations
     FactorStore<double> f64_;

@@ -4,13 +4,15 @@
 // a later process factors and solves without recompressing.  Factorizations are not
 // stored: factoring is cheap next to the build and is redone on first use.
 //
-// Layout (native byte order, version 1):
+// Layout (native byte order, version 2; version 1 files, without the nested-basis
+// section, still load):
 //   "HMATB200" | u32 version | u32 kind | i64 N | i64 leaf | i64 nodes
 //   nodes x Node (the planner's struct, offsets into the arrays below included)
 //   array D | array U | array V | array B           (array = i64 count, count doubles)
 //   i32 gen | i32 dim | f64 p0 | f64 p1 | array points
 //   HSS only: array leafB | nodes x (i64 offU, i32 rankU, i64 offV, i32 rankV)
 //             nodes x (i32 rankU, i32 rankV, i64 offB12, i64 offB21) | array B (reference form)
+//             u32 nested | nested only: nodes x (i64 offR, i64 offW) | array RW
 // The tree in the file must be the one the planner makes for (N, leaf); load checks it.
 #include <cstdint>
 #include <cstdio>
@@ -29,7 +31,7 @@ namespace {
 inline bool fits(size_t off, size_t count, size_t n) { return off <= n && count <= n - off; }
 
 constexpr char MAGIC[8] = {'H', 'M', 'A', 'T', 'B', '2', '0', '0'};
-constexpr uint32_t VERSION = 1;
+constexpr uint32_t VERSION = 2;
 static_assert(std::is_trivially_copyable<Node>::value, "Node is written as raw bytes");
 
 struct File {
@@ -96,7 +98,7 @@ int Engine::file_kind(const char* path) {
     F.get(m, 8);
     HM_CHECK(std::memcmp(m, MAGIC, 8) == 0, HM_ERR_ARG, "operator file: not an hmat_b200 operator: " + F.path);
     const uint32_t v = F.get_v<uint32_t>();
-    HM_CHECK(v == VERSION, HM_ERR_ARG, "operator file: unsupported version " + std::to_string(v));
+    HM_CHECK(v == 1 || v == VERSION, HM_ERR_ARG, "operator file: unsupported version " + std::to_string(v));
     const uint32_t k = F.get_v<uint32_t>();
     HM_CHECK(k == HODLR || k == HSS, HM_ERR_ARG, "operator file: bad kind");
     return (int)k;
@@ -137,6 +139,14 @@ void Engine::save(const char* path) const {
             F.put_v<int64_t>((int64_t)hss_.offB21[i]);
         }
         put_array(F, hss_.B.p, hss_.B.n, stream_);
+        F.put_v<uint32_t>(hss_.nested ? 1u : 0u);
+        if (hss_.nested) {
+            for (size_t i = 0; i < nodes_.size(); ++i) {
+                F.put_v<int64_t>((int64_t)hss_.offR[i]);
+                F.put_v<int64_t>((int64_t)hss_.offW[i]);
+            }
+            put_array(F, hss_.RW.p, hss_.RW.n, stream_);
+        }
     }
     F.close_checked();
 }
@@ -146,7 +156,7 @@ void Engine::load(const char* path) {
     File F(path, "rb");
     char m[8];
     F.get(m, 8);
-    F.get_v<uint32_t>();
+    const uint32_t version = F.get_v<uint32_t>();
     F.get_v<uint32_t>();
     const int64_t N = F.get_v<int64_t>(), leaf = F.get_v<int64_t>(), nn = F.get_v<int64_t>();
     HM_CHECK(N > 0 && N < (int64_t(1) << 31) && leaf > 0 && leaf <= N, HM_ERR_ARG, "operator file: bad N/leaf");
@@ -219,6 +229,16 @@ void Engine::load(const char* path) {
             h.offB21[i] = (size_t)F.get_v<int64_t>();
         }
         get_array(F, HB, stream_);
+        h.nested = version >= 2 && F.get_v<uint32_t>() != 0;
+        if (h.nested) {
+            h.offR.resize(nodes.size());
+            h.offW.resize(nodes.size());
+            for (size_t i = 0; i < nodes.size(); ++i) {
+                h.offR[i] = (size_t)F.get_v<int64_t>();
+                h.offW[i] = (size_t)F.get_v<int64_t>();
+            }
+            get_array(F, h.RW, stream_);
+        }
         for (size_t i = 0; i < nodes.size(); ++i) {
             const Node& n = nodes[i];
             if (n.is_leaf) {
@@ -226,10 +246,18 @@ void Engine::load(const char* path) {
                          "operator file: HSS leaf ranks");
                 continue;
             }
-            // a node's rank is the sum of its children's (the reference form's B layout)
+            const int su = h.rankU[n.left] + h.rankU[n.right], sv = h.rankV[n.left] + h.rankV[n.right];
+            // reference form: a node's rank is the sum of its children's; nested form: at
+            // most that sum, 0 at the root, with R / W inside RW
+            const bool ranks_ok =
+                h.nested ? (n.parent < 0 ? h.rankU[i] == 0 && h.rankV[i] == 0
+                                         : h.rankU[i] >= 0 && h.rankV[i] >= 0 && h.rankU[i] <= su &&
+                                               h.rankV[i] <= sv &&
+                                               fits(h.offR[i], (size_t)su * h.rankU[i], h.RW.n) &&
+                                               fits(h.offW[i], (size_t)sv * h.rankV[i], h.RW.n))
+                         : h.rankU[i] == su && h.rankV[i] == sv;
             HM_CHECK(h.rankU[n.left] >= 0 && h.rankV[n.left] >= 0 && h.rankU[n.right] >= 0 &&
-                         h.rankV[n.right] >= 0 && h.rankU[i] == h.rankU[n.left] + h.rankU[n.right] &&
-                         h.rankV[i] == h.rankV[n.left] + h.rankV[n.right] &&
+                         h.rankV[n.right] >= 0 && ranks_ok &&
                          fits(h.offB12[i], (size_t)h.rankU[n.left] * h.rankV[n.right], HB.n) &&
                          fits(h.offB21[i], (size_t)h.rankU[n.right] * h.rankV[n.left], HB.n),
                      HM_ERR_ARG, "operator file: HSS B range");

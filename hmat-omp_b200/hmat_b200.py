@@ -80,6 +80,8 @@ def load() -> C.CDLL:
     L.hm_hodlr_build_from_dense_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
     PP = C.POINTER(C.c_void_p)
     L.hm_set_rank_profile.argtypes = [C.c_void_p, C.c_int, _ip, _ip]
+    L.hm_hss_set_nested.argtypes = [C.c_void_p, C.c_int]
+    L.hm_hss_is_nested.argtypes = [C.c_void_p]
     L.hm_hodlr_import.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip, PP, PP, PP, PP, PP]
     L.hm_num_nodes.argtypes = [C.c_void_p]
     L.hm_export_tree.argtypes = [C.c_void_p] + [_ip] * 6
@@ -486,12 +488,27 @@ class HODLRMatrix(_Handle):
 
 
 class HSSMatrix(_Handle):
-    """Mirror of HSSMatrix (hss_routines.h:10-307) on the device path."""
+    """Mirror of HSSMatrix (hss_routines.h:10-307) on the device path.
+
+    ``nested=True`` selects the nested-basis form (hm_hss_set_nested): compressed
+    transfers R / W instead of the reference's identities, the same leaf bases."""
 
     D, U, V, R, W, B = 0, 1, 2, 3, 4, 5
 
-    def __init__(self, tol: float = 1e-9, **kw):
+    def __init__(self, tol: float = 1e-9, nested: bool = False, **kw):
         super().__init__(tol, **kw)
+        if nested:
+            self.set_nested(True)
+
+    def set_nested(self, on: bool) -> None:
+        """Form of the next builds: nested bases (True) or the reference's identity
+        transfers (False)."""
+        self._check(self._L.hm_hss_set_nested(self._h, 1 if on else 0))
+
+    @property
+    def nested(self) -> bool:
+        """Whether the current operator is a nested-basis HSS."""
+        return bool(self._L.hm_hss_is_nested(self._h))
 
     def build_from_dense(self, A: np.ndarray, leaf_size: int):
         A = np.asfortranarray(A, dtype=np.float64)

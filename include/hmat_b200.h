@@ -137,6 +137,22 @@ HM_API int hm_hss_build_from_dense(hm_handle* h, const double* A, int N, int lda
 HM_API int hm_hss_build_from_kernel(hm_handle* h, int kernel, const double* points, int dim, int N,
                                     const double* params, int nparams, int leaf_size);
 
+/* Nested-basis HSS (no counterpart: the reference's transfers are identities,
+ * hss_routines.h:86-90).  nested != 0 makes the next hm_hss_build_from_dense /
+ * hm_hss_build_from_kernel on this handle keep the leaf bases of the reference form and
+ * compress every internal node's off-diagonal strip onto its children's bases:
+ * U_t = diag(U_left, U_right) R_t, V_t = diag(V_left, V_right) W_t, with R_t / W_t the
+ * leading singular vectors of the projected strips, truncated by the rule every other
+ * block uses (#{s > tol s_0}, at least 1, capped by max_rank).  Ranks then stay at the
+ * numerical rank of each strip instead of growing with the number of leaves below.
+ * hm_export_tree returns the nested ranks (0 at the root); hm_get_factor returns the
+ * leaf U / V, R (rank_U(left) + rank_U(right)) x rank_U, W likewise, and B at the nested
+ * ranks.  Multiply, factor and solve run on the same operator; hm_save / hm_load keep
+ * the form.  nested = 0 restores the reference form.  hm_hss_is_nested: 1 when the
+ * handle's current operator is a nested-basis HSS, else 0. */
+HM_API int hm_hss_set_nested(hm_handle* h, int nested);
+HM_API int hm_hss_is_nested(const hm_handle* h);
+
 /* ---- serialized operators (no counterpart in the reference, which has no format) ----
  * hm_save writes the built operator (tree, leaf blocks, bases, coupling blocks; for HSS
  * also the reference-form leaf bases and B that hm_get_factor exports; for kernel builds

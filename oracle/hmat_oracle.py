@@ -19,6 +19,9 @@ Contents (each function cites the reference lines it restates):
                       adjoint that the GPU path implements.
   * ``HssOracle``   — hss_routines.h: build_topo, leaf compression, identity
                       transfers, up/down-sweep multiply, stable Woodbury solve.
+  * ``HssNestedOracle`` — the nested-basis HSS extension (compressed transfers; no
+                      reference counterpart): the specification its device build and
+                      telescoping multiply are checked against.
   * kernel generators for the benchmark configurations.
 """
 from __future__ import annotations
@@ -640,6 +643,108 @@ class HssOracle:
 
     def factor(self) -> HodlrFactors:
         return level_factor(self.nodes, *self.generic())
+
+
+class HssNestedOracle(HssOracle):
+    """Nested-basis HSS: an extension with no reference counterpart (the reference's
+    transfers are identities, hss_routines.h:86-90), stated here as the specification the
+    device build is checked against.
+
+    Leaves: the reference form's strip bases (``HssOracle.build_from_dense``).  Internal
+    node t (children a, b), bottom-up: R_t = the leading left singular vectors of the
+    projected strip [U_a^T A[I_a, I_t^c]; U_b^T A[I_b, I_t^c]] kept by
+    ``truncation_rank`` (W_t from the column strip likewise), U_t = diag(U_a, U_b) R_t
+    (expanded, ``EU``), and B12 = U_a^T A[I_a, I_b] V_b, B21 = U_b^T A[I_b, I_a] V_a at the
+    nested ranks.  The root has no strip: rank 0, no transfer."""
+
+    def build_from_dense(self, A: np.ndarray, leaf: int, sketch) -> None:
+        self.N = N = A.shape[0]
+        self.nodes = hss_tree(N, leaf)
+
+        def comp(blk):
+            return compress_rsvd(blk, self.tol, self.rsvd_rank, sketch, self.oversample,
+                                 self.min_dim, 0, self.max_rank)
+
+        for n in reversed(self.nodes):   # children have larger ids than their parent
+            s, e = n.start, n.end
+            if n.is_leaf:
+                n.D = A[s:e, s:e].copy()
+                row = A[s:e, :].copy()
+                row[:, s:e] = 0.0
+                n.U = n.EU = comp(row).U
+                col = A[:, s:e].T.copy()
+                col[:, s:e] = 0.0
+                n.V = n.EV = comp(col).U
+                n.rank_U, n.rank_V = n.U.shape[1], n.V.shape[1]
+                continue
+            lc, rc = n.left, n.right
+            m = lc.end
+            n.B12 = lc.EU.T @ A[s:m, m:e] @ rc.EV
+            n.B21 = rc.EU.T @ A[m:e, s:m] @ lc.EV
+            if n.parent is None:
+                n.rank_U = n.rank_V = 0
+                n.R = n.W = None
+                continue
+            out = np.r_[0:s, e:N]
+            SU = np.vstack([lc.EU.T @ A[s:m][:, out], rc.EU.T @ A[m:e][:, out]])
+            SV = np.vstack([lc.EV.T @ A[out][:, s:m].T, rc.EV.T @ A[out][:, m:e].T])
+            Ru, su, _ = sla.svd(SU, full_matrices=False, lapack_driver="gesvd")
+            Rv, sv, _ = sla.svd(SV, full_matrices=False, lapack_driver="gesvd")
+            n.R = Ru[:, :truncation_rank(su, self.tol, self.max_rank)].copy()
+            n.W = Rv[:, :truncation_rank(sv, self.tol, self.max_rank)].copy()
+            n.rank_U, n.rank_V = n.R.shape[1], n.W.shape[1]
+            n.EU = sla.block_diag(lc.EU, rc.EU) @ n.R
+            n.EV = sla.block_diag(lc.EV, rc.EV) @ n.W
+
+    def multiply(self, x: np.ndarray) -> np.ndarray:
+        """Telescoping product: up-sweep g_leaf = V^T x, g_t = W_t^T [g_a; g_b];
+        down-sweep [f_a; f_b] = R_t f_t + [B12 g_b; B21 g_a]; y = D x + U f."""
+        x = np.asarray(x, dtype=np.float64)
+        vec = x.ndim == 1
+        X = x.reshape(self.N, -1)
+        s_ = X.shape[1]
+        g = {}
+        for n in reversed(self.nodes):
+            if n.is_leaf:
+                g[n.id] = n.V.T @ X[n.start:n.end]
+            elif n.parent is not None:
+                g[n.id] = n.W.T @ np.vstack([g[n.left.id], g[n.right.id]])
+        f = {}
+        for n in self.nodes:
+            if n.is_leaf:
+                continue
+            lc, rc = n.left, n.right
+            fa = n.B12 @ g[rc.id]
+            fb = n.B21 @ g[lc.id]
+            if n.parent is not None:
+                t = n.R @ f[n.id]
+                fa = fa + t[:lc.rank_U]
+                fb = fb + t[lc.rank_U:]
+            f[lc.id], f[rc.id] = fa, fb
+        Y = np.zeros_like(X)
+        for n in self.nodes:
+            if n.is_leaf:
+                Y[n.start:n.end] = n.D @ X[n.start:n.end] + (n.U @ f[n.id] if n.id in f else 0.0)
+        return Y.ravel() if vec else Y
+
+    def generic(self):
+        """The operator in the two-block form of ``level_factor`` (expanded bases)."""
+        leaves = {n.id: n.D for n in self.nodes if n.is_leaf}
+        gen = {n.id: (n.left.EU, n.left.EV, n.right.EU, n.right.EV, n.B12, n.B21)
+               for n in self.nodes if not n.is_leaf}
+        return leaves, gen
+
+    def dense(self) -> np.ndarray:
+        """The compressed operator as a dense matrix."""
+        Y = np.zeros((self.N, self.N))
+        for n in self.nodes:
+            if n.is_leaf:
+                Y[n.start:n.end, n.start:n.end] = n.D
+            else:
+                lc, rc = n.left, n.right
+                Y[lc.start:lc.end, rc.start:rc.end] = lc.EU @ n.B12 @ rc.EV.T
+                Y[rc.start:rc.end, lc.start:lc.end] = rc.EU @ n.B21 @ lc.EV.T
+        return Y
 
 
 # ----------------------------------------------------------------------------------
