@@ -431,6 +431,7 @@ def run_ours(args):
         "profile": {k: {"launches": v[0], "ms": v[1], "flops": v[2], "bytes": v[3]} for k, v in prof.items()},
     }
     out["roofline"] = roofline(prof)
+    out["sweeps_hbm"] = sweep_rates(prof)
     h.close()
     if rank == 0:
         out["like_for_like"] = like_for_like(args, stream)
@@ -687,6 +688,24 @@ def roofline(prof: dict):
                      "frac": fl / sec / 1e12 / ceiling, "peak_note": note,
                      "hbm_frac": by / sec / 1e9 / hbm})
     return base
+
+
+def sweep_rates(prof: dict):
+    """Achieved rates of the solve and matvec sweeps of the profiled mixed step: algorithmic
+    bytes (operands read once, outputs written once) over the summed CUDA-event time of
+    each labelled step, as a fraction of the measured HBM copy bandwidth."""
+    try:
+        hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
+    except Exception:
+        hbm = 6650.0
+    out = {}
+    for name, (n, ms, fl, by) in sorted(prof.items()):
+        label = name.split(":", 1)[-1]
+        if not (label.startswith("solve.") or label.startswith("matvec.")) or ms <= 0:
+            continue
+        gbs = by / (ms / 1e3) / 1e9
+        out[name] = {"launches": n, "ms": ms, "gbs": gbs, "hbm_frac": gbs / hbm, "tflops": fl / (ms / 1e3) / 1e12}
+    return out
 
 
 def run_hss(args):

@@ -159,16 +159,32 @@ class Plan {
         steps_.clear();
         chunks_.clear();
         used_ = cap_ = 0;
+        ext_ = nullptr;
+        ext_cap_ = ext_used_ = 0;
     }
     size_t scratch_bytes() const {
         size_t b = 0;
         for (auto& c : chunks_) b += c.n;
         return b;
     }
+    // Serve scratch from caller-owned device memory first (the plan neither frees it nor
+    // may outlive it); requests that no longer fit fall back to owned chunks.  Loops that
+    // build one plan per chunk of work reuse one workspace this way instead of allocating
+    // and freeing (a device synchronisation) their scratch chunk by chunk.
+    void use_arena(void* base, size_t bytes) {
+        ext_ = static_cast<unsigned char*>(base);
+        ext_cap_ = bytes;
+        ext_used_ = 0;
+    }
 
   private:
     void* bump(size_t bytes) {
         bytes = align_up(std::max<size_t>(bytes, 1), 256);
+        if (ext_ && ext_used_ + bytes <= ext_cap_) {
+            void* p = ext_ + ext_used_;
+            ext_used_ += bytes;
+            return p;
+        }
         if (chunks_.empty() || used_ + bytes > cap_) {
             size_t c = std::max<size_t>(bytes, size_t(64) << 20);
             chunks_.emplace_back(c);
@@ -183,6 +199,8 @@ class Plan {
     std::vector<std::unique_ptr<Step>> steps_;
     std::vector<DBuf<unsigned char>> chunks_;
     size_t used_ = 0, cap_ = 0;
+    unsigned char* ext_ = nullptr;
+    size_t ext_cap_ = 0, ext_used_ = 0;
     mutable std::shared_ptr<CUgraphExec_st> graph_;
     mutable int* graph_status_ = nullptr;
     mutable int runs_ = 0;

@@ -968,19 +968,29 @@ void Engine::build_hss(const Source& src) {
     }
     dLeafB.alloc(std::max<size_t>(out_total, 1));
     DBuf<int> dRank(std::max<size_t>(strips.size(), 1));
-    // chunks of strips bounded by a workspace budget
+    // chunks of strips bounded by a workspace budget; one workspace serves every chunk
     const size_t budget = size_t(16) << 30;
-    size_t i0 = 0;
-    while (i0 < strips.size()) {
+    std::vector<std::pair<size_t, size_t>> chunks;
+    size_t ws_bytes = 0;
+    for (size_t i0 = 0; i0 < strips.size();) {
         size_t i1 = i0, bytes = 0;
         while (i1 < strips.size()) {
             const Strip& s = strips[i1];
-            const size_t b = 8 * ((size_t)s.m * N + 5 * (size_t)N * s.k + 6 * (size_t)s.m * s.k + 8 * (size_t)s.k * s.k);
+            const size_t b = 8 * ((size_t)s.m * N + 5 * (size_t)N * s.k + 6 * (size_t)s.m * s.k + 8 * (size_t)s.k * s.k) +
+                             (size_t(1) << 20);   // alignment and small tables
             if (i1 > i0 && bytes + b > budget) break;
             bytes += b;
             ++i1;
         }
+        chunks.emplace_back(i0, i1);
+        ws_bytes = std::max(ws_bytes, bytes);
+        i0 = i1;
+    }
+    DBuf<unsigned char> ws(std::max<size_t>(ws_bytes, 1));
+    for (const auto& ch : chunks) {
+        const size_t i0 = ch.first, i1 = ch.second;
         Plan plan;
+        plan.use_arena(ws.p, ws.n);
         std::vector<std::tuple<int, int, int, int, int, double*, int>> fill;
         auto zero = std::make_unique<IdentStep>();
         std::vector<SvdProblem> full;
@@ -1061,8 +1071,8 @@ void Engine::build_hss(const Source& src) {
         plan.run(stream_, dstatus.p);
         HM_CUDA(cudaStreamSynchronize(stream_));
         check_status("hss build: leaf strips");
-        i0 = i1;
     }
+    ws.release();
     // ranks: leaves from their strips, internal nodes the sums (hss_routines.h:82-83)
     std::vector<int> rk(strips.size());
     if (!strips.empty())

@@ -60,12 +60,22 @@ void Engine::build_hss_nested(const Source& src) {
     }
     auto one = [](size_t n) { return std::max<size_t>(n, 1); };
     Plan keep;                          // arena: R/W, expanded bases and B of every node
-    std::unique_ptr<Plan> below;        // arena: pair buffers of the level below
+    std::unique_ptr<Plan> below;        // pair buffers of the level below (in below_ws)
+    DBuf<unsigned char> below_ws;
+    auto al = [](size_t bytes) { return (std::max<size_t>(bytes, 1) + 255) / 256 * 256; };
     const size_t budget = size_t(8) << 30;   // SVD scratch per chunk
+    DBuf<unsigned char> ws;                   // one workspace for the chunks' scratch
     for (int d = (int)levels_.size() - 1; d >= 0; --d) {
         const std::vector<int>& lvl = levels_[d];
         if (lvl.empty()) continue;
+        size_t pair_bytes = 0;   // this level's pair buffers, in one allocation
+        for (int t : lvl) {
+            const Node& n = nodes_[t];
+            pair_bytes += al(8 * (size_t)N * (kU[n.left] + kU[n.right])) + al(8 * (size_t)N * (kV[n.left] + kV[n.right]));
+        }
+        DBuf<unsigned char> pair_ws(pair_bytes);
         auto pairs = std::make_unique<Plan>();
+        pairs->use_arena(pair_ws.p, pair_ws.n);
         for (int t : lvl) {
             const Node& n = nodes_[t];
             NestedNode& x = nb[t];
@@ -92,12 +102,15 @@ void Engine::build_hss_nested(const Source& src) {
             size_t i1 = i0, bytes = 0;
             while (i1 < lvl.size()) {
                 const NestedNode& x = nb[lvl[i1]];
-                const size_t b = 8 * (3 * (size_t)N * (x.kpU + x.kpV) + 8 * ((size_t)x.kpU * x.kpU + (size_t)x.kpV * x.kpV));
+                const size_t b = 8 * (3 * (size_t)N * (x.kpU + x.kpV) + 8 * ((size_t)x.kpU * x.kpU + (size_t)x.kpV * x.kpV)) +
+                                 (size_t(64) << 10);   // alignment and small tables
                 if (i1 > i0 && bytes + b > budget) break;
                 bytes += b;
                 ++i1;
             }
+            if (ws.n < bytes) ws.alloc(bytes);
             Plan plan;
+            plan.use_arena(ws.p, ws.n);
             auto pre = std::make_unique<IdentStep>();      // expanded blocks under a rank-0 child
             auto gP = std::make_unique<GemmStep<double>>(CFG_64x64, src.gen);   // leaf panels
             gP->gp = src.gp;
@@ -210,8 +223,10 @@ void Engine::build_hss_nested(const Source& src) {
             }
         }
         below = std::move(pairs);   // this level's pairs feed the next level's panels
+        below_ws = std::move(pair_ws);
     }
     below.reset();
+    below_ws.release();
 
     // The engine's two-level storage: expanded bases of every non-root node, B per node.
     for (int i = 0; i < nn; ++i) {
