@@ -21,6 +21,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "hmat_b200.h")
 HM_OK, HM_ERR_ARG, HM_ERR_CUDA, HM_ERR_SINGULAR, HM_ERR_NO_CONVERGE = 0, 1, 2, 3, 4
 HM_ERR_NONFINITE, HM_ERR_STATE, HM_ERR_UNSUPPORTED, HM_ERR_IR, HM_ERR_TIMEOUT = 5, 6, 7, 8, 9
 GEMM_AUTO, GEMM_TENSOR_CORES, GEMM_FMA, GEMM_TEST_STALL = 0, 1, 2, 16
+OP_N, OP_T = 0, 1   # opA / opB of Dense.gemm: as stored, or transposed
 SKETCH_REFERENCE_UNIFORM, SKETCH_REFERENCE_NORMAL, SKETCH_DEVICE_NORMAL = 0, 1, 2
 FP64, MIXED = 0, 1
 KERNEL_CAUCHY, KERNEL_GAUSSIAN, KERNEL_COULOMB = 1, 2, 3
