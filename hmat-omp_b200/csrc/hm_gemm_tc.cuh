@@ -84,6 +84,11 @@ __device__ __forceinline__ void tma2d(uint32_t dst, const void* tmap, int x, int
         "l"(tmap), "r"(x), "r"(y), "r"(b)
         : "memory");
 }
+// TMA: prefetch a tile of global memory into L2 (no shared memory, no completion)
+__device__ __forceinline__ void tma2d_prefetch(const void* tmap, int x, int y) {
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];\n" ::"l"(tmap), "r"(x), "r"(y)
+                 : "memory");
+}
 // TMA: shared tile -> global (store), or added into global (reduce-add), as a bulk group
 __device__ __forceinline__ void tma2d_store(const void* tmap, int x, int y, uint32_t src) {
     asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(tmap),
@@ -358,8 +363,37 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
                 const bool a_mn = GEN == GEN_DENSE && D.opA == OP_N, b_mn = D.opB == OP_T;
                 const CUtensorMap* ma = tmaps + 3 * ti.p;
                 const CUtensorMap* mb = ma + 1;
+                // the next tile's first k-blocks (short-k tiles: all of it) into L2 while
+                // this one's last ST k-blocks stream, so its stage loads do not wait on DRAM
+                // latency (earlier, on long tiles, the lines would be evicted before use)
+                auto prefetch_next = [&]() {
+                    if (tile + (int)gridDim.x >= ntiles) return;
+                    const TileInfo tn = decode<BN>(descs, tile_problem, tile + gridDim.x);
+                    const GemmDesc<float>& Dn = descs[tn.p];
+                    const bool na_mn = Dn.opA == OP_N, nb_mn = Dn.opB == OP_T;
+                    const CUtensorMap* pa = tmaps + 3 * tn.p;
+                    for (int kt = 0; kt < min(tn.nk, ST); ++kt) {
+                        const int k0 = tn.kb + kt * BK;
+                        if constexpr (GEN == GEN_DENSE) {
+                            if (na_mn) {
+#pragma unroll
+                                for (int c = 0; c < BM / 32; ++c) tma2d_prefetch(pa, tn.m0 + 32 * c, k0);
+                            } else {
+                                tma2d_prefetch(pa, k0, tn.m0);
+                            }
+                        }
+                        if (nb_mn) {
+#pragma unroll
+                            for (int c = 0; c < BN / 32; ++c) tma2d_prefetch(pa + 1, tn.n0 + 32 * c, k0);
+                        } else {
+                            tma2d_prefetch(pa + 1, k0, tn.n0);
+                        }
+                    }
+                };
+                if (ti.nk == 0) prefetch_next();
                 for (int kt = 0; kt < ti.nk; ++kt, ++slot) {
                     const int st = slot % ST;
+                    if (kt == max(0, ti.nk - ST)) prefetch_next();
                     if (!wait_bar(empty(st), ((slot / ST) & 1) ^ 1, abort_flag, status, lim)) { ok = false; break; }
                     const uint32_t base = stage0 + (uint32_t)st * S::STAGE;
                     const uint32_t bbase = base + 2 * S::A_BYTES;
@@ -566,6 +600,14 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
                     c_pending = true;
                 }
                 mbar_arrive(cfree);
+                // after a short-k tile, the next tile's C into L2: its load then waits on
+                // L2, not DRAM (long tiles leave the load time to land anyway)
+                if (ti.nk <= ST && tile + (int)gridDim.x < ntiles) {
+                    const TileInfo tn = decode<BN>(descs, tile_problem, tile + gridDim.x);
+                    const GemmDesc<float>& Dn = descs[tn.p];
+                    if (Dn.ksplit <= 1 && Dn.beta != 0.f && c_tma_ok(Dn.C, Dn.ldc))
+                        tma2d_prefetch(tmaps + 3 * tn.p + 2, tn.m0, tn.n0);
+                }
             }
             const int acc = accn & 1;
             if (!wait_bar_warp(tfull(acc), (accn >> 1) & 1, abort_flag, status, lim)) break;
