@@ -309,7 +309,7 @@ __device__ __forceinline__ void jac_pair(int r, int i, int kk, int& p, int& q) {
 }
 
 __global__ void __launch_bounds__(256) jacobi_kernel(const EigDesc* __restrict__ descs, int* status,
-                                                     int max_sweeps, int use_smem) {
+                                                     int max_sweeps, int use_smem, int w_smem) {
     extern __shared__ double sm[];
     const EigDesc d = descs[blockIdx.x];
     const int k = d.k;
@@ -322,8 +322,11 @@ __global__ void __launch_bounds__(256) jacobi_kernel(const EigDesc* __restrict__
     const int kk = (k + 1) & ~1;              // even number of players (k = dummy if odd)
     const int half = kk / 2;
     double* sn = cs + half;
-    double* W = d.W;
-    const int ldw = d.ldw;
+    // the eigenvector matrix accumulates in shared memory when it fits (every rotation
+    // round reads and writes two of its columns), and is written out once at the end
+    const bool w_in_smem = in_smem && w_smem != 0;
+    double* W = w_in_smem ? sn + half : d.W;
+    const int ldw = w_in_smem ? k : d.ldw;
     __shared__ int s_rot;
     if (in_smem)
         for (int e = tid; e < k * k; e += nt) {
@@ -391,7 +394,8 @@ __global__ void __launch_bounds__(256) jacobi_kernel(const EigDesc* __restrict__
                 W[i + (size_t)q * ldw] = s * wp + c * wq;
             }
             __syncthreads();
-            // G <- J^T G (rows p, q)
+            // G <- J^T G (rows p, q); the annihilated pair (p, q), (q, p) set to exact zeros
+            // (only this pair's own updates touch those two entries)
             for (int e = tid; e < half * k; e += nt) {
                 const int t = e / k, j = e % k;
                 const double s = sn[t];
@@ -400,17 +404,8 @@ __global__ void __launch_bounds__(256) jacobi_kernel(const EigDesc* __restrict__
                 jac_pair(r, t, kk, p, q);
                 const double c = cs[t];
                 const double gp = g[p + j * ld], gq = g[q + j * ld];
-                g[p + j * ld] = c * gp - s * gq;
-                g[q + j * ld] = s * gp + c * gq;
-            }
-            __syncthreads();
-            // exact zeros for the annihilated pairs, symmetric
-            for (int t = tid; t < half; t += nt) {
-                if (sn[t] == 0.0) continue;
-                int p, q;
-                jac_pair(r, t, kk, p, q);
-                g[p + q * ld] = 0.0;
-                g[q + p * ld] = 0.0;
+                g[p + j * ld] = j == q ? 0.0 : c * gp - s * gq;
+                g[q + j * ld] = j == p ? 0.0 : s * gp + c * gq;
             }
             __syncthreads();
         }
@@ -419,16 +414,26 @@ __global__ void __launch_bounds__(256) jacobi_kernel(const EigDesc* __restrict__
     }
     if (!converged && tid == 0) atomicOr(status, ST_NO_CONVERGE);
     for (int i = tid; i < k; i += nt) d.lam[i] = g[i + i * ld];
+    if (w_in_smem) {
+        __syncthreads();
+        for (int e = tid; e < k * k; e += nt) {
+            const int i = e % k, j = e / k;
+            d.W[i + (size_t)j * d.ldw] = W[e];
+        }
+    }
 }
 
 void launch_jacobi(const DevTable<EigDesc>& t, int* status, cudaStream_t s, int max_sweeps) {
     if (t.h.empty()) return;
     int kmax = 0;
     for (auto& d : t.h) kmax = std::max(kmax, d.k);
-    size_t smem = (kmax <= JAC_SMEM_MAX ? (size_t)kmax * kmax * 8 : 0) + ((size_t)kmax + 2) * 8;
+    const bool g_smem = kmax <= JAC_SMEM_MAX;
+    const bool w_smem = g_smem && kmax <= JAC_W_SMEM_MAX;
+    size_t smem = (g_smem ? (size_t)kmax * kmax * 8 : 0) + ((size_t)kmax + 2) * 8 +
+                  (w_smem ? (size_t)kmax * kmax * 8 : 0);
     static size_t cur = 0;
     ensure_dyn_smem(jacobi_kernel, smem, cur);
-    jacobi_kernel<<<t.size(), 256, smem, s>>>(t.d.p, status, max_sweeps, kmax <= JAC_SMEM_MAX);
+    jacobi_kernel<<<t.size(), 256, smem, s>>>(t.d.p, status, max_sweeps, g_smem, w_smem);
     HM_CUDA(cudaGetLastError());
 }
 

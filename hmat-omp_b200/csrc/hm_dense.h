@@ -17,8 +17,10 @@ namespace hm {
 constexpr int GJ_MAX = 128;
 // Widest sketch (rsvd_rank + oversample) and full-SVD block the Jacobi kernels take.
 constexpr int SKETCH_MAX = 160;
-// Largest Gram matrix held in shared memory by the Jacobi eigen-solver.
+// Largest Gram matrix held in shared memory by the Jacobi eigen-solver, and the largest
+// whose eigenvector matrix is accumulated there too (both: 2 k^2 doubles <= ~190 KB).
 constexpr int JAC_SMEM_MAX = 128;
+constexpr int JAC_W_SMEM_MAX = 108;
 
 struct GJDesc {
     const double* A;
