@@ -784,6 +784,9 @@ void GemmBatch<T>::finalize_tc(cudaStream_t s, bool force) {
         HM_CUDA(cudaMemcpyAsync(tcmaps_.p, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s));
         HM_CUDA(cudaStreamSynchronize(s));   // the host vectors are locals
         tc_tiles_ = tt;
+        // at most 4 k-blocks per tile on average: the epilogue bounds the tile rate, so
+        // it gets twice the warps
+        tc_epw_ = kblocks <= 4LL * tt ? 8 : 4;
         use_tc_ = true;
     }
 }
@@ -920,10 +923,18 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) cons
                 HM_CUDA(cudaGetLastError());
                 return;
             }
-            if (pipe_bn_ == 32) tc::launch<32>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);
-            else if (pipe_bn_ == 64) tc::launch<64>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);
-            else if (pipe_bn_ == 96) tc::launch<96>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);
-            else tc::launch<128>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, tc_stall_ ? 1 : 0);
+            const int stall = tc_stall_ ? 1 : 0;
+            if (tc_epw_ == 8) {
+                if (pipe_bn_ == 32) tc::launch<32, GEN_DENSE, 8>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall);
+                else if (pipe_bn_ == 64) tc::launch<64, GEN_DENSE, 8>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall);
+                else if (pipe_bn_ == 96) tc::launch<96, GEN_DENSE, 8>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall);
+                else tc::launch<128, GEN_DENSE, 8>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall);
+            } else {
+                if (pipe_bn_ == 32) tc::launch<32>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall);
+                else if (pipe_bn_ == 64) tc::launch<64>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall);
+                else if (pipe_bn_ == 96) tc::launch<96>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall);
+                else tc::launch<128>(tc_tiles_, sms, s, tcd_.p, tct_.p, maps, st, stall);
+            }
             HM_CUDA(cudaGetLastError());
             return;
         }

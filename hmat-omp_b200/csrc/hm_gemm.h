@@ -189,6 +189,7 @@ class GemmBatch {
     bool gen_tc_ = false;   // generated-A batch on the tensor cores
     int gen_bn_ = 0;        // its tile width
     int tc_tiles_ = 0;
+    int tc_epw_ = 4;   // epilogue warps of the tensor-core kernel (8 for short-k batches)
     DBuf<GemmDesc<T>> tcd_;
     DBuf<int> tct_;
     DBuf<unsigned char> tcmaps_;

@@ -27,11 +27,13 @@
 //              MMAs: per k-block 4 k-steps x 4 products of 128 x BN x 8, then a commit
 //              that frees the stage; after a tile's last k-block, a commit that hands the
 //              accumulator to the epilogue.
-//   warps 10-13 epilogue: tcgen05.ld of the accumulator rows this warp may access (lane
-//              quarter warp % 4) into the shared C tile (loaded first by TMA when beta != 0:
-//              C = alpha acc + beta C), released accumulator, then one TMA store of the
-//              tile (a TMA reduce-add for split-K), so a tile's epilogue overlaps the
-//              next tile's MMAs.
+//   warps 10.. epilogue: 4 warps, or for short-k batches 8 (two per TMEM lane quarter,
+//              each taking half of the tile's columns): tcgen05.ld of the main and correction accumulators
+//              (one wait per 16 columns) into the shared C tile (loaded first by TMA when
+//              beta != 0: C = alpha acc + beta C), released accumulator, then one TMA store
+//              of the tile (a TMA reduce-add for split-K), so a tile's epilogue overlaps
+//              the next tile's MMAs.  (With four warps the epilogue bounded short-k tiles:
+//              the MMA thread waited for a free accumulator 60% of the time.)
 // Every wait on an mbarrier gives up after about a second of clock, sets ST_TIMEOUT in
 // the status word and makes all roles leave; the tensor memory is always released.
 // Teardown waits (copies and MMAs already issued) keep the one-second bound even when a
@@ -44,8 +46,10 @@ namespace tc {
 constexpr int BM = 128, BK = 32;
 constexpr int NCONV = 256;               // converter threads (warps 1-8)
 constexpr int MMA_WARP = 9;
-constexpr int EPI_WARP0 = 10;            // warps 10-13
-constexpr int NT = 14 * 32;
+constexpr int EPI_WARP0 = 10;            // warps 10.. (4 or 8 epilogue warps)
+// threads of a CTA with EPW epilogue warps
+template <int EPW>
+constexpr int nthreads() { return (EPI_WARP0 + EPW) * 32; }
 
 template <int BN>
 struct Shape {
@@ -150,17 +154,27 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
                  : "memory");
 }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
+// Two 16-column loads (the main and the correction accumulator) and one wait.
+__device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float* v, float* w) {
+    uint32_t r[16], q[16];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr)
+        : "r"(ta)
+        : "memory");
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]),
+          "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
+        : "r"(tb)
         : "memory");
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 16; ++i) {
+        v[i] = __uint_as_float(r[i]);
+        w[i] = __uint_as_float(q[i]);
+    }
 }
 __device__ __forceinline__ float lds_f32(uint32_t a) {
     float x;
@@ -294,8 +308,8 @@ __device__ __forceinline__ TileInfo decode(const GemmDesc<float>* __restrict__ d
 // GEN != GEN_DENSE: A is not read from memory but evaluated by the converter warps from
 // the kernel generator (entry (ga_r0 + i, ga_c0 + k) of op(A), or its transpose for
 // opA = OP_T) straight into the K-major stage layout; the TMA brings only B.
-template <int BN, int GEN>
-__global__ void __launch_bounds__(NT, 1)
+template <int BN, int GEN, int EPW>
+__global__ void __launch_bounds__(nthreads<EPW>(), 1)
 gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restrict__ tile_problem, int ntiles,
                  const CUtensorMap* __restrict__ tmaps, int* status, int stall, const GenParams gp) {
     using S = Shape<BN>;
@@ -336,11 +350,11 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(tfull(a), 1);
-            mbar_init(tempty(a), 128);
+            mbar_init(tempty(a), EPW * 32);
         }
         mbar_init(done, 1);
         mbar_init(cfull, 1);
-        mbar_init(cdone, 128);
+        mbar_init(cdone, EPW * 32);
         mbar_init(cfree, 1);
         s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -570,7 +584,8 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
         // beta != 0, the results are written into it, and one TMA store (or, for
         // split-K, one TMA reduce-add) writes it back; the leader thread issues the
         // copies and orders the buffer's reuse.
-        const int q = warp & 3;
+        const int q = warp & 3;                          // TMEM lane quarter of this warp
+        const int half = (warp - EPI_WARP0) >> 2;        // which half of the tile's columns
         const int row = 32 * q + lane;
         const bool leader = warp == EPI_WARP0 && lane == 0;
         int accn = 0, rdn = 0;    // tiles seen; tiles whose C tile was loaded
@@ -623,13 +638,13 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
             // C reads all issued together, then the results (the 16-column body is unrolled;
             // the outer loop is not, to keep the kernel's code small: instruction fetch
             // stalls led this kernel's profile)
+            constexpr int RH = BN / 16 / (EPW / 4);   // 16-column rounds per warp
 #pragma unroll 1
-            for (int c = 0; c < BN / 16; ++c) {
+            for (int c = half * RH; c < (half + 1) * RH; ++c) {
                 if (16 * c >= nt) break;
                 float v[16], w[16], cc[16];
                 if (ti.nk > 0) {
-                    tmem_ld16(tbase + (uint32_t)(16 * c), v);
-                    tmem_ld16(tbase + (uint32_t)(S::HALF_COLS + 16 * c), w);
+                    tmem_ld16x2(tbase + (uint32_t)(16 * c), tbase + (uint32_t)(S::HALF_COLS + 16 * c), v, w);
                 } else {
 #pragma unroll
                     for (int j = 0; j < 16; ++j) v[j] = w[j] = 0.f;
@@ -684,14 +699,18 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
     }
 }
 
-template <int BN, int GEN = GEN_DENSE>
+// EPW: epilogue warps, 8 for short-k batches (the epilogue bounds them), 4 otherwise
+// (more polling warps would take issue slots from the converters of long-k tiles)
+template <int BN, int GEN = GEN_DENSE, int EPW = 4>
 void launch(int tiles, int sms, cudaStream_t s, const GemmDesc<float>* d, const int* tile_problem,
             const CUtensorMap* tmaps, int* status, int stall, const GenParams& gp = GenParams()) {
+    static_assert(EPW == 4 || EPW == 8, "epilogue warps");
     using S = Shape<BN>;
     static size_t cur = 0;
-    ensure_dyn_smem(gemm_tc32_kernel<BN, GEN>, S::SMEM, cur);
+    ensure_dyn_smem(gemm_tc32_kernel<BN, GEN, EPW>, S::SMEM, cur);
     const int grid = std::max(1, std::min(tiles, sms));
-    gemm_tc32_kernel<BN, GEN><<<grid, NT, S::SMEM, s>>>(d, tile_problem, tiles, tmaps, status, stall, gp);
+    gemm_tc32_kernel<BN, GEN, EPW><<<grid, nthreads<EPW>(), S::SMEM, s>>>(d, tile_problem, tiles, tmaps, status,
+                                                                          stall, gp);
 }
 
 // Whether the tensor-core kernel can take a problem: the TMA wants 16-byte aligned bases
