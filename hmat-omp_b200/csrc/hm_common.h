@@ -34,6 +34,10 @@ struct Error : std::runtime_error {
         if (!(cond)) throw ::hm::Error((code), std::string(msg));     \
     } while (0)
 
+// max that propagates NaN (std::max(a, NaN) returns a): a residual norm that is NaN in
+// one column must make the whole check fail, not vanish from it.
+inline double max_nan(double a, double b) { return (a != a || b != b) ? (a != a ? a : b) : (a < b ? b : a); }
+
 // Device-side status word bits (written by kernels, read by the host after a phase).
 enum : int {
     ST_SINGULAR = 1,        // zero / non-finite pivot in an inversion

@@ -1921,7 +1921,7 @@ void Engine::solve_mixed(const double* db, int s, int ldb, double* dx, int ldx, 
         for (int j = 0; j < s; ++j) {
             double den = std::sqrt(hn[s + j]);
             double rel = den > 0 ? std::sqrt(hn[j]) / den : std::sqrt(hn[j]);
-            worst = std::max(worst, rel);
+            worst = max_nan(worst, rel);
         }
         if (!(worst == worst)) break;  // NaN
         if (worst <= opts_.ir_tol) { ++it; break; }
@@ -1994,7 +1994,7 @@ void Engine::solve_exact_device(const double* db, int s, int ldb, double* dx, in
         worst = 0.0;
         for (int j = 0; j < s; ++j) {
             const double den = std::sqrt(hn[s + j]);
-            worst = std::max(worst, den > 0 ? std::sqrt(hn[j]) / den : std::sqrt(hn[j]));
+            worst = max_nan(worst, den > 0 ? std::sqrt(hn[j]) / den : std::sqrt(hn[j]));
         }
         if (!(worst == worst) || worst <= tol || it >= max_iter) break;
         solve_device(exR_.p, s, N_, exD_.p, N_, nullptr);

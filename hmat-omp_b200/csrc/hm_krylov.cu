@@ -146,7 +146,7 @@ void Engine::solve_gmres_device(const double* db, int s, int ldb, double* dx, in
         worst = 0.0;
         for (int j = 0; j < s; ++j) {
             const double beta = std::sqrt(hdots[j]);
-            worst = std::max(worst, beta / bnorm[j]);
+            worst = max_nan(worst, beta / bnorm[j]);
             g[(size_t)j * (m + 1)] = beta;
             for (int i = 1; i <= m; ++i) g[(size_t)j * (m + 1) + i] = 0.0;
             hcoef[j] = beta > 0 ? 1.0 / beta : 0.0;
