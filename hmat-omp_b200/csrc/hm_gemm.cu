@@ -840,10 +840,11 @@ void GemmBatch<T>::finalize_tc_gen(cudaStream_t s) {
 template <int GEN>
 static void launch_tc_gen(int bn, int tiles, int sms, cudaStream_t s, const GemmDesc<float>* d, const int* tp,
                           const CUtensorMap* maps, int* st, int stall, const GenParams& gp) {
-    if (bn == 32) tc::launch<32, GEN>(tiles, sms, s, d, tp, maps, st, stall, gp);
-    else if (bn == 64) tc::launch<64, GEN>(tiles, sms, s, d, tp, maps, st, stall, gp);
-    else if (bn == 96) tc::launch<96, GEN>(tiles, sms, s, d, tp, maps, st, stall, gp);
-    else tc::launch<128, GEN>(tiles, sms, s, d, tp, maps, st, stall, gp);
+    // the entry generation in the converter warps bounds these: 12 of them
+    if (bn == 32) tc::launch<32, GEN, 4, 12>(tiles, sms, s, d, tp, maps, st, stall, gp);
+    else if (bn == 64) tc::launch<64, GEN, 4, 12>(tiles, sms, s, d, tp, maps, st, stall, gp);
+    else if (bn == 96) tc::launch<96, GEN, 4, 12>(tiles, sms, s, d, tp, maps, st, stall, gp);
+    else tc::launch<128, GEN, 4, 12>(tiles, sms, s, d, tp, maps, st, stall, gp);
 }
 
 static int sm_count() {

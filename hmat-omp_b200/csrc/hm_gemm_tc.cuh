@@ -21,13 +21,14 @@
 //              (K-major, 128-byte swizzle, when k is contiguous; MN-major, 128-byte
 //              swizzle with 32-byte granules, when rows/columns are); out-of-range rows
 //              and k are zero-filled by the TMA.
-//   warps 1-8  converters: the hi/lo split of a landed stage, hi in place and lo into a
-//              twin buffer; up to 4 stages in flight.
-//   warp 9     allocates the tensor memory (two accumulator buffers) and one lane issues the
+//   warps 1..NCW converters (8, or 12 for generated-A batches): the hi/lo
+//              split of a landed stage, hi in place and lo into a twin buffer; up to 4
+//              stages in flight.
+//   warp NCW+1 allocates the tensor memory (two accumulator buffers) and one lane issues the
 //              MMAs: per k-block 4 k-steps x 4 products of 128 x BN x 8, then a commit
 //              that frees the stage; after a tile's last k-block, a commit that hands the
 //              accumulator to the epilogue.
-//   warps 10.. epilogue: 4 warps, or for short-k batches 8 (two per TMEM lane quarter,
+//   the rest   epilogue: 4 warps, or for short-k batches 8 (two per TMEM lane quarter,
 //              each taking half of the tile's columns): tcgen05.ld of the main and correction accumulators
 //              (one wait per 16 columns) into the shared C tile (loaded first by TMA when
 //              beta != 0: C = alpha acc + beta C), released accumulator, then one TMA store
@@ -44,12 +45,10 @@
 namespace tc {
 
 constexpr int BM = 128, BK = 32;
-constexpr int NCONV = 256;               // converter threads (warps 1-8)
-constexpr int MMA_WARP = 9;
-constexpr int EPI_WARP0 = 10;            // warps 10.. (4 or 8 epilogue warps)
-// threads of a CTA with EPW epilogue warps
-template <int EPW>
-constexpr int nthreads() { return (EPI_WARP0 + EPW) * 32; }
+// Warps: 0 the TMA producer, 1..NCW the converters, NCW + 1 the MMA issuer, then EPW
+// epilogue warps.  Threads of such a CTA:
+template <int EPW, int NCW>
+constexpr int nthreads() { return (NCW + 2 + EPW) * 32; }
 
 template <int BN>
 struct Shape {
@@ -308,10 +307,13 @@ __device__ __forceinline__ TileInfo decode(const GemmDesc<float>* __restrict__ d
 // GEN != GEN_DENSE: A is not read from memory but evaluated by the converter warps from
 // the kernel generator (entry (ga_r0 + i, ga_c0 + k) of op(A), or its transpose for
 // opA = OP_T) straight into the K-major stage layout; the TMA brings only B.
-template <int BN, int GEN, int EPW>
-__global__ void __launch_bounds__(nthreads<EPW>(), 1)
+template <int BN, int GEN, int EPW, int NCW>
+__global__ void __launch_bounds__(nthreads<EPW, NCW>(), 1)
 gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restrict__ tile_problem, int ntiles,
                  const CUtensorMap* __restrict__ tmaps, int* status, int stall, const GenParams gp) {
+    constexpr int NCONV = NCW * 32;        // converter threads
+    constexpr int MMA_WARP = NCW + 1;
+    constexpr int EPI_WARP0 = NCW + 2;
     using S = Shape<BN>;
     constexpr int ST = S::ST;
     extern __shared__ unsigned char smraw[];
@@ -699,18 +701,21 @@ gemm_tc32_kernel(const GemmDesc<float>* __restrict__ descs, const int* __restric
     }
 }
 
-// EPW: epilogue warps, 8 for short-k batches (the epilogue bounds them), 4 otherwise
-// (more polling warps would take issue slots from the converters of long-k tiles)
-template <int BN, int GEN = GEN_DENSE, int EPW = 4>
+// EPW: epilogue warps, 8 for short-k batches (the epilogue bounds them), 4 otherwise.
+// NCW: converter warps, 8, or 12 for generated-A batches, where the entry generation in
+// the converters bounds the kernel (12 made the Coulomb sketch 17% faster; dense long-k
+// batches, not converter-bound, were 2% slower with 12).
+template <int BN, int GEN = GEN_DENSE, int EPW = 4, int NCW = 8>
 void launch(int tiles, int sms, cudaStream_t s, const GemmDesc<float>* d, const int* tile_problem,
             const CUtensorMap* tmaps, int* status, int stall, const GenParams& gp = GenParams()) {
     static_assert(EPW == 4 || EPW == 8, "epilogue warps");
+    static_assert(NCW == 8 || NCW == 12, "converter warps (a multiple of 2 keeps the chunk k-groups)");
     using S = Shape<BN>;
     static size_t cur = 0;
-    ensure_dyn_smem(gemm_tc32_kernel<BN, GEN, EPW>, S::SMEM, cur);
+    ensure_dyn_smem(gemm_tc32_kernel<BN, GEN, EPW, NCW>, S::SMEM, cur);
     const int grid = std::max(1, std::min(tiles, sms));
-    gemm_tc32_kernel<BN, GEN, EPW><<<grid, nthreads<EPW>(), S::SMEM, s>>>(d, tile_problem, tiles, tmaps, status,
-                                                                          stall, gp);
+    gemm_tc32_kernel<BN, GEN, EPW, NCW><<<grid, nthreads<EPW, NCW>(), S::SMEM, s>>>(d, tile_problem, tiles, tmaps,
+                                                                                     status, stall, gp);
 }
 
 // Whether the tensor-core kernel can take a problem: the TMA wants 16-byte aligned bases
