@@ -372,6 +372,17 @@ static CfgShape cfg_shape(int cfg) {
     }
 }
 
+// Target k per slice when a long-k problem with few output tiles is split (atomically
+// reduced slices); HM_KSPLIT_K overrides the default.
+static int ksplit_k() {
+    static const int v = [] {
+        const char* e = std::getenv("HM_KSPLIT_K");
+        const int x = e ? std::atoi(e) : 256;
+        return x >= 32 ? x : 256;
+    }();
+    return v;
+}
+
 template <typename T>
 void GemmBatch<T>::add(int m, int n, int k, T alpha, const T* A, int lda, int opA, const T* B,
                        int ldb, int opB, T beta, T* C, int ldc, const T* kscale, int ksplit,
@@ -393,7 +404,8 @@ void GemmBatch<T>::add(int m, int n, int k, T alpha, const T* A, int lda, int op
     if (ksplit <= 0) {
         int tiles = d.tiles_m * d.tiles_n;
         ksplit = 1;
-        if (tiles < 32 && k >= 512) ksplit = std::min(std::max(1, k / 256), std::max(1, 128 / tiles));
+        const int kk = ksplit_k();
+        if (tiles < 32 && k >= 2 * kk) ksplit = std::min(std::max(1, k / kk), std::max(1, 128 / tiles));
     }
     ksplit = std::max(1, std::min(ksplit, std::max(1, ceil_div(std::max(k, 1), cs.BK))));
     if (ksplit > 1 && beta != T(0)) {

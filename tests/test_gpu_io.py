@@ -78,6 +78,34 @@ def test_hss_roundtrip_keeps_reference_factors(tmp_path):
     assert O.rel_err(h.solve(b), r.solve(b)) < 1e-12
 
 
+def test_version1_files_load(tmp_path):
+    """Files of the first format version (no nested-basis section) still load: a HODLR file
+    differs only in its version word; a reference-form HSS file also lacks the trailing
+    nested flag of version 2."""
+    x = np.random.default_rng(4).standard_normal((1024, 3))
+    m = _gauss(1024)
+    f = tmp_path / "hodlr.hmat"
+    m.save(str(f))
+    data = f.read_bytes()
+    g = tmp_path / "hodlr_v1.hmat"
+    g.write_bytes(data[:8] + struct.pack("<I", 1) + data[12:])
+    r = H.load_operator(str(g), 1e-10)
+    assert np.array_equal(m.multiply(x), r.multiply(x))
+    c = CASES["hss_gauss_512"]
+    A = make_matrix(c)
+    h = H.HSSMatrix(c["tol"], rsvd_rank=c["rsvd_rank"], seed=c["seed"])
+    h.build_from_dense(A, c["leaf"])
+    f = tmp_path / "hss.hmat"
+    h.save(str(f))
+    data = f.read_bytes()
+    assert struct.unpack("<I", data[-4:])[0] == 0   # version 2: the nested flag ends the file
+    g = tmp_path / "hss_v1.hmat"
+    g.write_bytes(data[:8] + struct.pack("<I", 1) + data[12:-4])
+    r = H.load_operator(str(g), c["tol"])
+    xs = x[:512]
+    assert not r.nested and np.array_equal(h.multiply(xs), r.multiply(xs))
+
+
 def test_bad_files_are_refused(tmp_path):
     m = _gauss(1024)
     f = tmp_path / "op.hmat"
