@@ -1,7 +1,8 @@
 """Offline tile autotuner for the batched GEMM steps.
 
 Runs a workload once per tile choice (tile width BN of the warp-tiled kernel in
-{32, 64, 96, 128}, its shape (default, 64-row tiles, 8 x 8 outputs per lane for FP64),
+{32, 64, 96, 128}, its shape (default, 64-row tiles, 8 x 8 outputs per lane for FP64,
+96-row tiles),
 tc on/off: the tcgen05 kernel for the FP32 batches the accuracy policy lets on it, the
 FP64 MMA kernel for FP64 batches) with the choice forced on every batch (HM_TILE_FORCE), times
 every GEMM step with the library's profiler, and keeps, per batch signature, the fastest
@@ -29,7 +30,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-CHOICES = [(bn, sm, tc) for bn, sm, tc in itertools.product((32, 64, 96, 128), (0, 1, 2), (0, 1))]
+CHOICES = [(bn, sm, tc) for bn, sm, tc in itertools.product((32, 64, 96, 128), (0, 1, 2, 3), (0, 1))]
 
 
 def _headline(H):

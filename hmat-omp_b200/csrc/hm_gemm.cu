@@ -373,10 +373,14 @@ static CfgShape cfg_shape(int cfg) {
 }
 
 // Target k per slice when a long-k problem with few output tiles is split (atomically
-// reduced slices); HM_KSPLIT_K overrides the default.
+// reduced slices).  Each slice accumulates in T, so the FP32 slice length bounds the
+// rounding of the FP32 projections that the mixed refinement's contraction depends on
+// (at 1024 the headline's refinement needs a third sweep).  HM_KSPLIT_K (FP32) and
+// HM_KSPLIT_K_F64 override the default of 256.
+template <typename T>
 static int ksplit_k() {
     static const int v = [] {
-        const char* e = std::getenv("HM_KSPLIT_K");
+        const char* e = std::getenv(sizeof(T) == 8 ? "HM_KSPLIT_K_F64" : "HM_KSPLIT_K");
         const int x = e ? std::atoi(e) : 256;
         return x >= 32 ? x : 256;
     }();
@@ -404,7 +408,7 @@ void GemmBatch<T>::add(int m, int n, int k, T alpha, const T* A, int lda, int op
     if (ksplit <= 0) {
         int tiles = d.tiles_m * d.tiles_n;
         ksplit = 1;
-        const int kk = ksplit_k();
+        const int kk = ksplit_k<T>();
         if (tiles < 32 && k >= 2 * kk) ksplit = std::min(std::max(1, k / kk), std::max(1, 128 / tiles));
     }
     ksplit = std::max(1, std::min(ksplit, std::max(1, ceil_div(std::max(k, 1), cs.BK))));
@@ -456,7 +460,7 @@ TileTable& tile_table() {
 }
 
 bool valid_choice(const TileChoice& c) {
-    return (c.bn == 32 || c.bn == 64 || c.bn == 96 || c.bn == 128) && (c.small >= 0 && c.small <= 2) &&
+    return (c.bn == 32 || c.bn == 64 || c.bn == 96 || c.bn == 128) && (c.small >= 0 && c.small <= 3) &&
            (c.tc == 0 || c.tc == 1);
 }
 
@@ -541,7 +545,7 @@ const TileChoice* forced_choice() {
         c.bn = bn;
         c.small = sm;
         c.tc = tc;
-        HM_CHECK(valid_choice(c), HM_ERR_ARG, "HM_TILE_FORCE: bn in {32,64,96,128}, shape 0-2, tc 0 or 1");
+        HM_CHECK(valid_choice(c), HM_ERR_ARG, "HM_TILE_FORCE: bn in {32,64,96,128}, shape 0-3, tc 0 or 1");
         return true;
     }();
     return on ? &c : nullptr;
@@ -606,6 +610,17 @@ static bool fp64_big_forced() {
     static const bool on = [] {
         const char* e = std::getenv("HM_FP64_BIG");
         return e && e[0] == '1' && e[1] == 0;
+    }();
+    return on;
+}
+
+// 96-row tiles for batches whose every problem has a multiple of 96 rows (projections
+// onto rank-96 bases) that the chosen shape would pad, on top of the tile table's choice
+// (not of HM_TILE_FORCE's); HM_TILE96=0 turns this off.
+static bool tile96_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("HM_TILE96");
+        return !(e && e[0] == '0' && e[1] == 0);
     }();
     return on;
 }
@@ -700,7 +715,16 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         pipe_shape_ = have_tuned ? tuned.small : (big > 64 && pad_big > 0.25 * rows && pad_small < pad_big ? 1 : 0);
         if (!have_tuned && pipe_shape_ == 0 && fp64_big_forced()) pipe_shape_ = 2;
         pipe_shape_ = tile::shape_for(sizeof(T), pipe_shape_);
-        if (use_dmma_) pipe_shape_ = 0;
+        if (use_dmma_ || (has_chains_ && pipe_shape_ == 3)) pipe_shape_ = 0;   // no 96-row chain kernel
+        if (!use_dmma_ && !has_chains_ && pipe_shape_ != 3 && tile96_enabled() && !forced_choice()) {
+            const int bmc = tile::bm_for(sizeof(T), pipe_bn_, pipe_shape_);
+            bool all96 = true, pads = false;
+            for (auto& d : h_) {
+                all96 &= d.m % 96 == 0;
+                pads |= d.m % bmc != 0;
+            }
+            if (all96 && pads) pipe_shape_ = 3;
+        }
         const int BM = use_dmma_ ? dmma::bm_for(pipe_bn_) : tile::bm_for(sizeof(T), pipe_bn_, pipe_shape_);
         std::vector<GemmDesc<T>> dv(h_);
         int tt = 0;
@@ -980,7 +1004,8 @@ void GemmBatch<T>::launch(cudaStream_t s, const GenParams& gp, int* status) cons
         throw Error(HM_ERR_UNSUPPORTED, "chained GEMM problems are FP64 only");
     }
     if (pipe_bn_) {
-        if (pipe_shape_ == 2) launch_tile<T, 2, false>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
+        if (pipe_shape_ == 3) launch_tile<T, 3, false>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
+        else if (pipe_shape_ == 2) launch_tile<T, 2, false>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
         else if (pipe_shape_ == 1) launch_tile<T, 1, false>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
         else launch_tile<T, 0, false>(pipe_bn_, pipe_tiles_, s, d_.p, tmap_.p);
     }

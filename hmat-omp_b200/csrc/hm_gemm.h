@@ -92,7 +92,7 @@ enum : int { CFG_64x64 = 0, CFG_N_SKINNY = 1 };
 // tile_table.json beside the loaded library ({"signature": [bn, small, tc], ...},
 // written by autotune.py).  Batches without an entry keep the built-in heuristics.
 struct TileChoice {
-    int bn = 0, small = 0, tc = 1;   // small: the shape (0, 1, 2)
+    int bn = 0, small = 0, tc = 1;   // small: the shape (0 default, 1 64-row, 2 FP64 8 x 8, 3 96-row)
 };
 bool tile_choice(const std::string& sig, TileChoice& out);
 // Replace the table with the one in `path` (an empty path clears it); false if the file

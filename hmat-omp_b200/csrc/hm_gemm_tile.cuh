@@ -65,6 +65,16 @@ template <> struct For<double, 128, 2> { using C = Cfg<double, 2, 4, 2, 2, 1>; }
 template <> struct For<double, 96, 2> { using C = Cfg<double, 2, 3, 2, 2, 1>; };
 template <> struct For<double, 64, 2> { using C = Cfg<double, 2, 2, 2, 2, 1>; };
 template <> struct For<double, 32, 2> { using C = Cfg<double, 4, 1, 2, 2, 1>; };
+// SHAPE 3: 96-row tiles (three warp rows), for batches whose rows come in multiples of 96
+// (projections onto rank-96 bases: m = rank), where 64- or 128-row tiles pad a quarter
+template <> struct For<float, 128, 3> { using C = Cfg<float, 3, 4, 1, 2>; };
+template <> struct For<float, 96, 3> { using C = Cfg<float, 3, 2, 1, 3, 2>; };
+template <> struct For<float, 64, 3> { using C = Cfg<float, 3, 2, 1, 2, 3>; };
+template <> struct For<float, 32, 3> { using C = Cfg<float, 3, 2, 1, 1, 4>; };
+template <> struct For<double, 128, 3> { using C = Cfg<double, 3, 4, 1, 2, 1>; };
+template <> struct For<double, 96, 3> { using C = Cfg<double, 3, 2, 1, 3, 1>; };
+template <> struct For<double, 64, 3> { using C = Cfg<double, 3, 2, 1, 2, 2>; };
+template <> struct For<double, 32, 3> { using C = Cfg<double, 3, 2, 1, 1, 3>; };
 
 // SHAPE 2 exists for FP64 only (FP32 batches fall back to SHAPE 0)
 inline int shape_for(size_t elem, int shape) { return (shape == 2 && elem == 4) ? 0 : shape; }
@@ -72,6 +82,7 @@ inline int shape_for(size_t elem, int shape) { return (shape == 2 && elem == 4) 
 inline int bm_for(size_t elem, int bn, int shape = 0) {
     shape = shape_for(elem, shape);
     if (shape == 1) return 64;
+    if (shape == 3) return 96;
     if (shape == 2) return bn == 32 ? 256 : 128;
     if (elem == 4) return bn == 32 ? 256 : 128;
     return bn == 128 ? 64 : 128;

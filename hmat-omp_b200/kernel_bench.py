@@ -33,6 +33,9 @@ def main():
     ap.add_argument("--n", type=int, default=96)
     ap.add_argument("--k", type=int, default=96)
     ap.add_argument("--beta", type=float, default=1.0)
+    ap.add_argument("--opa", type=int, default=0, choices=[0, 1],
+                    help="1: op(A) = A^T with A stored k x m (the projections V^T x: m = rank, k = node rows)")
+    ap.add_argument("--ksplit", type=int, default=1, help="k slices per problem (0: the library's choice)")
     ap.add_argument("--order", type=int, default=256, help="inverse: matrix order")
     ap.add_argument("--iters", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
@@ -50,16 +53,18 @@ def main():
     if a.what == "gemm":
         dt = torch.float32 if a.dtype == "f32" else torch.float64
         w = 4 if a.dtype == "f32" else 8
-        A = torch.randn(a.count, a.k, a.m, dtype=dt, device=dev)     # each problem column-major m x k
+        # each problem column-major: m x k (opa 0) or k x m (opa 1)
+        A = torch.randn(a.count, a.k, a.m, dtype=dt, device=dev) if a.opa == 0 else \
+            torch.randn(a.count, a.m, a.k, dtype=dt, device=dev)
         B = torch.randn(a.count, a.n, a.k, dtype=dt, device=dev)     # k x n
         C = torch.randn(a.count, a.n, a.m, dtype=dt, device=dev)     # m x n
         flags = {"fma": H.GEMM_FMA, "tc": H.GEMM_TENSOR_CORES, "auto": H.GEMM_AUTO}[a.kernel]
         args = ([a.m] * a.count, [a.n] * a.count, [a.k] * a.count, 1.0, [A[i].data_ptr() for i in range(a.count)],
-                [a.m] * a.count, 0, [B[i].data_ptr() for i in range(a.count)], [a.k] * a.count, 0, a.beta,
+                [a.m if a.opa == 0 else a.k] * a.count, a.opa, [B[i].data_ptr() for i in range(a.count)], [a.k] * a.count, 0, a.beta,
                 [C[i].data_ptr() for i in range(a.count)], [a.m] * a.count)
 
         def run():
-            d.gemm(*args, ksplit=1, flags=flags, dtype=a.dtype)
+            d.gemm(*args, ksplit=a.ksplit, flags=flags, dtype=a.dtype)
         flops = 2.0 * a.m * a.n * a.k * a.count
         nbytes = w * a.count * (a.m * a.k + a.k * a.n + a.m * a.n * (2 if a.beta != 0 else 1))
     else:
@@ -85,7 +90,7 @@ def main():
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / a.iters
     print(json.dumps({"what": a.what, "dtype": a.dtype, "kernel": a.kernel, "count": a.count, "m": a.m, "n": a.n,
-                      "k": a.k, "beta": a.beta, "ms_per_launch_incl_host": ms, "flops": flops, "bytes": nbytes,
+                      "k": a.k, "beta": a.beta, "opa": a.opa, "ksplit": a.ksplit, "ms_per_launch_incl_host": ms, "flops": flops, "bytes": nbytes,
                       "tflops": flops / ms / 1e9, "gbs": nbytes / ms / 1e6,
                       "note": "each call also plans and uploads its tables (synchronising): the time includes that"}))
 

@@ -6,12 +6,16 @@
   store) or whose leading dimension is not TMA-addressable.  Elementwise bound of an FP32
   GEMM: |C - C64| <= 8 k u32 (|alpha| |A||B| + |beta| |C0|), u32 = 2^-24.
 * the FP64 MMA kernel against an FP64 product (1e-13 relative).
+* the warp-tiled kernel's 96-row tiles at every tile width, FP32 and FP64, forced by a
+  tile-table entry.
 * the tcgen05 kernel's bounded waits: HM_GEMM_TEST_STALL makes them run out, the call
   returns HM_ERR_TIMEOUT, and the next call on the same handle is correct.
 * hm_inverse_batched_device (Matrix::inverse, matrix.h:133-149) with pivoting at every
   size: matrices whose leading half-block is singular, in place and out of place;
   X A - I within 50 n cond(A) u64 (normwise); a singular matrix gives HM_ERR_SINGULAR.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -86,6 +90,67 @@ def test_gemm_f32_vs_fp64(kernel):
             # rows past m in the padded leading dimension are untouched
             if p["ldc"] > m:
                 assert torch.count_nonzero(p["C"][:, m:]).item() == 0
+
+
+def _gemm_signature(dtype, count, m, n, k):
+    """The tuning signature GemmBatch::finalize gives a C-ABI batch of `count` problems
+    of one shape: tag|type|p(count, next power of 2)|m(next power of 2)|n(multiple of 32)|
+    k(median, next power of 2)."""
+    def p2(v):
+        q = 1
+        while q < v:
+            q <<= 1
+        return q
+    return f"gemm_batched|{dtype}|p{p2(count)}|m{p2(m)}|n{-(-n // 32) * 32}|k{p2(k)}"
+
+
+# (m, n, k, opA, opB, beta, ksplit, ld pad) for the 96-row tiles: whole tiles (m = 96,
+# 192), a ragged last tile (m = 290), split-K with beta 0 and 1, both operand layouts
+TILE96_CASES = [
+    (96, 64, 2048, 1, 0, 0.0, 0, 0),     # the projection shape V^T x: automatic split-K
+    (192, 96, 300, 0, 1, 1.0, 1, 0),
+    (290, 40, 256, 1, 1, -2.0, 1, 1),
+    (96, 128, 4096, 0, 0, 1.0, 4, 0),
+]
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+def test_gemm_tile96_vs_fp64(dtype, tmp_path):
+    """The warp-tiled kernel's 96-row tile shape (shape 3) at every tile width, forced by a
+    tile-table entry, against FP64 products (FP32: the elementwise bound above; FP64:
+    1e-13 normwise)."""
+    import json
+    torch = _torch()
+    tdt = torch.float32 if dtype == "f32" else torch.float64
+    d = H.Dense()
+    rng = np.random.default_rng(10)
+    alpha = 0.75
+    try:
+        for bn in (32, 64, 96, 128):
+            for (m, n, k, opA, opB, beta, ksplit, pad) in TILE96_CASES:
+                f = tmp_path / f"t{bn}.json"
+                f.write_text(json.dumps({_gemm_signature(dtype, 3, m, n, k): [bn, 3, 0]}))
+                H.tile_table_load(str(f))
+                probs = [_gemm_problem(torch, rng, m, n, k, opA, opB, beta, pad, tdt) for _ in range(3)]
+                d.gemm([m] * 3, [n] * 3, [k] * 3, alpha, [p["A"].data_ptr() for p in probs],
+                       [p["lda"] for p in probs], opA, [p["B"].data_ptr() for p in probs], [p["ldb"] for p in probs],
+                       opB, beta, [p["C"].data_ptr() for p in probs], [p["ldc"] for p in probs], ksplit=ksplit,
+                       flags=H.GEMM_FMA, dtype=dtype)
+                torch.cuda.synchronize()
+                for p in probs:
+                    ref = alpha * p["opa"] @ p["opb"] + beta * p["C0"]
+                    got = p["C"][:, :m].T.double().cpu().numpy()
+                    if dtype == "f32":
+                        bound = 8 * k * U32 * (abs(alpha) * np.abs(p["opa"]) @ np.abs(p["opb"]) +
+                                               abs(beta) * np.abs(p["C0"]))
+                        assert np.all(np.abs(got - ref) <= bound), (bn, m, n, k)
+                    else:
+                        assert np.linalg.norm(got - ref) <= 1e-13 * np.linalg.norm(ref), (bn, m, n, k)
+                    if p["ldc"] > m:
+                        assert torch.count_nonzero(p["C"][:, m:]).item() == 0
+    finally:   # the library's own table again
+        H.tile_table_load(os.environ.get("HM_TILE_TABLE") or
+                          os.path.join(os.path.dirname(os.path.abspath(H.__file__)), "tile_table.json"))
 
 
 def test_gemm_tc_rejects_unaligned():

@@ -30,7 +30,7 @@ def test_valid_table_loads(tmp_path, lib):
 
 @pytest.mark.parametrize("text", [
     '{"a": [48, 0, 0]}',          # bn not a tile width
-    '{"a": [64, 3, 0]}',          # shape not 0/1/2
+    '{"a": [64, 4, 0]}',          # shape not 0-3
     '{"a": [64, 0]}',             # too short
     '{"a": [64, 0, 0] "b": [32, 0, 0]}',
     '["a", 64, 0, 0]',
