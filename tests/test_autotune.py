@@ -26,5 +26,5 @@ def test_select_keeps_only_clear_wins_and_drops_stale_entries():
 
 
 def test_choices_cover_every_tile_width_and_flag():
-    assert len(autotune.CHOICES) == 24
+    assert len(autotune.CHOICES) == 32
     assert {c[0] for c in autotune.CHOICES} == {32, 64, 96, 128}
