@@ -418,3 +418,154 @@ def to_torch_share(top: dict, device):
     import torch
     cv = lambda a: torch.as_tensor(a, dtype=torch.float64, device=device)
     return {d: TopCoupling(cv(c.B12), cv(c.B21), cv(c.U), cv(c.V)) for d, c in top.items()}
+
+
+# ------------------------------------------------------------------------------------
+# Sharded compression of the top-level couplings
+# ------------------------------------------------------------------------------------
+def _packed_allreduce(ops, allreduce, shapes: list, me: int, mine):
+    """Sum over all ranks of one buffer holding block i (shapes[i] = (rows, cols)) side by
+    side; this rank writes `mine` into block `me` and gets that block's sum back."""
+    rows = max(max(r for r, _ in shapes), 1)
+    offs, c0 = [], 0
+    for _, c in shapes:
+        offs.append(c0)
+        c0 += c
+    buf = ops.zeros(rows, max(c0, 1))
+    r, c = shapes[me]
+    if r and c and mine is not None:
+        buf[:r, offs[me]:offs[me] + c] = mine
+    out = allreduce(buf)
+    out = buf if out is None else out
+    return out[:r, offs[me]:offs[me] + c]
+
+
+def build_top_sharded(plan: ShardPlan, rank: int, block_product, tol: float, max_rank: int, oversample: int = 10,
+                      power_iters: int = 0, seed: int = 0, ops=None, allreduce=None):
+    """Compress the couplings of every top node (depth < p) with their rows spread over
+    the ranks, so that no rank builds more than its own rows of the operator.
+
+    For top node n with children c1 = [start, mid) and c2 = [mid, end), the ranks under c1
+    hold A12 = A[c1, c2] by rows and the ranks under c2 hold A21 = A[c2, c1].  Each block
+    is compressed by a randomized range finder (the steps of compression.h:67-99) whose
+    row dimension is distributed:
+      Y_g = A[R_g, C] Omega          (local rows R_g; Omega |C| x k from (seed, depth,
+                                      slot, side), the same on every rank of the block)
+      [power iterations: Y_g = A[R_g, C] (sum_g A[R_g, C]^T Q_g)]
+      Q_g = Y_g W L^{-1/2}            (Gram-eigen orthonormalisation, twice: G = sum_g
+                                      Y_g^T Y_g is all-reduced, k x k; directions with
+                                      eigenvalues below 1e-28 of the largest become zero)
+      X   = sum_g A[R_g, C]^T Q_g     (all-reduced, |C| x k)
+      X   = Z S W^T (SVD, redundantly on every rank of the block)
+      A[R, C] ~= (Q W_r) diag(S_r) Z_r^T,  r = #{S_i > tol S_0} (<= max_rank, >= 1).
+    U rows stay where they were computed; Z_r (the other child's basis) and S_r go to the
+    ranks under the other child by one packed all-reduce per depth.
+
+    block_product(r0, r1, c0, c1, X, trans) returns A[r0:r1, c0:c1] @ X (trans False) or
+    A[r0:r1, c0:c1]^T @ X (trans True) in the ops back end.  Every rank issues the same
+    collectives in the same order (packed per depth).  Returns (top, table, count):
+    {depth: TopCoupling} for this rank's path, the replicated rank table
+    {(depth, slot): (p1, p2, q1, q2)} that ShardedHODLR takes, and the number of
+    collectives issued."""
+    import numpy as np
+    ops = ops or NumpyOps()
+    allreduce = allreduce or numpy_allreduce_gloo
+    k = max_rank + oversample
+    s_g, e_g = plan.bounds[rank]
+    top, table, count = {}, {}, 0
+
+    def to_np(a):
+        return a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+
+    def from_np(a, like):
+        if hasattr(like, "detach"):
+            import torch
+            return torch.as_tensor(a, dtype=torch.float64, device=like.device)
+        return np.asarray(a, dtype=np.float64)
+
+    for d, lvl in enumerate(plan.levels):
+        me = plan.path(rank)[d]
+        side = plan.side(me, rank)
+        # block of node i, side j at position 2 i + j in every packed buffer
+        pos = 2 * me.slot + side
+        R0, R1 = (me.start, me.mid) if side == 0 else (me.mid, me.end)     # this block's rows
+        C0, C1 = (me.mid, me.end) if side == 0 else (me.start, me.mid)     # its columns
+        ncol = C1 - C0
+        colsz = []
+        for m in lvl:
+            colsz += [m.end - m.mid, m.mid - m.start]
+
+        def reduce_kk(mine):
+            nonlocal count
+            count += 1
+            return _packed_allreduce(ops, allreduce, [(k, k)] * (2 * len(lvl)), pos, mine)
+
+        def reduce_cols(mine):
+            nonlocal count
+            count += 1
+            return _packed_allreduce(ops, allreduce, [(c, k) for c in colsz], pos, mine)
+
+        def orth(Y):
+            for _ in range(2):
+                G = to_np(reduce_kk(Y.T @ Y))
+                G = 0.5 * (G + G.T)
+                lam, W = np.linalg.eigh(G)
+                lmax = max(lam.max(), 0.0)
+                keep = lam > 1e-28 * lmax if lmax > 0 else np.zeros_like(lam, dtype=bool)
+                scale = np.where(keep, 1.0 / np.sqrt(np.where(keep, lam, 1.0)), 0.0)
+                Y = Y @ from_np(W * scale[None, :], Y)
+            return Y
+
+        omega = np.random.default_rng([seed, d, me.slot, side]).standard_normal((ncol, k))
+        like = ops.zeros(1, 1)
+        Y = block_product(s_g, e_g, C0, C1, from_np(omega, like), False)
+        for _ in range(power_iters):
+            Q = orth(Y)
+            Z = reduce_cols(block_product(s_g, e_g, C0, C1, Q, True))
+            Y = block_product(s_g, e_g, C0, C1, Z, False)
+        Q = orth(Y)
+        X = to_np(reduce_cols(block_product(s_g, e_g, C0, C1, Q, True)))
+        Zs, S, Wt = np.linalg.svd(X, full_matrices=False)
+        r = 1
+        if S.size and S[0] > 1e-15:
+            r = max(1, min(int(np.sum(S > tol * S[0])), max_rank))
+        U_rows = Q @ from_np(Wt.T[:, :r], Q)
+        # ranks and singular values to everyone (only the first rank of each block
+        # contributes, so the sums are the values)
+        first = (s_g == R0)
+        meta = np.zeros((1, 1 + max_rank))
+        if first:
+            meta[0, 0] = r
+            meta[0, 1:1 + r] = S[:r]
+        count += 1
+        allmeta = to_np(allreduce(from_np(np.concatenate(
+            [meta if i == pos else np.zeros_like(meta) for i in range(2 * len(lvl))], axis=1), like)))
+        rk = [int(round(allmeta[0, i * (1 + max_rank)])) for i in range(2 * len(lvl))]
+        sv = [allmeta[0, i * (1 + max_rank) + 1:i * (1 + max_rank) + 1 + rk[i]] for i in range(2 * len(lvl))]
+        for i, m in enumerate(lvl):
+            r12, r21 = rk[2 * i], rk[2 * i + 1]
+            table[(d, m.slot)] = (r12, r21, r21, r12)
+        # the other child's basis: block (2 i + j) carries Z_r of side j (|C_j| x r_j),
+        # written by the block's first rank; each rank reads the opposite block
+        shapes = [(colsz[i], rk[i]) for i in range(2 * len(lvl))]
+        rows = max(max(c for c, _ in shapes), 1)
+        offs, c0 = [], 0
+        for _, c in shapes:
+            offs.append(c0)
+            c0 += c
+        buf = ops.zeros(rows, max(c0, 1))
+        if first:
+            buf[:ncol, offs[pos]:offs[pos] + r] = from_np(Zs[:, :r], like)
+        count += 1
+        out = allreduce(buf)
+        out = buf if out is None else out
+        o = pos ^ 1
+        Vother = out[:colsz[o], offs[o]:offs[o] + rk[o]]   # the basis of this rank's child, all rows
+        B_mine = from_np(np.diag(sv[pos]), like)
+        B_other = from_np(np.diag(sv[pos ^ 1]), like)
+        V_rows = Vother[s_g - R0:e_g - R0]
+        if side == 0:
+            top[d] = TopCoupling(B_mine, B_other, U_rows, V_rows)
+        else:
+            top[d] = TopCoupling(B_other, B_mine, U_rows, V_rows)
+    return top, table, count
