@@ -614,9 +614,11 @@ static bool fp64_big_forced() {
     return on;
 }
 
-// 96-row tiles for batches whose every problem has a multiple of 96 rows (projections
-// onto rank-96 bases) that the chosen shape would pad, on top of the tile table's choice
-// (not of HM_TILE_FORCE's); HM_TILE96=0 turns this off.
+// 96-row tiles for batches of tile width <= 64 whose every problem has a multiple of 96
+// rows (projections onto rank-96 bases of 64 right-hand sides) that the chosen shape would
+// pad, on top of the tile table's choice (not of HM_TILE_FORCE's); HM_TILE96=0 turns this
+// off.  At width 96 (V^T Q, V^T W of the factorization) the 96 x 96 tile measured slower
+// than the table's choice: 1 CTA of 6 warps per SM in FP64.
 static bool tile96_enabled() {
     static const bool on = [] {
         const char* e = std::getenv("HM_TILE96");
@@ -716,7 +718,8 @@ void GemmBatch<T>::finalize(cudaStream_t s) {
         if (!have_tuned && pipe_shape_ == 0 && fp64_big_forced()) pipe_shape_ = 2;
         pipe_shape_ = tile::shape_for(sizeof(T), pipe_shape_);
         if (use_dmma_ || (has_chains_ && pipe_shape_ == 3)) pipe_shape_ = 0;   // no 96-row chain kernel
-        if (!use_dmma_ && !has_chains_ && pipe_shape_ != 3 && tile96_enabled() && !forced_choice()) {
+        if (!use_dmma_ && !has_chains_ && pipe_shape_ != 3 && pipe_bn_ <= 64 && tile96_enabled() &&
+            !forced_choice()) {
             const int bmc = tile::bm_for(sizeof(T), pipe_bn_, pipe_shape_);
             bool all96 = true, pads = false;
             for (auto& d : h_) {

@@ -355,8 +355,8 @@ HM_API size_t hm_profile_sequence(char* buf, size_t len);
 /* ---- tile autotuning (no counterpart in the reference) ----
  * Batched-GEMM steps pick their kernel and tile shape (width BN of the warp-tiled kernel;
  * shape 0 default, 1 64-row tiles, 2 8 x 8 outputs per lane for FP64, 3 96-row tiles;
- * batches whose rows all come in multiples of 96 take 96-row tiles unless the table's
- * shape already fits them or HM_TILE96=0; tc: the tcgen05
+ * batches of tile width <= 64 whose rows all come in multiples of 96 take 96-row tiles
+ * unless the table's shape already fits them or HM_TILE96=0; tc: the tcgen05
  * kernel for eligible FP32 batches, the FP64 MMA kernel for FP64 batches) from a table
  * keyed by the batch's signature (step, element type, bucketed problem count and m/n/k),
  * written by hmat-omp_b200/autotune.py from timed sweeps:
