@@ -480,4 +480,48 @@ int hm_inverse_batched_device(hm_handle* h, int count, const int* n, const doubl
     });
 }
 
+int hm_kernel_block_product_device(hm_handle* h, int kernel, const double* points, int dim, int N,
+                                   const double* params, int nparams, int r0, int r1, int c0, int c1, int trans,
+                                   const double* dX, int ldx, int nrhs, double* dY, int ldy) {
+    return guard(h, [&] {
+        HM_CHECK(points && N > 0 && dim >= 1 && dim <= 3 && params && nparams >= 2, HM_ERR_ARG,
+                 "kernel_block_product: bad arguments");
+        const int gen = kernel == HM_KERNEL_CAUCHY ? hm::GEN_CAUCHY
+                        : kernel == HM_KERNEL_GAUSSIAN ? hm::GEN_GAUSSIAN
+                        : kernel == HM_KERNEL_COULOMB ? hm::GEN_COULOMB : -1;
+        HM_CHECK(gen > 0, HM_ERR_ARG, "kernel_block_product: unknown kernel");
+        HM_CHECK(kernel != HM_KERNEL_CAUCHY || dim == 1, HM_ERR_ARG, "Cauchy points are 1-D");
+        HM_CHECK(0 <= r0 && r0 <= r1 && r1 <= N && 0 <= c0 && c0 <= c1 && c1 <= N, HM_ERR_ARG,
+                 "kernel_block_product: row or column range outside [0, N)");
+        const int m = trans ? c1 - c0 : r1 - r0, k = trans ? r1 - r0 : c1 - c0;
+        HM_CHECK(nrhs >= 0 && ldx >= std::max(1, k) && ldy >= std::max(1, m), HM_ERR_ARG,
+                 "kernel_block_product: bad column count or leading dimension");
+        if (m == 0 || nrhs == 0) return;
+        HM_CHECK(dY && (k == 0 || dX), HM_ERR_ARG, "kernel_block_product: null matrix");
+        const size_t npts = kernel == HM_KERNEL_CAUCHY ? 2 * (size_t)N : (size_t)N * dim;
+        for (size_t i = 0; i < npts; ++i)
+            HM_CHECK(std::isfinite(points[i]), HM_ERR_NONFINITE, "kernel_block_product: non-finite point");
+        cudaStream_t s = h->stream;
+        hm::DBuf<double> dp(npts);
+        HM_CUDA(cudaMemcpyAsync(dp.p, points, npts * sizeof(double), cudaMemcpyHostToDevice, s));
+        hm::GenParams gp;
+        gp.pts = dp.p;
+        gp.N = N;
+        gp.dim = dim;
+        gp.p0 = params[0];
+        gp.p1 = params[1];
+        // the generated operand is op(A) with A(i, j) = entry(r0 + i, c0 + j)
+        hm::GemmBatch<double> batch(nrhs <= 16 ? hm::CFG_N_SKINNY : hm::CFG_64x64, gen);
+        batch.set_tag("kernel_block_product");
+        batch.add(m, nrhs, k, 1.0, nullptr, 0, trans ? hm::OP_T : hm::OP_N, dX, ldx, hm::OP_N, 0.0, dY, ldy, nullptr, 0,
+                  r0, c0);
+        batch.finalize(s);
+        hm::DBuf<int> status(1);
+        status.zero(s);
+        batch.launch(s, gp, status.p);
+        hm::count_launch(batch.nlaunch());
+        HM_CUDA(cudaStreamSynchronize(s));   // the points buffer outlives the launch
+    });
+}
+
 }  // extern "C"

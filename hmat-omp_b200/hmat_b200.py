@@ -124,6 +124,9 @@ def load() -> C.CDLL:
         getattr(L, f).argtypes = [C.c_void_p, C.c_int, _ip, _ip, _ip, T, PPd, _ip, C.c_int, PPd, _ip, C.c_int, T,
                                   PPd, _ip, C.c_int, C.c_int]
     L.hm_inverse_batched_device.argtypes = [C.c_void_p, C.c_int, _ip, PPd, _ip, PPd, _ip]
+    L.hm_kernel_block_product_device.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                                 C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                                 C.c_int, C.c_int, C.c_void_p, C.c_int]
     L.hm_tile_table_load.argtypes = [C.c_char_p]
     L.hm_tile_table_size.argtypes = []
     _lib = L
@@ -426,6 +429,19 @@ class Dense(_Handle):
         na, la, lx = self._ia(n), self._ia(lda), self._ia(ldx)
         self._check(self._L.hm_inverse_batched_device(self._h, cnt, na.ctypes.data_as(_ip), PP(*A),
                                                       la.ctypes.data_as(_ip), PP(*X), lx.ctypes.data_as(_ip)))
+
+    def kernel_block_product(self, kernel, points, params, r0, r1, c0, c1, X, ldx, nrhs, Y, ldy, trans=False):
+        """Y = A[r0:r1, c0:c1] X (or its transpose times X) with A generated from `points`
+        (host, hm_hodlr_build_from_kernel's layout); X, Y device pointers, column-major."""
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        if kernel == KERNEL_CAUCHY:
+            N, dim = pts.size // 2, 1
+        else:
+            N, dim = pts.reshape(pts.shape[0], -1).shape
+        prm = np.ascontiguousarray(params, dtype=np.float64)
+        self._check(self._L.hm_kernel_block_product_device(self._h, kernel, pts.ctypes.data, dim, N, prm.ctypes.data,
+                                                           len(prm), r0, r1, c0, c1, int(bool(trans)), C.c_void_p(X),
+                                                           ldx, nrhs, C.c_void_p(Y), ldy))
 
 
 class HODLRMatrix(_Handle):

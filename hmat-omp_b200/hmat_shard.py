@@ -569,3 +569,22 @@ def build_top_sharded(plan: ShardPlan, rank: int, block_product, tol: float, max
         else:
             top[d] = TopCoupling(B_other, B_mine, U_rows, V_rows)
     return top, table, count
+
+
+def device_block_product(dense, kernel: int, points, params):
+    """block_product for build_top_sharded on the device: A[r0:r1, c0:c1] @ X (or the
+    transposed product) with A's entries generated by the engine
+    (hm_kernel_block_product_device), never stored.  X and the result are FP64 torch
+    tensors on the device; `dense` is an hmat_b200.Dense handle working on torch's current
+    stream, `points` the host points of hm_hodlr_build_from_kernel's layout."""
+    import torch
+
+    def prod(r0, r1, c0, c1, X, trans):
+        m = (c1 - c0) if trans else (r1 - r0)
+        k, s = X.shape
+        Xc = X.T.contiguous()                                   # column-major k x s
+        Yc = torch.empty((s, m), dtype=torch.float64, device=X.device)
+        dense.kernel_block_product(kernel, points, params, r0, r1, c0, c1, Xc.data_ptr(), max(k, 1), s,
+                                   Yc.data_ptr(), max(m, 1), trans=trans)
+        return Yc.T
+    return prod

@@ -334,6 +334,17 @@ HM_API int hm_gemm_batched_f64_device(hm_handle* h, int count, const int* m, con
  * pivot is zero or non-finite.  Runs on the handle's stream; synchronises. */
 HM_API int hm_inverse_batched_device(hm_handle* h, int count, const int* n, const double* const* A,
                                      const int* lda, double* const* X, const int* ldx);
+/* Y = A[r0:r1, c0:c1] X (trans 0) or Y = A[r0:r1, c0:c1]^T X (trans 1) for a kernel matrix
+ * A generated on the device from `points` (the layout and kernels of
+ * hm_hodlr_build_from_kernel; params p0, p1), entries never stored: FP64, 2 m k nrhs
+ * flops.  The product a rank needs to compress its rows of a coupling block without
+ * forming it (the sharded build of hmat_shard.build_top_sharded; the reference forms its
+ * blocks densely, compression.h:77-87).  X (k x nrhs, ld ldx) and Y (m x nrhs, ld ldy) are
+ * device memory, column-major, with m = r1 - r0 and k = c1 - c0 (swapped for trans).
+ * Runs on the handle's stream; synchronises. */
+HM_API int hm_kernel_block_product_device(hm_handle* h, int kernel, const double* points, int dim, int N,
+                                          const double* params, int nparams, int r0, int r1, int c0, int c1,
+                                          int trans, const double* dX, int ldx, int nrhs, double* dY, int ldy);
 
 /* ---- instrumentation (no counterpart in the reference, which only wall-clocks its
  *      drivers: main_hodlr.cpp:14-24) ---- */

@@ -8,6 +8,8 @@
 * the FP64 MMA kernel against an FP64 product (1e-13 relative).
 * the warp-tiled kernel's 96-row tiles at every tile width, FP32 and FP64, forced by a
   tile-table entry.
+* hm_kernel_block_product_device (a generated kernel block times X, and its transpose)
+  against the dense FP64 matrix, for the three kernels.
 * the tcgen05 kernel's bounded waits: HM_GEMM_TEST_STALL makes them run out, the call
   returns HM_ERR_TIMEOUT, and the next call on the same handle is correct.
 * hm_inverse_batched_device (Matrix::inverse, matrix.h:133-149) with pivoting at every
@@ -151,6 +153,45 @@ def test_gemm_tile96_vs_fp64(dtype, tmp_path):
     finally:   # the library's own table again
         H.tile_table_load(os.environ.get("HM_TILE_TABLE") or
                           os.path.join(os.path.dirname(os.path.abspath(H.__file__)), "tile_table.json"))
+
+
+@pytest.mark.parametrize("kernel", [H.KERNEL_COULOMB, H.KERNEL_GAUSSIAN, H.KERNEL_CAUCHY])
+def test_kernel_block_product_vs_dense(kernel):
+    """hm_kernel_block_product_device: A[r0:r1, c0:c1] X and its transpose product with A
+    generated on the device, against the dense FP64 matrix (1e-13 normwise): off-diagonal
+    blocks, a block across the diagonal (the shift), skinny and wide right-hand sides."""
+    import hmat_oracle as O
+    torch = _torch()
+    d = H.Dense()
+    rng = np.random.default_rng(12)
+    N = 3000
+    if kernel == H.KERNEL_COULOMB:
+        pts, params = rng.random((N, 2)), [1e-3, 4.0]
+        A = O.coulomb_matrix(pts, 1e-3, 4.0)
+    elif kernel == H.KERNEL_GAUSSIAN:
+        pts, params = np.sort(rng.random(N)).reshape(-1, 1), [0.05, 1e-2]
+        A = O.gaussian_matrix(pts[:, 0], 0.05, 1e-2)
+    else:
+        pts, params = np.concatenate([np.arange(N) / N, (np.arange(N) + 0.5) / N]), [0.0, 0.0]
+        A = O.cauchy_matrix(N)
+    for (r0, r1, c0, c1) in [(0, 1000, 1500, 3000), (1500, 3000, 0, 1500), (200, 900, 100, 800)]:
+        for nrhs in (5, 70):
+            for trans in (False, True):
+                blk = A[r0:r1, c0:c1]
+                op = blk.T if trans else blk
+                m, k = op.shape
+                X = rng.standard_normal((k, nrhs))
+                Xd = torch.from_numpy(np.asfortranarray(X).T.copy()).cuda()      # column-major k x nrhs
+                Yd = torch.full((nrhs, m + 3), 7.0, dtype=torch.float64, device="cuda")   # ld = m + 3
+                d.kernel_block_product(kernel, pts, params, r0, r1, c0, c1, Xd.data_ptr(), k, nrhs,
+                                       Yd.data_ptr(), m + 3, trans=trans)
+                torch.cuda.synchronize()
+                Y = Yd[:, :m].T.cpu().numpy()
+                ref = op @ X
+                assert np.linalg.norm(Y - ref) <= 1e-13 * np.linalg.norm(ref), (r0, r1, c0, c1, nrhs, trans)
+                assert torch.all(Yd[:, m:] == 7.0).item()      # rows past m untouched
+    with pytest.raises(H.HmError):
+        d.kernel_block_product(kernel, pts, params, 0, N + 1, 0, 10, Xd.data_ptr(), 10, 1, Yd.data_ptr(), N + 1)
 
 
 def test_gemm_tc_rejects_unaligned():
