@@ -11,7 +11,9 @@ tolerance 1e-10, which the top couplings do not reach at these ranks.  Checked:
   power iteration and 10 oversampling columns is near-optimal);
 * the sharded factor + solve against a dense LAPACK solve of the operator the ranks built
   (their subtrees expanded, the couplings assembled): <= 1e-10;
-* the same number of collectives and one rank table on every rank."""
+* the same number of collectives and one rank table on every rank.
+Both array back ends run it: numpy, and torch tensors (the device path's code, here on
+the CPU) with torch.distributed's all-reduce."""
 import os
 import socket
 import sys
@@ -53,7 +55,7 @@ class _LocalSolver:
         return self.F.solve(Y)
 
 
-def _worker(rank, world, port, q):
+def _worker(rank, world, port, backend, q):
     sys.path[:0] = [os.path.join(ROOT, "hmat-omp_b200"), os.path.join(ROOT, "oracle")]
     import torch.distributed as dist
 
@@ -65,13 +67,22 @@ def _worker(rank, world, port, q):
         plan = S.partition(N, LEAF, world)
         s, e = plan.owner_range(rank)
 
+        if backend == "torch":
+            import torch
+            At = torch.from_numpy(A)
+            ops, allreduce = S.TorchOps("cpu"), S.torch_allreduce
+        else:
+            At, ops, allreduce = A, S.NumpyOps(), S.numpy_allreduce_gloo
+
         def block_product(r0, r1, c0, c1, X, trans):
             assert (r0, r1) == (s, e)       # only this rank's rows are ever asked for
-            blk = A[r0:r1, c0:c1]
+            blk = At[r0:r1, c0:c1]
             return blk.T @ X if trans else blk @ X
 
         top, table, nc = S.build_top_sharded(plan, rank, block_product, TOL, MAXR, oversample=10, power_iters=1,
-                                             seed=5, ops=S.NumpyOps(), allreduce=S.numpy_allreduce_gloo)
+                                             seed=5, ops=ops, allreduce=allreduce)
+        np_of = (lambda t: t.numpy()) if backend == "torch" else (lambda t: t)
+        top = {d: S.TopCoupling(*(np_of(t) for t in (c.B12, c.B21, c.U, c.V))) for d, c in top.items()}
         local = _LocalSolver(A[s:e, s:e])
         sh = S.ShardedHODLR(plan, rank, local, top, table, S.NumpyOps(), S.numpy_allreduce_gloo)
         b = np.random.default_rng(11).standard_normal((N, 3))
@@ -84,8 +95,8 @@ def _worker(rank, world, port, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_sharded_build_and_solve(world):
+@pytest.mark.parametrize("world,backend", [(2, "numpy"), (4, "numpy"), (2, "torch")])
+def test_sharded_build_and_solve(world, backend):
     import torch.multiprocessing as mp
     sys.path[:0] = [os.path.join(ROOT, "hmat-omp_b200"), os.path.join(ROOT, "oracle")]
     import hmat_oracle as O
@@ -93,7 +104,7 @@ def test_sharded_build_and_solve(world):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, backend, q)) for r in range(world)]
     for p in procs:
         p.start()
     out = sorted((q.get(timeout=300) for _ in procs), key=lambda t: t[0])
