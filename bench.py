@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--refine", type=int, default=1, help="FP64 refinement steps (batched workload)")
     ap.add_argument("--shard", default="none", choices=["none", "subtree"],
                     help="subtree: one headline system sharded over the ranks by subtrees (FP64)")
+    ap.add_argument("--shard-build", default="sharded", choices=["sharded", "whole"],
+                    help="--shard subtree: build only this rank's rows (sharded) or the whole operator per rank")
     ap.add_argument("--hss-form", default="reference", choices=["reference", "nested"],
                     help="hss workload: identity transfers (the reference's form) or nested bases")
     return ap.parse_args()
@@ -461,8 +463,11 @@ def run_shard(args):
     over the ranks by subtrees (hmat_shard.py): rank g keeps its depth-log2(P) subtree in
     its own engine handle and its rows of the top couplings; a step is the FP64
     factorization (local engine + top levels) and the solve, with NCCL all-reduces of the
-    top levels' small matrices.  Every rank builds the whole operator (the top-level
-    compression is not sharded).  Strong scaling: the work is fixed as P grows."""
+    top levels' small matrices.  The build is sharded too (--shard-build sharded, the
+    default): each rank builds its own subtree from its own points and compresses its rows
+    of the top couplings (hmat_shard.build_top_sharded with generated block products on
+    the device); --shard-build whole builds the whole operator on every rank and slices it.
+    Strong scaling: the work is fixed as P grows."""
     import torch
     import torch.distributed as dist
     import hmat_b200 as H
@@ -478,20 +483,34 @@ def run_shard(args):
     torch.cuda.set_stream(torch.cuda.Stream(device=dev))   # a real stream: the library launches on it
     stream = torch.cuda.current_stream()
     N, s = args.n, args.nrhs
+    pts, params = morton_points(N, 3), [1e-3, 4.0]
     h = H.HODLRMatrix(1e-10, rsvd_rank=args.rank, oversample=10, max_rank=args.rank, sketch=H.SKETCH_DEVICE_NORMAL,
                       seed=0, precision=H.FP64)
     h.set_stream(stream.cuda_stream)
-    h.build_from_kernel(H.KERNEL_COULOMB, morton_points(N, 3), [1e-3, 4.0], args.leaf)
     plan = S.partition(N, args.leaf, world)
     r0, r1 = plan.owner_range(rank)
+    t_build = time.perf_counter()
     if world == 1:
+        h.build_from_kernel(H.KERNEL_COULOMB, pts, params, args.leaf)
         local, top, table = S.EngineLocalSolver.from_handle(h), {}, {}
+    elif args.shard_build == "sharded":
+        dense = H.Dense()
+        dense.set_stream(stream.cuda_stream)
+        top, table, _ = S.build_top_sharded(plan, rank, S.device_block_product(dense, H.KERNEL_COULOMB, pts, params),
+                                            1e-10, args.rank, oversample=10, seed=0, ops=S.TorchOps(dev),
+                                            allreduce=S.torch_allreduce)
+        dense.close()
+        h.build_from_kernel(H.KERNEL_COULOMB, pts[r0:r1], params, args.leaf)    # this rank's subtree only
+        local = S.EngineLocalSolver.from_handle(h)
     else:
+        h.build_from_kernel(H.KERNEL_COULOMB, pts, params, args.leaf)
         nodes = S.nodes_from_handle(h, (r0, r1))
         sub, top, table = S.rank_share(plan, rank, nodes)
         local = S.EngineLocalSolver(sub, r0, args.leaf, stream.cuda_stream)
         top = S.to_torch_share(top, dev)
         h.close()
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t_build
     sh = S.ShardedHODLR(plan, rank, local, top, table, S.TorchOps(dev), S.torch_allreduce)
     b = torch.from_numpy(np.random.default_rng(3).standard_normal((N, s))[r0:r1].copy()).to(dev)
 
@@ -518,7 +537,8 @@ def run_shard(args):
             "value": s / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": dict(workload_config(args), parallelism=f"subtree shards x{world}"),
-            "collectives_per_step": sh.collectives // max(1, args.steps + args.warmup)}))
+            "collectives_per_step": sh.collectives // max(1, args.steps + args.warmup),
+            "build_s_rank0": t_build, "shard_build": args.shard_build if world > 1 else "whole"}))
     if world > 1:
         dist.destroy_process_group()
 
