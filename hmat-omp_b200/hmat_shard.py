@@ -184,20 +184,8 @@ class ShardedHODLR:
     def _reduce_packed(self, d: int, shapes: list, mine):
         """All-reduce one buffer holding a block per top node of depth d (shapes[i] =
         (rows, cols) of node i's block); this rank fills its node's block with `mine`."""
-        me = self.path[d].slot
-        tot_rows = max(r for r, _ in shapes)
-        offs, c0 = [], 0
-        for _, c in shapes:
-            offs.append(c0)
-            c0 += c
-        buf = self.ops.zeros(tot_rows, max(c0, 1))
-        r, c = shapes[me]
-        if r and c:
-            buf[:r, offs[me]:offs[me] + c] = mine
-        out = self.allreduce(buf)
-        out = buf if out is None else out
         self.collectives += 1
-        return out[:r, offs[me]:offs[me] + c]
+        return _packed_allreduce(self.ops, self.allreduce, shapes, self.path[d].slot, mine)
 
     def _side_rows(self, d: int):
         n = self.path[d]
